@@ -1,0 +1,97 @@
+"""ctypes binding of the C ABI in include/aniso_b200.h (libaniso_b200.so, built in-tree).
+
+There is no fallback: if the library is missing, importing the package fails with the command
+that builds it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libaniso_b200.so")
+
+OK = 0
+ERR_ARGUMENT = 1
+ERR_CUDA = 2
+ERR_NO_DEVICE = 3
+ERR_OUT_OF_MEMORY = 4
+ERR_DEVICE_WAIT = 5
+
+# Every symbol include/aniso_b200.h declares.
+EXPORTS = [
+    "aniso_b200_available",
+    "aniso_b200_scene_create",
+    "aniso_b200_scene_create_raw",
+    "aniso_b200_scene_destroy",
+    "aniso_b200_render",
+    "aniso_b200_render_device",
+    "aniso_b200_sync",
+    "aniso_b200_last_error",
+    "aniso_b200_debug_projection",
+    "aniso_b200_debug_sorted",
+    "aniso_b200_sort_projection",
+]
+
+
+class Camera(ctypes.Structure):
+    _fields_ = [("R", ctypes.c_double * 9), ("t", ctypes.c_double * 3), ("fx", ctypes.c_double),
+                ("fy", ctypes.c_double), ("cx", ctypes.c_double), ("cy", ctypes.c_double),
+                ("width", ctypes.c_int32), ("height", ctypes.c_int32)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("sh_degree", ctypes.c_int32), ("splat_scale", ctypes.c_float)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("visible", ctypes.c_uint64), ("tile_pairs", ctypes.c_uint64), ("project_ms", ctypes.c_double),
+                ("sort_ms", ctypes.c_double), ("blend_ms", ctypes.c_double)]
+
+
+class AnisoError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("aniso_b200 error %d: %s" % (code, message))
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("%s is missing: build it with `python -m aniso_b200.build`" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    I64, I32, U64 = ctypes.c_int64, ctypes.c_int32, ctypes.c_uint64
+    sig = {
+        "aniso_b200_available": [ctypes.POINTER(I32)],
+        "aniso_b200_scene_create": [P, P, I64, I32, ctypes.POINTER(P)],
+        "aniso_b200_scene_create_raw": [P, P, P, P, P, P, I64, I32, ctypes.POINTER(P)],
+        "aniso_b200_scene_destroy": [P],
+        "aniso_b200_render": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, ctypes.POINTER(Stats)],
+        "aniso_b200_render_device": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, P],
+        "aniso_b200_sync": [P, ctypes.POINTER(Stats)],
+        "aniso_b200_debug_projection": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, P, P, P, P, P],
+        "aniso_b200_debug_sorted": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, P, U64, P,
+                                    ctypes.POINTER(U64)],
+        "aniso_b200_sort_projection": [I64, P, P, P, I32, I32, P, P, U64, P, ctypes.POINTER(U64)],
+    }
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    lib.aniso_b200_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    lib.aniso_b200_last_error.restype = ctypes.c_size_t
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib.aniso_b200_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int):
+    if rc != OK:
+        raise AnisoError(rc, last_error())

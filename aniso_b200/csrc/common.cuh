@@ -1,0 +1,200 @@
+// Shared device-side definitions of the B200 Gaussian-splat rasterizer.
+//
+// Layout in HBM (one scene, N Gaussians, all 16-byte aligned so every load is a 128-bit load):
+//   pos_op  float4[N]   x, y, z, opacity (activated)
+//   scale   float4[N]   sx, sy, sz, 0     (activated, i.e. exp of the PLY's log-scale)
+//   rot     float4[N]   w, x, y, z        (normalised)
+//   sh      float4[P][N]  P = ceil(3K/4) planes; plane p holds floats 4p..4p+3 of the
+//                         Gaussian's 3K SH floats in [coefficient][channel] order (gaussian.h:33-35)
+// Per view:
+//   rec     float4[3][N]  blend record of each visible Gaussian (see SplatRecord)
+//   rect    uint64[N]     16x16-tile rectangle x0 | y0 << 16 | x1 << 32 | y1 << 48
+//   vis_key / vis_idx     compacted visible list: depth bits and Gaussian index, index order
+//   pair_key / pair_val   one (tile, Gaussian) pair per tile a splat touches
+//   ranges  uint2[tiles]  [start, end) of each tile's run in the sorted pair list
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ab2 {
+
+constexpr int kTile = 16;     // key / blend tile edge in pixels (gpu_render.cu:15)
+constexpr int kCpuTile = 8;   // the CPU renderer's binning tile (render.cpp:16)
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kMaxPasses = 4;
+constexpr unsigned kSpinLimit = 1u << 20;  // bound on every look-back wait
+
+// Per-view constants, packed on the host exactly as gpu_render.cu:301-316 packs CameraParams.
+struct CamParams {
+    float R[9];  // world to camera, row major
+    float t[3];
+    float eye[3];
+    float fx, fy, cx, cy;
+    int width, height, tilesX, tilesY;
+    int shDegree;   // rendered degree: min(option, scene)
+    int shCoeffs;   // coefficients per channel stored in the scene
+    float splatScale;
+};
+
+struct SceneView {
+    const float4* pos_op;
+    const float4* scale;
+    const float4* rot;
+    const float4* sh;   // planes
+    int64_t n;
+    int sh_planes;
+};
+
+// Control block of one frame. Zeroed (except epoch, which advances) by frame_begin.
+struct Ctrl {
+    unsigned long long pair_total;  // sum of tiles touched over visible Gaussians
+    unsigned int vis_count;         // visible Gaussians
+    unsigned int flags;             // kFlag* bits, read back by the host after the frame
+    unsigned int epoch;             // tags look-back status words of this frame
+    unsigned int sticky_flags;      // OR of the flags of earlier frames since the host last read it
+    unsigned long long max_pair_total;  // largest pair_total of earlier frames since then
+    unsigned int chunk_ctr[16];     // dynamic chunk counters, one per kernel launch of the frame
+    unsigned int depth_hist[kMaxPasses * kRadix];
+    unsigned int tile_hist[kMaxPasses * kRadix];
+};
+
+enum : unsigned {
+    kFlagOverflow = 1u,  // pairs exceeded the pair capacity: nothing after duplication ran
+    kFlagTimeout = 2u,   // a look-back wait hit kSpinLimit (never expected)
+};
+
+// Chunk counter slots.
+enum : int { kCtrPre = 0, kCtrDepth0 = 1, kCtrDup = 5, kCtrTile0 = 6, kCtrCompact = 10 };
+
+// ---- look-back status words: [epoch:30][flag:2][value:32] ------------------------------------
+enum : unsigned { kStAgg = 1u, kStInc = 2u };
+
+__device__ __forceinline__ unsigned long long st_make(unsigned epoch, unsigned flag, unsigned value) {
+    return (static_cast<unsigned long long>(epoch & 0x3FFFFFFFu) << 34) |
+           (static_cast<unsigned long long>(flag) << 32) | value;
+}
+__device__ __forceinline__ unsigned st_flag(unsigned long long s, unsigned epoch) {
+    return (static_cast<unsigned>(s >> 34) == (epoch & 0x3FFFFFFFu)) ? static_cast<unsigned>(s >> 32) & 3u : 0u;
+}
+__device__ __forceinline__ void st_store(unsigned long long* p, unsigned long long v) {
+    *reinterpret_cast<volatile unsigned long long*>(p) = v;
+}
+__device__ __forceinline__ unsigned long long st_load(const unsigned long long* p) {
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Inclusive warp scan.
+__device__ __forceinline__ unsigned warp_incl_scan(unsigned v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= o) v += y;
+    }
+    return v;
+}
+
+// Exclusive scan over a block of NT threads (NT a multiple of 32, at most 1024); s_tmp holds
+// NT/32 words. Returns the thread's exclusive prefix and the block total.
+template <int NT>
+__device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* s_tmp, unsigned& total) {
+    constexpr int W = NT / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned incl = warp_incl_scan(v);
+    if (lane == 31) s_tmp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned x = lane < W ? s_tmp[lane] : 0u;
+        x = warp_incl_scan(x);
+        if (lane < W) s_tmp[lane] = x;
+    }
+    __syncthreads();
+    total = s_tmp[W - 1];
+    const unsigned before = warp > 0 ? s_tmp[warp - 1] : 0u;
+    __syncthreads();
+    return before + incl - v;
+}
+
+// Decoupled look-back for one running total, done by one whole warp. Publishes `aggregate` for
+// `chunk`, waits (bounded) for the predecessors, publishes the inclusive total and returns the
+// exclusive prefix to every lane.
+__device__ __forceinline__ unsigned lookback_warp(unsigned long long* status, unsigned chunk, unsigned aggregate,
+                                                  unsigned epoch, unsigned* flags) {
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) st_store(status + chunk, st_make(epoch, chunk == 0 ? kStInc : kStAgg, aggregate));
+    unsigned exclusive = 0;
+    if (chunk > 0) {
+        long long pos = static_cast<long long>(chunk) - 1;
+        unsigned spins = 0;
+        while (true) {
+            const long long idx = pos - lane;
+            unsigned flag, value;
+            if (idx >= 0) {
+                const unsigned long long s = st_load(status + idx);
+                flag = st_flag(s, epoch);
+                value = static_cast<unsigned>(s);
+            } else {
+                flag = kStInc;
+                value = 0;
+            }
+            const unsigned inc = __ballot_sync(0xFFFFFFFFu, flag == kStInc);
+            const unsigned ready = __ballot_sync(0xFFFFFFFFu, flag != 0);
+            if (inc) {
+                const int k = __ffs(inc) - 1;
+                const unsigned need = k == 31 ? 0xFFFFFFFFu : ((2u << k) - 1u);
+                if ((ready & need) == need) {
+                    unsigned v = lane <= k ? value : 0u;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+                    exclusive += v;
+                    break;
+                }
+            } else if (ready == 0xFFFFFFFFu) {
+                unsigned v = value;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+                exclusive += v;
+                pos -= 32;
+                continue;
+            }
+            if (++spins > kSpinLimit) {
+                if (lane == 0) atomicOr(flags, kFlagTimeout);
+                break;
+            }
+        }
+        if (lane == 0) st_store(status + chunk, st_make(epoch, kStInc, exclusive + aggregate));
+    }
+    return exclusive;
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Blend record: three float4 per visible Gaussian.
+//   r0 = (u, v, A2, B2)     r1 = (C2, L, r, g)     r2 = (b, bx, by, 0)
+// where the exponent of the Gaussian in base 2 is A2 dx^2 + B2 dx dy + C2 dy^2 (the conic scaled
+// by -log2(e)/2, -log2(e), -log2(e)/2), L = log2(opacity), and bx / by hold two int16 pixel bounds
+// (lo | hi << 16): the pixels that lie both in the splat's 8x8-tile rectangle (render.cpp:166-171)
+// and inside the ellipse where alpha can reach 1/255 (with a safety margin).
+struct SplatRecord {
+    float4 r0, r1, r2;
+};
+
+__device__ __forceinline__ unsigned pack_i16x2(int lo, int hi) {
+    return (static_cast<unsigned>(lo) & 0xFFFFu) | (static_cast<unsigned>(hi) << 16);
+}
+__device__ __forceinline__ int unpack_lo(unsigned v) { return static_cast<int>(static_cast<short>(v & 0xFFFFu)); }
+__device__ __forceinline__ int unpack_hi(unsigned v) { return static_cast<int>(static_cast<short>(v >> 16)); }
+
+}  // namespace ab2

@@ -1,0 +1,69 @@
+// Host-side launchers of the rasterizer kernels (internal to the library).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace ab2 {
+
+// Optional per-Gaussian outputs in the reference kernel's own layout (gpu_render.cu:86-88), for
+// the parity tests: uv float2, conicOpacity float4, depth float, rgb float3, rect uint4,
+// tilesTouched uint32 (0 for culled Gaussians).
+struct DebugProjection {
+    float2* uv = nullptr;
+    float4* conic_opacity = nullptr;
+    float* depth = nullptr;
+    float* rgb = nullptr;
+    uint4* rect = nullptr;
+    unsigned* tiles_touched = nullptr;
+};
+
+// Clears the frame's control block (counters, histograms, flags) and advances its epoch.
+void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
+
+void launch_preprocess(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
+                       unsigned long long* rect16, unsigned* vis_key, unsigned* vis_idx, unsigned long long* status,
+                       const DebugProjection* dbg, cudaStream_t stream);
+
+// One stable onesweep LSD radix pass over (key, value) u32 pairs, 8-bit digit at `shift`.
+// `count` is read on the device; blocks beyond it exit. `hist` holds this digit's global
+// histogram; `status` has max_chunks * 256 words.
+int onesweep_items_per_thread();
+unsigned onesweep_chunk_items();
+void launch_onesweep(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
+                     const unsigned* count, const unsigned long long* count64, unsigned capacity, int shift,
+                     const unsigned* hist, unsigned long long* status, unsigned* chunk_ctr, Ctrl* ctrl,
+                     cudaStream_t stream);
+
+// Expands the depth-sorted visible list into (tile, Gaussian) pairs in depth order, building the
+// tile-digit histograms; sets kFlagOverflow (and writes nothing) if the pairs exceed capacity.
+unsigned duplicate_chunk_items();
+void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
+                      unsigned max_visible, int tiles_x, int tile_passes, unsigned* pair_key, unsigned* pair_val,
+                      unsigned long long* status, cudaStream_t stream);
+
+// ranges[tile] = [start, end) over the sorted tile keys (gpu_render.cu:164-177); ranges must be
+// zeroed before.
+void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capacity, uint2* ranges,
+                   cudaStream_t stream);
+
+// Compacts an externally given projection (tiles_touched, depth) into the visible list, as the
+// preprocess kernel does, for sorting a projection computed elsewhere.
+void launch_compact_projection(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
+                               Ctrl* ctrl, unsigned* vis_key, unsigned* vis_idx, unsigned long long* rect16,
+                               unsigned long long* status, cudaStream_t stream);
+
+// Blend outputs.
+struct BlendOut {
+    uint8_t* rgb8 = nullptr;        // H x W x 3 (gpu_render.cu:227-232 rounding)
+    float* rgbf = nullptr;          // H x W x 3 unclamped colour (differentiable path)
+    float* t_final = nullptr;       // H x W transmittance after the last applied splat
+    unsigned* n_contrib = nullptr;  // H x W: position in the tile list one past the last applied splat
+};
+
+void launch_blend(const uint2* ranges, const unsigned* sorted_vals, const SplatRecord* rec, const Ctrl* ctrl,
+                  int width, int height, int tiles_x, int tiles_y, const BlendOut& out, cudaStream_t stream);
+
+}  // namespace ab2

@@ -1,0 +1,273 @@
+// Step 1 of the rasterizer: one thread per Gaussian.
+//
+// Projects each Gaussian the way gpu_render.cu:86-145 does (the same fp32 expressions in the same
+// order, compiled without fast-math, so depth, rectangle and conic come out bit-identical to the
+// reference kernel built without --use_fast_math), then, fused into the same kernel:
+//   * writes the blend record (SplatRecord) and the 16x16-tile rectangle of visible Gaussians;
+//   * compacts the visible Gaussians, in index order, into (depth bits, index) with a single-pass
+//     decoupled look-back -- the input of the stable depth sort;
+//   * builds the four 8-bit digit histograms of the depth bits for the onesweep passes and sums
+//     the pair count (tiles touched) of the frame.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ab2 {
+namespace {
+
+constexpr float kShC1 = 0.4886025119029199f;
+constexpr float kShC2_0 = 1.0925484305920792f, kShC2_1 = -1.0925484305920792f, kShC2_2 = 0.31539156525252005f,
+                kShC2_3 = -1.0925484305920792f, kShC2_4 = 0.5462742152960396f;
+constexpr float kShC3_0 = -0.5900435899266435f, kShC3_1 = 2.890611442640554f, kShC3_2 = -0.4570457994644658f,
+                kShC3_3 = 0.3731763325901154f, kShC3_4 = -0.4570457994644658f, kShC3_5 = 1.445305721320277f,
+                kShC3_6 = -0.5900435899266435f;
+
+// SH colour of degree D along (x, y, z): the basis of sh.cpp:18-58 / gpu_render.cu:56-83, summed in
+// the same order, then +0.5 and clamped at 0.
+template <int D>
+__device__ __forceinline__ float3 sh_color(const float* sh, float x, float y, float z) {
+    float b[16];
+    b[0] = 0.28209479177387814f;
+    if (D >= 1) {
+        b[1] = -kShC1 * y; b[2] = kShC1 * z; b[3] = -kShC1 * x;
+    }
+    if (D >= 2) {
+        const float xx = x * x, yy = y * y, zz = z * z;
+        b[4] = kShC2_0 * x * y; b[5] = kShC2_1 * y * z; b[6] = kShC2_2 * (2 * zz - xx - yy);
+        b[7] = kShC2_3 * x * z; b[8] = kShC2_4 * (xx - yy);
+        if (D >= 3) {
+            b[9] = kShC3_0 * y * (3 * xx - yy); b[10] = kShC3_1 * x * y * z; b[11] = kShC3_2 * y * (4 * zz - xx - yy);
+            b[12] = kShC3_3 * z * (2 * zz - 3 * xx - 3 * yy); b[13] = kShC3_4 * x * (4 * zz - xx - yy);
+            b[14] = kShC3_5 * z * (xx - yy); b[15] = kShC3_6 * x * (xx - 3 * yy);
+        }
+    }
+    constexpr int count = (D + 1) * (D + 1);
+    float3 c = make_float3(0.5f, 0.5f, 0.5f);
+#pragma unroll
+    for (int k = 0; k < count; ++k) {
+        c.x += b[k] * sh[k * 3 + 0];
+        c.y += b[k] * sh[k * 3 + 1];
+        c.z += b[k] * sh[k * 3 + 2];
+    }
+    return make_float3(fmaxf(c.x, 0.f), fmaxf(c.y, 0.f), fmaxf(c.z, 0.f));
+}
+
+struct Projected {
+    float u, v, depth;
+    float a, b, c, det;       // 2D covariance (with the 0.3 low-pass) and its determinant
+    float conicA, conicB, conicC;
+    int radius;
+    int x0, y0, x1, y1;       // 16x16-tile rectangle
+};
+
+// The culling and projection of gpu_render.cu:93-135. Returns false when the Gaussian is culled.
+__device__ __forceinline__ bool project(const float4 pg, const float4 sg, const float4 q, const CamParams& cam,
+                                        Projected& o) {
+    const float gx = pg.x, gy = pg.y, gz = pg.z;
+    const float px = cam.R[0] * gx + cam.R[1] * gy + cam.R[2] * gz + cam.t[0];
+    const float py = cam.R[3] * gx + cam.R[4] * gy + cam.R[5] * gz + cam.t[1];
+    const float pz = cam.R[6] * gx + cam.R[7] * gy + cam.R[8] * gz + cam.t[2];
+    if (pz < 0.2f) return false;
+
+    const float w = q.x, x = q.y, y = q.z, z = q.w;
+    const float Rq[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)},
+                            {2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)},
+                            {2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)}};
+    const float s[3] = {sg.x * cam.splatScale, sg.y * cam.splatScale, sg.z * cam.splatScale};
+    float M[3][3], S[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) M[r][c] = Rq[r][c] * s[c];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) S[r][c] = M[r][0] * M[c][0] + M[r][1] * M[c][1] + M[r][2] * M[c][2];
+
+    const float limX = 1.3f * 0.5f * cam.width / cam.fx, limY = 1.3f * 0.5f * cam.height / cam.fy;
+    const float tx = fminf(limX, fmaxf(-limX, px / pz)) * pz;
+    const float ty = fminf(limY, fmaxf(-limY, py / pz)) * pz;
+    const float J[2][3] = {{cam.fx / pz, 0, -cam.fx * tx / (pz * pz)}, {0, cam.fy / pz, -cam.fy * ty / (pz * pz)}};
+    float T[2][3];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) T[r][c] = J[r][0] * cam.R[c] + J[r][1] * cam.R[3 + c] + J[r][2] * cam.R[6 + c];
+    float TS[2][3];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) TS[r][c] = T[r][0] * S[0][c] + T[r][1] * S[1][c] + T[r][2] * S[2][c];
+    const float a = TS[0][0] * T[0][0] + TS[0][1] * T[0][1] + TS[0][2] * T[0][2] + 0.3f;
+    const float b = TS[0][0] * T[1][0] + TS[0][1] * T[1][1] + TS[0][2] * T[1][2];
+    const float c = TS[1][0] * T[1][0] + TS[1][1] * T[1][1] + TS[1][2] * T[1][2] + 0.3f;
+    const float det = a * c - b * b;
+    if (det <= 0) return false;
+
+    const float mid = 0.5f * (a + c);
+    const float lambda = mid + sqrtf(fmaxf(0.1f, mid * mid - det));
+    const int radius = (int)ceilf(3.0f * sqrtf(lambda));
+    const float u = cam.fx * px / pz + cam.cx, v = cam.fy * py / pz + cam.cy;
+    if (u + radius < 0 || v + radius < 0 || u - radius >= cam.width || v - radius >= cam.height) return false;
+
+    const int x0 = max(0, (int)(u - radius) / kTile), y0 = max(0, (int)(v - radius) / kTile);
+    const int x1 = min(cam.tilesX - 1, (int)(u + radius) / kTile), y1 = min(cam.tilesY - 1, (int)(v + radius) / kTile);
+    if (x1 < x0 || y1 < y0) return false;
+
+    o.u = u; o.v = v; o.depth = pz;
+    o.a = a; o.b = b; o.c = c; o.det = det;
+    o.conicA = c / det; o.conicB = -b / det; o.conicC = a / det;
+    o.radius = radius;
+    o.x0 = x0; o.y0 = y0; o.x1 = x1; o.y1 = y1;
+    return true;
+}
+
+// Pixel bounds [lo, hi] on one axis that a splat can reach with alpha >= 1/255, cut to the pixels
+// of its 8x8-tile rectangle (render.cpp:166-171) and to the image.
+__device__ __forceinline__ unsigned axis_bounds(float centre, float cov, float tau, int radius, int size) {
+    const int tiles8 = (size + kCpuTile - 1) / kCpuTile;
+    const int t0 = max(0, (int)(centre - radius) / kCpuTile);
+    const int t1 = min(tiles8 - 1, (int)(centre + radius) / kCpuTile);
+    int lo = t0 * kCpuTile, hi = min(t1 * kCpuTile + kCpuTile - 1, size - 1);
+    if (tau >= 0.f) {
+        const float h = sqrtf(2.0f * tau * cov) * 1.001f + 0.05f;
+        const float flo = fminf(fmaxf(ceilf(centre - h - 0.5f), -1.0f), (float)size);
+        const float fhi = fminf(fmaxf(floorf(centre + h - 0.5f), -1.0f), (float)size);
+        lo = max(lo, (int)flo);
+        hi = min(hi, (int)fhi);
+    } else {
+        lo = 1;
+        hi = 0;
+    }
+    if (lo > hi) {
+        lo = 1;
+        hi = 0;
+    }
+    return pack_i16x2(lo, hi);
+}
+
+template <int D, bool kDebug>
+__global__ void __launch_bounds__(256) preprocess_kernel(SceneView sc, CamParams cam, Ctrl* __restrict__ ctrl,
+                                                         SplatRecord* __restrict__ rec,
+                                                         unsigned long long* __restrict__ rect16,
+                                                         unsigned* __restrict__ vis_key,
+                                                         unsigned* __restrict__ vis_idx,
+                                                         unsigned long long* __restrict__ status, DebugProjection dbg) {
+    __shared__ unsigned s_chunk;
+    __shared__ unsigned s_tmp[8];
+    __shared__ unsigned s_base;
+    __shared__ unsigned s_hist[kMaxPasses * kRadix];
+    const int tid = threadIdx.x;
+    for (int k = tid; k < kMaxPasses * kRadix; k += 256) s_hist[k] = 0;
+    if (tid == 0) s_chunk = atomicAdd(&ctrl->chunk_ctr[kCtrPre], 1u);
+    __syncthreads();
+    const unsigned chunk = s_chunk;
+    const int64_t i = static_cast<int64_t>(chunk) * 256 + tid;
+
+    bool vis = false;
+    unsigned depth_bits = 0, count = 0;
+    if (i < sc.n) {
+        const float4 pg = sc.pos_op[i];
+        const float4 sg = sc.scale[i];
+        const float4 q = sc.rot[i];
+        Projected p;
+        vis = project(pg, sg, q, cam, p);
+        if (kDebug) dbg.tiles_touched[i] = 0;
+        if (vis) {
+            // Colour along the unit direction from the camera centre (gpu_render.cu:137-139).
+            constexpr int planes = ((D + 1) * (D + 1) * 3 + 3) / 4;
+            float sh[planes * 4];
+#pragma unroll
+            for (int k = 0; k < planes; ++k) {
+                const float4 f = sc.sh[static_cast<int64_t>(k) * sc.n + i];
+                sh[4 * k + 0] = f.x;
+                sh[4 * k + 1] = f.y;
+                sh[4 * k + 2] = f.z;
+                sh[4 * k + 3] = f.w;
+            }
+            float3 d = make_float3(pg.x - cam.eye[0], pg.y - cam.eye[1], pg.z - cam.eye[2]);
+            const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+            const float3 rgb = sh_color<D>(sh, d.x / len, d.y / len, d.z / len);
+
+            const float opacity = pg.w;
+            // alpha = min(0.99, opacity * exp(power)) >= 1/255 needs power >= -ln(255 opacity): a
+            // margin of 1% + 0.02 on that bound keeps the cut conservative under rounding. A NaN
+            // opacity gives alpha 0.99 everywhere (as fminf does in the reference), so no cut then.
+            float tau = logf(255.0f * opacity) * 1.01f + 0.02f;
+            if (isnan(tau)) tau = 3.0e38f;
+            const unsigned bx = axis_bounds(p.u, p.a, tau, p.radius, cam.width);
+            const unsigned by = axis_bounds(p.v, p.c, tau, p.radius, cam.height);
+            constexpr float kHalfLog2e = -0.72134752044448170368f;  // -log2(e) / 2
+            constexpr float kLog2e = -1.44269504088896340736f;      // -log2(e)
+            SplatRecord r;
+            r.r0 = make_float4(p.u, p.v, kHalfLog2e * p.conicA, kLog2e * p.conicB);
+            r.r1 = make_float4(kHalfLog2e * p.conicC, log2f(opacity), rgb.x, rgb.y);
+            r.r2 = make_float4(rgb.z, __uint_as_float(bx), __uint_as_float(by), 0.f);
+            rec[i] = r;
+            rect16[i] = static_cast<unsigned long long>(p.x0) | (static_cast<unsigned long long>(p.y0) << 16) |
+                        (static_cast<unsigned long long>(p.x1) << 32) | (static_cast<unsigned long long>(p.y1) << 48);
+            depth_bits = __float_as_uint(p.depth);
+            count = static_cast<unsigned>((p.x1 - p.x0 + 1) * (p.y1 - p.y0 + 1));
+            if (kDebug) {
+                dbg.uv[i] = make_float2(p.u, p.v);
+                dbg.conic_opacity[i] = make_float4(p.conicA, p.conicB, p.conicC, opacity);
+                dbg.depth[i] = p.depth;
+                dbg.rgb[3 * i + 0] = rgb.x;
+                dbg.rgb[3 * i + 1] = rgb.y;
+                dbg.rgb[3 * i + 2] = rgb.z;
+                dbg.rect[i] = make_uint4(p.x0, p.y0, p.x1, p.y1);
+                dbg.tiles_touched[i] = count;
+            }
+#pragma unroll
+            for (int pass = 0; pass < kMaxPasses; ++pass)
+                atomicAdd(&s_hist[pass * kRadix + ((depth_bits >> (pass * kRadixBits)) & (kRadix - 1))], 1u);
+        }
+    }
+
+    // Stable compaction of the visible Gaussians (index order) with a decoupled look-back.
+    unsigned total = 0;
+    const unsigned local = block_excl_scan<256>(vis ? 1u : 0u, s_tmp, total);
+    unsigned pairs_total = 0;
+    block_excl_scan<256>(count, s_tmp, pairs_total);
+    if (tid < 32) {
+        const unsigned base = lookback_warp(status, chunk, total, ctrl->epoch, &ctrl->flags);
+        if (tid == 0) {
+            s_base = base;
+            if (total) atomicAdd(&ctrl->vis_count, total);
+            if (pairs_total) atomicAdd(&ctrl->pair_total, static_cast<unsigned long long>(pairs_total));
+        }
+    }
+    __syncthreads();
+    if (vis) {
+        vis_key[s_base + local] = depth_bits;
+        vis_idx[s_base + local] = static_cast<unsigned>(i);
+    }
+    for (int k = tid; k < kMaxPasses * kRadix; k += 256)
+        if (s_hist[k]) atomicAdd(&ctrl->depth_hist[k], s_hist[k]);
+}
+
+template <bool kDebug>
+void launch_preprocess_t(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
+                         unsigned long long* rect16, unsigned* vis_key, unsigned* vis_idx,
+                         unsigned long long* status, const DebugProjection& dbg, cudaStream_t stream) {
+    const unsigned blocks = static_cast<unsigned>((sc.n + 255) / 256);
+    if (blocks == 0) return;
+    switch (cam.shDegree) {
+        case 0: preprocess_kernel<0, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, dbg); break;
+        case 1: preprocess_kernel<1, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, dbg); break;
+        case 2: preprocess_kernel<2, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, dbg); break;
+        default: preprocess_kernel<3, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, dbg); break;
+    }
+}
+
+}  // namespace
+
+void launch_preprocess(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
+                       unsigned long long* rect16, unsigned* vis_key, unsigned* vis_idx, unsigned long long* status,
+                       const DebugProjection* dbg, cudaStream_t stream) {
+    if (dbg)
+        launch_preprocess_t<true>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, *dbg, stream);
+    else
+        launch_preprocess_t<false>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, DebugProjection{}, stream);
+}
+
+}  // namespace ab2

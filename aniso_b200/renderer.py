@@ -1,0 +1,177 @@
+"""Python mirror of the reference's GPU renderer interface, aniso::GpuRenderer
+(include/aniso/gpu_render.h:22-37), over the C ABI of libaniso_b200.so.
+
+    r = GpuRenderer(gaussians, sh, sh_degree)     # GpuRenderer(const Scene&): uploads once
+    img = r.render(camera, stats, options)        # Image render(const Camera&, RenderStats*, ...)
+    GpuRenderer.available()                       # static bool available()
+
+Errors raise AnisoError (the reference throws std::runtime_error, gpu_render.cu:18-21).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+
+@dataclasses.dataclass
+class RenderOptions:
+    """aniso::RenderOptions (render.h:28-33)."""
+
+    sh_degree: int = 3
+    splat_scale: float = 1.0
+
+    def c(self) -> _lib.Options:
+        return _lib.Options(int(self.sh_degree), float(self.splat_scale))
+
+
+def c_camera(cam) -> _lib.Camera:
+    c = _lib.Camera()
+    R = np.asarray(cam.R, np.float64).reshape(9)
+    t = np.asarray(cam.t, np.float64).reshape(3)
+    for k in range(9):
+        c.R[k] = float(R[k])
+    for k in range(3):
+        c.t[k] = float(t[k])
+    c.fx, c.fy, c.cx, c.cy = float(cam.fx), float(cam.fy), float(cam.cx), float(cam.cy)
+    c.width, c.height = int(cam.width), int(cam.height)
+    return c
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _stats_dict(s: _lib.Stats) -> dict:
+    return {"visible": int(s.visible), "tile_pairs": int(s.tile_pairs), "project_ms": s.project_ms,
+            "sort_ms": s.sort_ms, "blend_ms": s.blend_ms}
+
+
+class GpuRenderer:
+    def __init__(self, gaussians: np.ndarray, sh: np.ndarray, sh_degree: int):
+        g = np.ascontiguousarray(gaussians, np.float32)
+        s = np.ascontiguousarray(sh, np.float32)
+        n = g.shape[0]
+        if g.shape != (n, 11):
+            raise ValueError("gaussians must be (n, 11)")
+        if s.size != n * (sh_degree + 1) ** 2 * 3:
+            raise ValueError("sh must hold n * (degree+1)^2 * 3 floats")
+        self._h = ctypes.c_void_p()
+        check(lib.aniso_b200_scene_create(_ptr(g), _ptr(s), n, sh_degree, ctypes.byref(self._h)))
+        self.n = n
+        self.sh_degree = sh_degree
+
+    @classmethod
+    def from_raw(cls, raw) -> "GpuRenderer":
+        """Uploads a scene in the PLY's raw form and activates it on the device."""
+        self = cls.__new__(cls)
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        xyz, dc, rest, op, sc, rot = f(raw.xyz), f(raw.f_dc), f(raw.f_rest), f(raw.opacity), f(raw.scale), f(raw.rot)
+        self._h = ctypes.c_void_p()
+        check(lib.aniso_b200_scene_create_raw(_ptr(xyz), _ptr(dc), _ptr(rest), _ptr(op), _ptr(sc), _ptr(rot), raw.n,
+                                              raw.sh_degree, ctypes.byref(self._h)))
+        self.n = raw.n
+        self.sh_degree = raw.sh_degree
+        return self
+
+    @staticmethod
+    def available() -> bool:
+        a = ctypes.c_int32(0)
+        check(lib.aniso_b200_available(ctypes.byref(a)))
+        return bool(a.value)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.aniso_b200_scene_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, camera, stats: dict | None = None, options: RenderOptions | None = None,
+               out: np.ndarray | None = None) -> np.ndarray:
+        """RGB8 image (H, W, 3) in host memory; fills `stats` like RenderStats if given."""
+        o = (options or RenderOptions()).c()
+        c = c_camera(camera)
+        if out is None:
+            out = np.empty((camera.height, camera.width, 3), np.uint8)
+        assert out.shape == (camera.height, camera.width, 3) and out.dtype == np.uint8
+        st = _lib.Stats()
+        check(lib.aniso_b200_render(self._h, ctypes.byref(c), ctypes.byref(o), _ptr(out),
+                                    ctypes.byref(st) if stats is not None else None))
+        if stats is not None:
+            stats.update(_stats_dict(st))
+        return out
+
+    def render_device(self, camera, rgb_device_ptr: int, stream_ptr: int = 0,
+                      options: RenderOptions | None = None):
+        """Enqueues a render into device memory on a CUDA stream; no wait."""
+        o = (options or RenderOptions()).c()
+        c = c_camera(camera)
+        check(lib.aniso_b200_render_device(self._h, ctypes.byref(c), ctypes.byref(o), ctypes.c_void_p(rgb_device_ptr),
+                                           ctypes.c_void_p(stream_ptr)))
+
+    def sync(self) -> dict:
+        st = _lib.Stats()
+        check(lib.aniso_b200_sync(self._h, ctypes.byref(st)))
+        return _stats_dict(st)
+
+    def debug_projection(self, camera, options: RenderOptions | None = None) -> dict:
+        """Per-Gaussian projection in the reference kernel's layout (gpu_render.cu:86-88)."""
+        n = self.n
+        o = (options or RenderOptions()).c()
+        c = c_camera(camera)
+        out = {"uv": np.zeros((n, 2), np.float32), "conic_opacity": np.zeros((n, 4), np.float32),
+               "depth": np.zeros(n, np.float32), "rgb": np.zeros((n, 3), np.float32),
+               "rect": np.zeros((n, 4), np.uint32), "tiles_touched": np.zeros(n, np.uint32)}
+        check(lib.aniso_b200_debug_projection(self._h, ctypes.byref(c), ctypes.byref(o), _ptr(out["uv"]),
+                                              _ptr(out["conic_opacity"]), _ptr(out["depth"]), _ptr(out["rgb"]),
+                                              _ptr(out["rect"]), _ptr(out["tiles_touched"])))
+        return out
+
+    def debug_sorted(self, camera, options: RenderOptions | None = None, capacity: int | None = None):
+        """(tile ids u32[P], Gaussian indices u32[P], ranges u32[T, 2]) after the sort."""
+        o = (options or RenderOptions()).c()
+        c = c_camera(camera)
+        tiles_x = (camera.width + 15) // 16
+        tiles_y = (camera.height + 15) // 16
+        cap = capacity if capacity is not None else max(1, 64 * self.n + 1024)
+        tiles = np.zeros(cap, np.uint32)
+        values = np.zeros(cap, np.uint32)
+        ranges = np.zeros((tiles_x * tiles_y, 2), np.uint32)
+        pairs = ctypes.c_uint64(0)
+        check(lib.aniso_b200_debug_sorted(self._h, ctypes.byref(c), ctypes.byref(o), _ptr(tiles), _ptr(values), cap,
+                                          _ptr(ranges), ctypes.byref(pairs)))
+        p = pairs.value
+        return tiles[:p].copy(), values[:p].copy(), ranges
+
+
+def sort_projection(tiles_touched, rect, depth, tiles_x: int, tiles_y: int):
+    """The product's sort alone, on a projection given in the reference kernel's layout."""
+    tt = np.ascontiguousarray(tiles_touched, np.uint32)
+    rc = np.ascontiguousarray(rect, np.uint32).reshape(-1, 4)
+    dp = np.ascontiguousarray(depth, np.float32)
+    n = tt.shape[0]
+    cap = max(1, int(tt.astype(np.int64).sum()))
+    tiles = np.zeros(cap, np.uint32)
+    values = np.zeros(cap, np.uint32)
+    ranges = np.zeros((tiles_x * tiles_y, 2), np.uint32)
+    pairs = ctypes.c_uint64(0)
+    check(lib.aniso_b200_sort_projection(n, _ptr(tt), _ptr(rc), _ptr(dp), tiles_x, tiles_y, _ptr(tiles),
+                                         _ptr(values), cap, _ptr(ranges), ctypes.byref(pairs)))
+    p = pairs.value
+    return tiles[:p].copy(), values[:p].copy(), ranges
+
+
+def keys_of(tiles: np.ndarray, values: np.ndarray, depth: np.ndarray) -> np.ndarray:
+    """The reference's 64-bit sort keys (tile << 32 | depth bits, gpu_render.cu:157) of a pair list."""
+    bits = np.ascontiguousarray(depth, np.float32).view(np.uint32)
+    return (tiles.astype(np.uint64) << np.uint64(32)) | bits[values].astype(np.uint64)

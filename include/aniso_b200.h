@@ -1,0 +1,132 @@
+/*
+ * aniso_b200.h -- C ABI of the B200 (sm_100a) Gaussian-splat rasterizer.
+ *
+ * The drop-in boundary for the reference's CUDA renderer, class aniso::GpuRenderer
+ * (include/aniso/gpu_render.h:22-37, implemented in src/gpu_render.cu). Plain pointers, sizes and
+ * status codes only: every call returns ANISO_B200_OK (0) or an error code, never throws across
+ * the ABI and never traps on the device; aniso_b200_last_error() gives the message. The C++ shim
+ * aniso_b200/shim/gpu_render_shim.cpp rebuilds GpuRenderer's exact signatures and exception
+ * convention on top of these calls.
+ *
+ * Threading: like GpuRenderer, one scene object is used by one host thread at a time.
+ */
+#ifndef ANISO_B200_H
+#define ANISO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    ANISO_B200_OK = 0,
+    ANISO_B200_ERR_ARGUMENT = 1,       /* a null pointer, a negative size, an unsupported degree */
+    ANISO_B200_ERR_CUDA = 2,           /* a CUDA runtime call failed; the message names it */
+    ANISO_B200_ERR_NO_DEVICE = 3,      /* no CUDA device */
+    ANISO_B200_ERR_OUT_OF_MEMORY = 4,  /* a device allocation failed */
+    ANISO_B200_ERR_DEVICE_WAIT = 5     /* a bounded device-side wait gave up (never expected) */
+};
+
+/* Opaque: one uploaded scene plus the device work buffers of its renders. */
+typedef struct aniso_b200_scene aniso_b200_scene;
+
+/* aniso::Camera (include/aniso/camera.h:16-26): world-to-camera R (row-major) and t, pinhole
+ * intrinsics in pixels, image size. */
+typedef struct aniso_b200_camera {
+    double R[9];
+    double t[3];
+    double fx, fy, cx, cy;
+    int32_t width, height;
+} aniso_b200_camera;
+
+/* aniso::RenderOptions (include/aniso/render.h:28-33). */
+typedef struct aniso_b200_options {
+    int32_t sh_degree;  /* colour up to this SH degree (0..3), clamped to the scene's */
+    float splat_scale;  /* multiplies every Gaussian's scale (1 = unchanged) */
+} aniso_b200_options;
+
+/* aniso::RenderStats (include/aniso/render.h:9-14): stage times measured with CUDA events. */
+typedef struct aniso_b200_stats {
+    uint64_t visible;    /* Gaussians that survived culling */
+    uint64_t tile_pairs; /* splat-tile pairs at 16x16 tiles (the reference GPU path's count) */
+    double project_ms;   /* projection, compaction */
+    double sort_ms;      /* depth sort, duplication, tile sort, tile ranges */
+    double blend_ms;     /* blending */
+} aniso_b200_stats;
+
+/* GpuRenderer::available() (gpu_render.h:33, gpu_render.cu:262-265): *available = 1 if a CUDA
+ * device is present and usable, else 0. */
+int aniso_b200_available(int32_t* available);
+
+/* GpuRenderer::GpuRenderer(const Scene&) (gpu_render.h:24, gpu_render.cu:267-292).
+ * gaussians: n x 11 floats, the memory of std::vector<aniso::Gaussian> (gaussian.h:21-26):
+ *            position x y z, scale x y z, rotation w x y z, opacity -- already activated.
+ * sh:        n x (sh_degree+1)^2 x 3 floats, [coefficient][channel] (Scene::sh, gaussian.h:33-35).
+ * The scene is copied to the device; the caller's arrays are not retained. */
+int aniso_b200_scene_create(const float* gaussians, const float* sh, int64_t n, int32_t sh_degree,
+                            aniso_b200_scene** out);
+
+/* The raw (optimizer) form a 3DGS PLY stores, activated on the device as the reference loader
+ * does on the host (ply_loader.cpp:124-138): xyz n x 3, f_dc n x 3, f_rest n x 3((d+1)^2-1)
+ * channel-major, opacity logit n, log-scale n x 3, rot n x 4 (w first). Host pointers. */
+int aniso_b200_scene_create_raw(const float* xyz, const float* f_dc, const float* f_rest, const float* opacity,
+                                const float* log_scale, const float* rot, int64_t n, int32_t sh_degree,
+                                aniso_b200_scene** out);
+
+/* ~GpuRenderer (gpu_render.cu:294-297). Accepts NULL. */
+int aniso_b200_scene_destroy(aniso_b200_scene* scene);
+
+/* GpuRenderer::render(const Camera&, RenderStats*, const RenderOptions&) (gpu_render.h:30,
+ * gpu_render.cu:299-375): renders into a HOST buffer of width*height*3 bytes (RGB8, rows top to
+ * bottom, image.h:10-17) and returns when it is written. options and stats may be NULL
+ * (defaults: degree 3, scale 1). */
+int aniso_b200_render(aniso_b200_scene* scene, const aniso_b200_camera* camera, const aniso_b200_options* options,
+                      uint8_t* rgb_host, aniso_b200_stats* stats);
+
+/* The same render, stream-ordered, into a DEVICE buffer: enqueues the kernels on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) and returns without waiting. The pair
+ * buffers must already be large enough (a previous render of a similar view sizes them); a frame
+ * that needed more sets the overflow status that aniso_b200_sync() reports, and should be
+ * rendered again. */
+int aniso_b200_render_device(aniso_b200_scene* scene, const aniso_b200_camera* camera,
+                             const aniso_b200_options* options, uint8_t* rgb_device, void* stream);
+
+/* Waits for the scene's enqueued work; reports the last frame's counts (stats may be NULL) and
+ * returns ANISO_B200_ERR_ARGUMENT with message "pair capacity exceeded" if any frame since the
+ * previous sync overflowed (the capacity has then been grown for the next render). */
+int aniso_b200_sync(aniso_b200_scene* scene, aniso_b200_stats* stats);
+
+/* Copies the last error message (NUL-terminated, truncated to len) and returns its full length. */
+size_t aniso_b200_last_error(char* buf, size_t len);
+
+/* ---- introspection used by the parity tests (no counterpart in gpu_render.h) ---------------- */
+
+/* Runs the projection only and copies, per Gaussian, what the reference preprocess kernel
+ * writes (gpu_render.cu:86-88): uv n x 2, conic_opacity n x 4, depth n, rgb n x 3, rect n x 4
+ * (uint32 x0 y0 x1 y1), tiles_touched n (0 = culled). Any output may be NULL. */
+int aniso_b200_debug_projection(aniso_b200_scene* scene, const aniso_b200_camera* camera,
+                                const aniso_b200_options* options, float* uv, float* conic_opacity, float* depth,
+                                float* rgb, uint32_t* rect, uint32_t* tiles_touched);
+
+/* Runs projection and sort and copies the sorted pair list: tile ids and Gaussian indices
+ * (capacity entries at most) and ranges (tiles_x*tiles_y x 2). *pairs receives the count; returns
+ * ANISO_B200_ERR_ARGUMENT if capacity is too small. The reference's 64-bit key of pair k is
+ * (tile[k] << 32) | bits(depth[value[k]]). */
+int aniso_b200_debug_sorted(aniso_b200_scene* scene, const aniso_b200_camera* camera,
+                            const aniso_b200_options* options, uint32_t* tiles, uint32_t* values, uint64_t capacity,
+                            uint32_t* ranges, uint64_t* pairs);
+
+/* The sort alone on a projection computed elsewhere (host arrays in the reference kernel's
+ * layout: tiles_touched n, rect n x 4, depth n), for tiles_x x tiles_y tiles: the same outputs
+ * as aniso_b200_debug_sorted. Needs no scene. */
+int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const uint32_t* rect, const float* depth,
+                               int32_t tiles_x, int32_t tiles_y, uint32_t* tiles, uint32_t* values,
+                               uint64_t capacity, uint32_t* ranges, uint64_t* pairs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ANISO_B200_H */

@@ -1,0 +1,269 @@
+"""ORACLE -- test infrastructure, not product code.
+
+Python handles on the checkers that oracle/Makefile builds:
+
+* :class:`Restatement` -- ``_build/libaniso_oracle.so``, the C restatement (aniso_oracle.c) of the
+  reference CPU renderer and of the GPU path's integer work (keys, stable sort, tile ranges).
+* :class:`ReferenceCPU` -- ``_ref/libaniso_ref_cpu.so``, the reference's own CPU renderer,
+  loader and SH code compiled from its sources (render.cpp, sh.cpp, camera.cpp, ply_loader.cpp).
+* :class:`ReferenceGPU` -- ``_ref/libaniso_ref_gpu.so`` (no fast-math: the bit-exact key/range
+  oracle) or ``_ref/libaniso_ref_gpu_fast.so`` (as shipped): the reference's own CUDA kernels.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline / reference legs import this
+package, and only as the checker or the timed CPU baseline, never as the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATEMENT_SO = os.path.join(HERE, "_build", "libaniso_oracle.so")
+REF_CPU_SO = os.path.join(HERE, "_ref", "libaniso_ref_cpu.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libaniso_ref_gpu.so")
+REF_GPU_FAST_SO = os.path.join(HERE, "_ref", "libaniso_ref_gpu_fast.so")
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_I = ctypes.c_int
+_F = ctypes.c_float
+_U64 = ctypes.c_uint64
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(_P)
+
+
+def _cam(cam) -> np.ndarray:
+    return np.ascontiguousarray(cam.packed(), dtype=np.float64)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Restatement:
+    """The C restatement of the reference path (always buildable: it needs no reference files)."""
+
+    def __init__(self, path: str = RESTATEMENT_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path + " is missing: run `make -C oracle restatement`")
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.orc_activate.argtypes = [_I64, _P, _P, _P, _P, _P, _P, _I, _P, _P]
+        L.orc_sh_color.argtypes = [_P, _I, _F, _F, _F, _I, _P]
+        L.orc_camera_centre.argtypes = [_P, _P]
+        L.orc_make_splats.argtypes = [_I64, _P, _P, _I, _P, _I, _I, _I, _F, _P, _P, _P]
+        L.orc_render.argtypes = [_I64, _P, _P, _I, _P, _I, _I, _I, _F, _P, _P]
+        L.orc_render.restype = _I
+        L.orc_sort_keys.argtypes = [_I64, _P, _P, _P, _I, _I, _P, _P, _I64, _P]
+        L.orc_sort_keys.restype = _I64
+
+    def activate(self, raw):
+        n = raw.n
+        deg = raw.sh_degree
+        k = (deg + 1) ** 2
+        gauss = np.empty((n, 11), np.float32)
+        sh = np.empty((n, k * 3), np.float32)
+        xyz, dc, rest = _f32(raw.xyz), _f32(raw.f_dc), _f32(raw.f_rest)
+        op, sc, rot = _f32(raw.opacity), _f32(raw.scale), _f32(raw.rot)
+        self.lib.orc_activate(n, _ptr(xyz), _ptr(dc), _ptr(rest), _ptr(op), _ptr(sc), _ptr(rot), deg,
+                              _ptr(gauss), _ptr(sh))
+        return gauss, sh
+
+    def sh_color(self, sh, scene_degree, d, degree):
+        sh = _f32(sh)
+        out = np.empty(3, np.float32)
+        self.lib.orc_sh_color(_ptr(sh), scene_degree, float(d[0]), float(d[1]), float(d[2]), degree, _ptr(out))
+        return out
+
+    def camera_centre(self, cam):
+        c = _cam(cam)
+        out = np.empty(3, np.float32)
+        self.lib.orc_camera_centre(_ptr(c), _ptr(out))
+        return out
+
+    def make_splats(self, gauss, sh, scene_degree, cam, sh_degree=3, splat_scale=1.0):
+        gauss, sh = _f32(gauss), _f32(sh)
+        n = gauss.shape[0]
+        out = np.zeros((n, 10), np.float32)
+        radius = np.zeros(n, np.int32)
+        alive = np.zeros(n, np.uint8)
+        c = _cam(cam)
+        self.lib.orc_make_splats(n, _ptr(gauss), _ptr(sh), scene_degree, _ptr(c), cam.width, cam.height,
+                                 sh_degree, splat_scale, _ptr(out), _ptr(radius), _ptr(alive))
+        return out, radius, alive.astype(bool)
+
+    def render(self, gauss, sh, scene_degree, cam, sh_degree=3, splat_scale=1.0):
+        gauss, sh = _f32(gauss), _f32(sh)
+        img = np.zeros((cam.height, cam.width, 3), np.uint8)
+        stats = np.zeros(2, np.int64)
+        c = _cam(cam)
+        rc = self.lib.orc_render(gauss.shape[0], _ptr(gauss), _ptr(sh), scene_degree, _ptr(c), cam.width,
+                                 cam.height, sh_degree, splat_scale, _ptr(img), _ptr(stats))
+        if rc != 0:
+            raise MemoryError("orc_render failed")
+        return img, {"visible": int(stats[0]), "tile_pairs": int(stats[1])}
+
+    def sort_keys(self, tiles_touched, rect, depth, tiles_x, tiles_y):
+        """(keys u64[P], values u32[P], ranges u32[T, 2]) as the reference GPU path produces."""
+        tt = np.ascontiguousarray(tiles_touched, np.uint32)
+        rc = np.ascontiguousarray(rect, np.uint32).reshape(-1, 4)
+        dp = _f32(depth)
+        total = int(tt.astype(np.int64).sum())
+        keys = np.zeros(max(total, 1), np.uint64)
+        values = np.zeros(max(total, 1), np.uint32)
+        ranges = np.zeros((tiles_x * tiles_y, 2), np.uint32)
+        got = self.lib.orc_sort_keys(tt.shape[0], _ptr(tt), _ptr(rc), _ptr(dp), tiles_x, tiles_y, _ptr(keys),
+                                     _ptr(values), keys.shape[0], _ptr(ranges))
+        assert got == total
+        return keys[:total], values[:total], ranges
+
+
+class ReferenceCPU:
+    """The reference CPU renderer, loader and SH code, compiled from the reference's sources."""
+
+    def __init__(self, path: str = REF_CPU_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.ref_cpu_last_error.restype = ctypes.c_char_p
+        L.ref_cpu_render.argtypes = [_P, _P, _I64, _I, _P, _I, _I, _I, _F, _P, _P]
+        L.ref_cpu_make_splats.argtypes = [_P, _P, _I64, _I, _P, _I, _I, _I, _F, _P, _P, _P]
+        L.ref_cpu_sh_color.argtypes = [_P, _I, _F, _F, _F, _I, _P]
+        L.ref_cpu_load_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(_I64), ctypes.POINTER(_I), _P, _P]
+        L.ref_cpu_load_colmap.argtypes = [ctypes.c_char_p, ctypes.POINTER(_I), _P]
+        L.ref_cpu_camera_centre.argtypes = [_P, _P]
+
+    @staticmethod
+    def available(path: str = REF_CPU_SO) -> bool:
+        return os.path.exists(path)
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.ref_cpu_last_error().decode())
+
+    def render(self, gauss, sh, scene_degree, cam, sh_degree=3, splat_scale=1.0):
+        gauss, sh = _f32(gauss), _f32(sh)
+        img = np.zeros((cam.height, cam.width, 3), np.uint8)
+        stats = np.zeros(5, np.float64)
+        c = _cam(cam)
+        self._check(self.lib.ref_cpu_render(_ptr(gauss), _ptr(sh), gauss.shape[0], scene_degree, _ptr(c),
+                                            cam.width, cam.height, sh_degree, splat_scale, _ptr(img), _ptr(stats)))
+        return img, {"visible": int(stats[0]), "tile_pairs": int(stats[1]), "project_ms": stats[2],
+                     "sort_ms": stats[3], "blend_ms": stats[4]}
+
+    def make_splats(self, gauss, sh, scene_degree, cam, sh_degree=3, splat_scale=1.0):
+        gauss, sh = _f32(gauss), _f32(sh)
+        n = gauss.shape[0]
+        out = np.zeros((n, 10), np.float32)
+        radius = np.zeros(n, np.int32)
+        alive = np.zeros(n, np.uint8)
+        c = _cam(cam)
+        self._check(self.lib.ref_cpu_make_splats(_ptr(gauss), _ptr(sh), n, scene_degree, _ptr(c), cam.width,
+                                                 cam.height, sh_degree, splat_scale, _ptr(out), _ptr(radius),
+                                                 _ptr(alive)))
+        return out, radius, alive.astype(bool)
+
+    def sh_color(self, sh, scene_degree, d, degree):
+        sh = _f32(sh)
+        out = np.empty(3, np.float32)
+        self.lib.ref_cpu_sh_color(_ptr(sh), scene_degree, float(d[0]), float(d[1]), float(d[2]), degree, _ptr(out))
+        return out
+
+    def load_ply(self, path):
+        n, deg = _I64(0), _I(0)
+        self._check(self.lib.ref_cpu_load_ply(path.encode(), ctypes.byref(n), ctypes.byref(deg), None, None))
+        gauss = np.zeros((n.value, 11), np.float32)
+        sh = np.zeros((n.value, (deg.value + 1) ** 2 * 3), np.float32)
+        self._check(self.lib.ref_cpu_load_ply(path.encode(), ctypes.byref(n), ctypes.byref(deg), _ptr(gauss),
+                                              _ptr(sh)))
+        return gauss, sh, deg.value
+
+    def load_colmap(self, folder):
+        count = _I(0)
+        self._check(self.lib.ref_cpu_load_colmap(folder.encode(), ctypes.byref(count), None))
+        out = np.zeros((count.value, 20), np.float64)
+        self._check(self.lib.ref_cpu_load_colmap(folder.encode(), ctypes.byref(count), _ptr(out)))
+        return out
+
+    def camera_centre(self, cam):
+        c = _cam(cam)
+        out = np.empty(3, np.float32)
+        self.lib.ref_cpu_camera_centre(_ptr(c), _ptr(out))
+        return out
+
+
+class ReferenceGPU:
+    """The reference's CUDA kernels (gpu_render.cu) driven stage by stage; device pointers are
+    passed as integers (e.g. torch ``tensor.data_ptr()``)."""
+
+    def __init__(self, fast_math: bool = False):
+        path = REF_GPU_FAST_SO if fast_math else REF_GPU_SO
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.refgpu_last_error.restype = ctypes.c_char_p
+        L.refgpu_preprocess.argtypes = [_I, _U64, _U64, _U64, _U64, _U64, _I, _P, _I, _I, _I, _F,
+                                        _U64, _U64, _U64, _U64, _U64, _U64]
+        L.refgpu_sort.argtypes = [_I, _U64, _U64, _U64, _I, _I, _U64, _U64, _U64, _U64, ctypes.POINTER(_U64)]
+        L.refgpu_blend.argtypes = [_U64, _U64, _U64, _U64, _U64, _I, _I, _U64]
+        L.refgpu_renderer_create.argtypes = [_P, _P, _I64, _I]
+        L.refgpu_renderer_create.restype = _P
+        L.refgpu_renderer_render.argtypes = [_P, _P, _I, _I, _I, _F, _P, _P]
+        L.refgpu_renderer_destroy.argtypes = [_P]
+
+    @staticmethod
+    def available(fast_math: bool = False) -> bool:
+        return os.path.exists(REF_GPU_FAST_SO if fast_math else REF_GPU_SO)
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.refgpu_last_error().decode())
+
+    def preprocess(self, n, pos, scale, rot, opacity, sh, scene_degree, cam, sh_degree, splat_scale,
+                   uv, conic_opacity, depth, rgb, rect, tiles_touched):
+        c = _cam(cam)
+        self._check(self.lib.refgpu_preprocess(n, pos, scale, rot, opacity, sh, scene_degree, _ptr(c), cam.width,
+                                               cam.height, sh_degree, splat_scale, uv, conic_opacity, depth, rgb,
+                                               rect, tiles_touched))
+
+    def sort(self, n, tiles_touched, rect, depth, tiles_x, tiles_y, keys_out, values_out, capacity, ranges_out):
+        total = _U64(0)
+        self._check(self.lib.refgpu_sort(n, tiles_touched, rect, depth, tiles_x, tiles_y, keys_out, values_out,
+                                         capacity, ranges_out, ctypes.byref(total)))
+        return int(total.value)
+
+    def blend(self, ranges, values, uv, conic_opacity, rgb, w, h, out):
+        self._check(self.lib.refgpu_blend(ranges, values, uv, conic_opacity, rgb, w, h, out))
+
+    def renderer(self, gauss, sh, degree):
+        gauss, sh = _f32(gauss), _f32(sh)
+        h = self.lib.refgpu_renderer_create(_ptr(gauss), _ptr(sh), gauss.shape[0], degree)
+        if not h:
+            raise RuntimeError(self.lib.refgpu_last_error().decode())
+        return h
+
+    def render(self, handle, cam, sh_degree=3, splat_scale=1.0):
+        img = np.zeros((cam.height, cam.width, 3), np.uint8)
+        stats = np.zeros(5, np.float64)
+        c = _cam(cam)
+        self._check(self.lib.refgpu_renderer_render(handle, _ptr(c), cam.width, cam.height, sh_degree, splat_scale,
+                                                    _ptr(img), _ptr(stats)))
+        return img, {"visible": int(stats[0]), "tile_pairs": int(stats[1]), "project_ms": stats[2],
+                     "sort_ms": stats[3], "blend_ms": stats[4]}
+
+    def destroy(self, handle):
+        self.lib.refgpu_renderer_destroy(handle)
+
+
+def psnr(a: np.ndarray, b: np.ndarray) -> float:
+    """PSNR in dB of two RGB8 images, as tests/test_gpu_render.cpp:28-36 computes it."""
+    d = (a.astype(np.float64) - b.astype(np.float64)) / 255.0
+    mse = float((d * d).mean()) if d.size else 0.0
+    return 1e9 if mse == 0 else 10.0 * np.log10(1.0 / mse)

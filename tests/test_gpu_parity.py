@@ -1,0 +1,265 @@
+"""Parity of the B200 rasterizer with the reference, through the C ABI (needs a GPU).
+
+Bars (north star): images within 2/255 max-abs and at least 75 dB PSNR of the reference CPU
+renderer (render.cpp); tile ranges, sorted keys and values bit-identical to the reference GPU
+path (gpu_render.cu built without fast-math) given the same projection; the projection itself
+bit-identical to the reference preprocess kernel built the same way.
+"""
+import numpy as np
+import pytest
+
+import kat
+import oracle
+from aniso_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+MAX_ABS = 2      # levels of 255
+MIN_PSNR = 75.0  # dB
+
+
+@pytest.fixture(scope="module")
+def ab():
+    import aniso_b200
+
+    assert aniso_b200.GpuRenderer.available(), "no CUDA device"
+    return aniso_b200
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    assert torch.cuda.is_available()
+    return torch
+
+
+def cpu_render(gauss, sh, deg, cam, sh_degree=3, splat_scale=1.0):
+    """The reference CPU renderer where it was built, else the bit-identical restatement."""
+    if oracle.ReferenceCPU.available():
+        return oracle.ReferenceCPU().render(gauss, sh, deg, cam, sh_degree, splat_scale)
+    return oracle.Restatement().render(gauss, sh, deg, cam, sh_degree, splat_scale)
+
+
+def compare(gpu, cpu):
+    d = np.abs(gpu.astype(np.int32) - cpu.astype(np.int32))
+    return int(d.max()) if d.size else 0, oracle.psnr(gpu, cpu)
+
+
+def assert_image_parity(gpu, cpu, what=""):
+    m, p = compare(gpu, cpu)
+    assert m <= MAX_ABS and p >= MIN_PSNR, "%s: max-abs %d/255, PSNR %.1f dB" % (what, m, p)
+    return m, p
+
+
+# ---- the reference's known-answer tests (test_render.cpp:40-73), on the GPU ---------------------
+
+def test_kat_single_gaussian(ab):
+    g, sh, deg = kat.kat_single()
+    cam = kat.kat_camera()
+    img = ab.GpuRenderer(g, sh, deg).render(cam)
+    variance = np.float32(3.2) * np.float32(3.2) + np.float32(0.3)
+    expected = np.float32(0.8) * np.exp(np.float32(-0.5) * np.float32(0.5) / variance) * np.float32(255.0)
+    assert abs(int(img[32, 32, 0]) - int(expected + 0.5)) <= 1
+    assert img[32, 32, 1] == 0 and img[2, 2, 0] == 0
+    assert_image_parity(img, cpu_render(g, sh, deg, cam)[0], "single")
+
+
+def test_kat_front_hides_back(ab):
+    g, sh, deg = kat.kat_front_back()
+    cam = kat.kat_camera()
+    img = ab.GpuRenderer(g, sh, deg).render(cam)
+    assert img[32, 32, 1] > 240 and img[32, 32, 2] < 10
+    assert_image_parity(img, cpu_render(g, sh, deg, cam)[0], "front/back")
+
+
+def test_kat_behind_camera_is_culled(ab):
+    g, sh, deg = kat.kat_behind()
+    st = {}
+    img = ab.GpuRenderer(g, sh, deg).render(kat.kat_camera(), st)
+    assert st["visible"] == 0 and st["tile_pairs"] == 0
+    assert not img.any()
+
+
+# ---- test_gpu_render.cpp:62-91, with the tighter bars -------------------------------------------
+
+@pytest.mark.parametrize("w,h", [(320, 240), (333, 217)])
+def test_random_cloud_vs_cpu(ab, w, h):
+    g, sh, deg = kat.random_cloud(20000)
+    cam = kat.gpu_test_camera(w, h)
+    st = {}
+    img = ab.GpuRenderer(g, sh, deg).render(cam, st)
+    cpu, cst = cpu_render(g, sh, deg, cam)
+    assert st["visible"] == cst["visible"]
+    assert_image_parity(img, cpu, "%dx%d" % (w, h))
+
+
+def test_degree0_and_empty_view(ab):
+    g, sh, deg = kat.random_cloud(20000)
+    r = ab.GpuRenderer(g, sh, deg)
+    cam = kat.gpu_test_camera(320, 240)
+    opt = ab.RenderOptions(sh_degree=0)
+    assert_image_parity(r.render(cam, options=opt), cpu_render(g, sh, deg, cam, sh_degree=0)[0], "degree 0")
+    behind = scenes.Camera(320, 240, cam.fx, cam.fy, cam.cx, cam.cy, np.diag([-1.0, 1.0, -1.0]), np.zeros(3))
+    st = {}
+    black = r.render(behind, st)
+    assert not black.any() and st["tile_pairs"] == 0
+
+
+def test_splat_scale_and_degrees(ab):
+    g, sh, deg = kat.random_cloud(5000, seed=11)
+    r = ab.GpuRenderer(g, sh, deg)
+    cam = kat.gpu_test_camera(256, 192)
+    for d, s in [(1, 1.0), (2, 0.5), (3, 1.7)]:
+        img = r.render(cam, options=ab.RenderOptions(sh_degree=d, splat_scale=s))
+        assert_image_parity(img, cpu_render(g, sh, deg, cam, d, s)[0], "degree %d scale %g" % (d, s))
+
+
+# ---- bit-exact projection and sort vs the reference GPU kernels (no fast-math) -------------------
+
+def reference_projection(torch, g, sh, deg, cam, sh_degree=3, splat_scale=1.0):
+    """Runs the reference preprocess kernel (gpu_render.cu:86-145) on the same activated scene."""
+    ref = oracle.ReferenceGPU(fast_math=False)
+    n = g.shape[0]
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    pos, scale = dev(g[:, 0:3]), dev(g[:, 3:6])
+    rot, op, shd = dev(g[:, 6:10]), dev(g[:, 10]), dev(sh)
+    out = {"uv": torch.zeros(n, 2, device="cuda"), "conic_opacity": torch.zeros(n, 4, device="cuda"),
+           "depth": torch.zeros(n, device="cuda"), "rgb": torch.zeros(n, 3, device="cuda"),
+           "rect": torch.zeros(n, 4, dtype=torch.int32, device="cuda"),
+           "tiles_touched": torch.zeros(n, dtype=torch.int32, device="cuda")}
+    ref.preprocess(n, pos.data_ptr(), scale.data_ptr(), rot.data_ptr(), op.data_ptr(), shd.data_ptr(), deg, cam,
+                   sh_degree, splat_scale, out["uv"].data_ptr(), out["conic_opacity"].data_ptr(),
+                   out["depth"].data_ptr(), out["rgb"].data_ptr(), out["rect"].data_ptr(),
+                   out["tiles_touched"].data_ptr())
+    res = {k: v.cpu().numpy() for k, v in out.items()}
+    res["rect"] = res["rect"].view(np.uint32)
+    res["tiles_touched"] = res["tiles_touched"].view(np.uint32)
+    return res
+
+
+def reference_sort(torch, proj, tiles_x, tiles_y):
+    """Runs the reference's scan, duplicate, CUB sort and tileRanges (gpu_render.cu:324-345)."""
+    ref = oracle.ReferenceGPU(fast_math=False)
+    n = proj["depth"].shape[0]
+    total = int(proj["tiles_touched"].astype(np.int64).sum())
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    tt = dev(proj["tiles_touched"].view(np.int32))
+    rect = dev(proj["rect"].view(np.int32))
+    depth = dev(proj["depth"])
+    keys = torch.zeros(max(total, 1), dtype=torch.int64, device="cuda")
+    values = torch.zeros(max(total, 1), dtype=torch.int32, device="cuda")
+    ranges = torch.zeros(tiles_x * tiles_y, 2, dtype=torch.int32, device="cuda")
+    got = ref.sort(n, tt.data_ptr(), rect.data_ptr(), depth.data_ptr(), tiles_x, tiles_y, keys.data_ptr(),
+                   values.data_ptr(), max(total, 1), ranges.data_ptr())
+    assert got == total
+    return (keys.cpu().numpy().view(np.uint64)[:total], values.cpu().numpy().view(np.uint32)[:total],
+            ranges.cpu().numpy().view(np.uint32))
+
+
+PROJ_CASES = {
+    "cloud20k": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(333, 217)),
+    "config1": lambda: ((lambda s: oracle.Restatement().activate(s) + (3,))(scenes.config(1)[0][0]),
+                        scenes.config(1)[1][0][0]),
+}
+
+
+@pytest.mark.parametrize("case", sorted(PROJ_CASES))
+def test_projection_bit_exact_vs_reference_kernel(ab, torch_cuda, case):
+    if not oracle.ReferenceGPU.available():
+        pytest.skip("reference GPU library not built")
+    (g, sh, deg), cam = PROJ_CASES[case]()
+    mine = ab.GpuRenderer(g, sh, deg).debug_projection(cam)
+    ref = reference_projection(torch_cuda, g, sh, deg, cam)
+    np.testing.assert_array_equal(mine["tiles_touched"], ref["tiles_touched"])
+    vis = ref["tiles_touched"] > 0
+    np.testing.assert_array_equal(mine["rect"][vis], ref["rect"][vis])
+    np.testing.assert_array_equal(mine["depth"][vis].view(np.uint32), ref["depth"][vis].view(np.uint32))
+    np.testing.assert_array_equal(mine["uv"][vis].view(np.uint32), ref["uv"][vis].view(np.uint32))
+    np.testing.assert_array_equal(mine["conic_opacity"][vis].view(np.uint32),
+                                  ref["conic_opacity"][vis].view(np.uint32))
+    np.testing.assert_allclose(mine["rgb"][vis], ref["rgb"][vis], rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("case", sorted(PROJ_CASES))
+def test_sort_bit_exact_given_same_projection(ab, torch_cuda, case):
+    (g, sh, deg), cam = PROJ_CASES[case]()
+    r = ab.GpuRenderer(g, sh, deg)
+    proj = r.debug_projection(cam)
+    tx, ty = (cam.width + 15) // 16, (cam.height + 15) // 16
+    tiles, values, ranges = r.debug_sorted(cam)
+    keys = ab.keys_of(tiles, values, proj["depth"])
+    # the C restatement of the reference's integer work
+    okeys, ovalues, oranges = oracle.Restatement().sort_keys(proj["tiles_touched"], proj["rect"], proj["depth"], tx, ty)
+    np.testing.assert_array_equal(keys, okeys)
+    np.testing.assert_array_equal(values, ovalues)
+    np.testing.assert_array_equal(ranges, oranges)
+    # the product's sort alone on that projection
+    t2, v2, r2 = ab.sort_projection(proj["tiles_touched"], proj["rect"], proj["depth"], tx, ty)
+    np.testing.assert_array_equal(t2, tiles)
+    np.testing.assert_array_equal(v2, values)
+    np.testing.assert_array_equal(r2, ranges)
+    # the reference's own scan + duplicate + CUB sort + tileRanges on that projection
+    if oracle.ReferenceGPU.available():
+        rkeys, rvalues, rranges = reference_sort(torch_cuda, proj, tx, ty)
+        np.testing.assert_array_equal(keys, rkeys)
+        np.testing.assert_array_equal(values, rvalues)
+        np.testing.assert_array_equal(ranges, rranges)
+
+
+# ---- working-size scenes -----------------------------------------------------------------------
+
+@pytest.mark.slow
+def test_config1_vs_cpu(ab):
+    raw = scenes.config(1)[0][0]
+    cam = scenes.config(1)[1][0][0]
+    g, sh = oracle.Restatement().activate(raw)
+    st = {}
+    img = ab.GpuRenderer(g, sh, 3).render(cam, st)
+    cpu, cst = cpu_render(g, sh, 3, cam)
+    assert st["visible"] == cst["visible"] == 60601
+    assert_image_parity(img, cpu, "config 1")
+
+
+@pytest.mark.slow
+def test_config2_views_vs_cpu(ab):
+    scs, cams = scenes.config(2)
+    g, sh = oracle.Restatement().activate(scs[0])
+    r = ab.GpuRenderer(g, sh, 3)
+    for cam in cams[0][:16:5]:
+        img = r.render(cam)
+        cpu, _ = cpu_render(g, sh, 3, cam)
+        assert_image_parity(img, cpu, cam.name)
+
+
+def test_pair_overflow_regrows(ab):
+    """A frame with more pairs than the initial capacity (2^20) is rendered again after growing."""
+    rng = np.random.default_rng(5)
+    n = 400
+    g = np.zeros((n, 11), np.float32)
+    g[:, 0:2] = rng.uniform(-0.5, 0.5, (n, 2))
+    g[:, 2] = rng.uniform(3, 4, n)
+    g[:, 3:6] = 1.5  # huge: each covers the whole 1920x1080 frame (8160 tiles)
+    g[:, 6] = 1
+    g[:, 10] = 0.02
+    sh = rng.normal(0, 0.5, (n, 3)).astype(np.float32)
+    cam = scenes.Camera(1920, 1080, 1000.0, 1000.0, 960.0, 540.0, np.eye(3), np.zeros(3))
+    st = {}
+    img = ab.GpuRenderer(g, sh, 0).render(cam, st)
+    assert st["tile_pairs"] > (1 << 20)
+    assert_image_parity(img, cpu_render(g, sh, 0, cam)[0], "overflow")
+
+
+def test_render_device_stream_ordered(ab, torch_cuda):
+    torch = torch_cuda
+    g, sh, deg = kat.random_cloud(20000)
+    r = ab.GpuRenderer(g, sh, deg)
+    cams = [kat.gpu_test_camera(320, 240), kat.gpu_test_camera(333, 217)]
+    host = [r.render(c) for c in cams]
+    stream = torch.cuda.Stream()
+    outs = [torch.empty(c.height, c.width, 3, dtype=torch.uint8, device="cuda") for c in cams]
+    for c, o in zip(cams, outs):
+        r.render_device(c, o.data_ptr(), stream.cuda_stream)
+    r.sync()
+    for h, o in zip(host, outs):
+        np.testing.assert_array_equal(o.cpu().numpy(), h)
