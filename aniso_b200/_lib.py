@@ -31,6 +31,8 @@ EXPORTS = [
     "aniso_b200_debug_projection",
     "aniso_b200_debug_sorted",
     "aniso_b200_sort_projection",
+    "aniso_b200_profile",
+    "aniso_b200_profile_read",
 ]
 
 
@@ -57,7 +59,7 @@ class AnisoError(RuntimeError):
 
 def _load():
     if not os.path.exists(LIB_PATH):
-        raise ImportError("%s is missing: build it with `python -m aniso_b200.build`" % LIB_PATH)
+        raise ImportError("%s is missing: build it with `python aniso_b200/build.py`" % LIB_PATH)
     lib = ctypes.CDLL(LIB_PATH)
     P = ctypes.c_void_p
     I64, I32, U64 = ctypes.c_int64, ctypes.c_int32, ctypes.c_uint64
@@ -73,6 +75,9 @@ def _load():
         "aniso_b200_debug_sorted": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, P, U64, P,
                                     ctypes.POINTER(U64)],
         "aniso_b200_sort_projection": [I64, P, P, P, I32, I32, P, P, U64, P, ctypes.POINTER(U64)],
+        "aniso_b200_profile": [P, I32],
+        "aniso_b200_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(I64)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

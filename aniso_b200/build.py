@@ -1,7 +1,7 @@
 """Builds the in-tree CUDA library aniso_b200/libaniso_b200.so for sm_100a (B200) only.
 
-    python -m aniso_b200.build            # incremental
-    python -m aniso_b200.build --force    # rebuild everything
+    python aniso_b200/build.py            # incremental (runs without importing the package)
+    python aniso_b200/build.py --force    # rebuild everything
 
 Each csrc/*.cu file is compiled separately (in parallel) with -O3, IEEE division and square root
 (no --use_fast_math: the projection must round like the reference kernel built without it),

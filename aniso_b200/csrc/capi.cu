@@ -178,6 +178,10 @@ struct aniso_b200_scene {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     Ctrl* host_ctrl = nullptr;  // pinned
+    // Stage events of profiled render_device frames: 4 per frame, reused after each read.
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_ev;
+    size_t prof_frames = 0;
 
     SceneView view() const {
         SceneView v;
@@ -193,6 +197,7 @@ struct aniso_b200_scene {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto& e : prof_ev) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
         if (host_ctrl) cudaFreeHost(host_ctrl);
     }
@@ -250,8 +255,10 @@ __global__ void ingest_raw_kernel(const float* __restrict__ xyz, const float* __
     }
 }
 
+// Scenes may store up to degree 4 (the degrees the reference loader accepts, ply_loader.cpp:67-73);
+// colour is evaluated up to degree 3, as both reference renderers do.
 int validate_degree(int d) {
-    if (d < 0 || d > 3) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be 0..3");
+    if (d < 0 || d > 4) return fail(ANISO_B200_ERR_ARGUMENT, "scene sh_degree must be 0..4");
     return 0;
 }
 
@@ -311,29 +318,30 @@ int pack_camera(const aniso_b200_scene* s, const aniso_b200_camera* c, const ani
     cp.height = c->height;
     cp.tilesX = (c->width + kTile - 1) / kTile;
     cp.tilesY = (c->height + kTile - 1) / kTile;
-    cp.shDegree = std::min(opt_degree, s->degree);
+    cp.shDegree = std::min(std::min(opt_degree, s->degree), 3);
     cp.shCoeffs = (s->degree + 1) * (s->degree + 1);
     cp.splatScale = o ? o->splat_scale : 1.0f;
     return 0;
 }
 
-// Enqueues one frame. With stop_after_sort, the blend is skipped (introspection).
-int enqueue_frame(aniso_b200_scene* s, const CamParams& cam, const BlendOut& out, cudaStream_t st, bool timed,
+// Enqueues one frame; ev (4 events, may be NULL) brackets the stages. With stop_after_sort, the
+// blend is skipped (introspection).
+int enqueue_frame(aniso_b200_scene* s, const CamParams& cam, const BlendOut& out, cudaStream_t st, cudaEvent_t* ev,
                   const DebugProjection* dbg, bool stop_after_sort, int* final_buf) {
     Arena& A = s->arena;
     AB_TRY(A.tick(st));
-    if (timed) AB_CUDA(cudaEventRecord(s->ev[0], st));
+    if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
     launch_frame_begin(A.ctrl.p, st);
     launch_preprocess(s->view(), cam, A.ctrl.p, A.rec.p, A.rect16.p, A.vis_key[0].p, A.vis_idx[0].p, A.st_pre.p, dbg,
                       st);
-    if (timed) AB_CUDA(cudaEventRecord(s->ev[1], st));
+    if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
     int fin = 0;
     AB_TRY(enqueue_sort(A, cam.tilesX, cam.tilesY, st, &fin));
-    if (timed) AB_CUDA(cudaEventRecord(s->ev[2], st));
+    if (ev) AB_CUDA(cudaEventRecord(ev[2], st));
     if (!stop_after_sort)
         launch_blend(A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, cam.width, cam.height, cam.tilesX, cam.tilesY,
                      out, st);
-    if (timed) AB_CUDA(cudaEventRecord(s->ev[3], st));
+    if (ev) AB_CUDA(cudaEventRecord(ev[3], st));
     AB_CUDA(cudaGetLastError());
     if (final_buf) *final_buf = fin;
     return 0;
@@ -481,7 +489,7 @@ int aniso_b200_render(aniso_b200_scene* s, const aniso_b200_camera* camera, cons
     BlendOut out;
     out.rgb8 = s->arena.image.p;
     for (int attempt = 0; attempt < 3; ++attempt) {
-        AB_TRY(enqueue_frame(s, cam, out, s->stream, stats != nullptr, nullptr, false, nullptr));
+        AB_TRY(enqueue_frame(s, cam, out, s->stream, stats ? s->ev : nullptr, nullptr, false, nullptr));
         AB_CUDA(cudaMemcpyAsync(rgb_host, out.rgb8, bytes, cudaMemcpyDeviceToHost, s->stream));
         AB_TRY(read_ctrl(s, s->stream));
         int again = 0;
@@ -510,7 +518,43 @@ int aniso_b200_render_device(aniso_b200_scene* s, const aniso_b200_camera* camer
     AB_TRY(pack_camera(s, camera, options, cam));
     BlendOut out;
     out.rgb8 = rgb_device;
-    return enqueue_frame(s, cam, out, static_cast<cudaStream_t>(stream), false, nullptr, false, nullptr);
+    cudaEvent_t* ev = nullptr;
+    if (s->profiling) {
+        while (s->prof_ev.size() < 4 * (s->prof_frames + 1)) {
+            cudaEvent_t e;
+            AB_CUDA(cudaEventCreate(&e));
+            s->prof_ev.push_back(e);
+        }
+        ev = &s->prof_ev[4 * s->prof_frames++];
+    }
+    return enqueue_frame(s, cam, out, static_cast<cudaStream_t>(stream), ev, nullptr, false, nullptr);
+}
+
+int aniso_b200_profile(aniso_b200_scene* s, int32_t enable) {
+    if (!s) return fail(ANISO_B200_ERR_ARGUMENT, "scene is NULL");
+    s->profiling = enable != 0;
+    if (s->profiling) s->prof_frames = 0;
+    return ANISO_B200_OK;
+}
+
+int aniso_b200_profile_read(aniso_b200_scene* s, double* project_ms, double* sort_ms, double* blend_ms,
+                            int64_t* frames) {
+    if (!s) return fail(ANISO_B200_ERR_ARGUMENT, "scene is NULL");
+    double t[3] = {0, 0, 0};
+    for (size_t f = 0; f < s->prof_frames; ++f) {
+        const cudaEvent_t* e = &s->prof_ev[4 * f];
+        AB_CUDA(cudaEventSynchronize(e[3]));
+        for (int k = 0; k < 3; ++k) {
+            float ms = 0;
+            AB_CUDA(cudaEventElapsedTime(&ms, e[k], e[k + 1]));
+            t[k] += ms;
+        }
+    }
+    if (project_ms) *project_ms = t[0];
+    if (sort_ms) *sort_ms = t[1];
+    if (blend_ms) *blend_ms = t[2];
+    if (frames) *frames = static_cast<int64_t>(s->prof_frames);
+    return ANISO_B200_OK;
 }
 
 int aniso_b200_sync(aniso_b200_scene* s, aniso_b200_stats* stats) {
@@ -581,7 +625,7 @@ int aniso_b200_debug_sorted(aniso_b200_scene* s, const aniso_b200_camera* camera
     AB_TRY(pack_camera(s, camera, options, cam));
     int fin = 0;
     for (int attempt = 0; attempt < 3; ++attempt) {
-        AB_TRY(enqueue_frame(s, cam, BlendOut{}, s->stream, false, nullptr, true, &fin));
+        AB_TRY(enqueue_frame(s, cam, BlendOut{}, s->stream, nullptr, nullptr, true, &fin));
         AB_TRY(read_ctrl(s, s->stream));
         int again = 0;
         AB_TRY(settle(s, &again));

@@ -119,6 +119,17 @@ class GpuRenderer:
         check(lib.aniso_b200_render_device(self._h, ctypes.byref(c), ctypes.byref(o), ctypes.c_void_p(rgb_device_ptr),
                                            ctypes.c_void_p(stream_ptr)))
 
+    def profile(self, enable: bool = True):
+        """Starts (clearing the totals) or stops per-stage event timing of render_device frames."""
+        check(lib.aniso_b200_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        """Summed stage times (ms) of the profiled render_device frames, and their count."""
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        f = ctypes.c_int64()
+        check(lib.aniso_b200_profile_read(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(f)))
+        return {"project_ms": a.value, "sort_ms": b.value, "blend_ms": c.value, "frames": f.value}
+
     def sync(self) -> dict:
         st = _lib.Stats()
         check(lib.aniso_b200_sync(self._h, ctypes.byref(st)))

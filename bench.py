@@ -1,0 +1,325 @@
+"""Benchmark of the B200 Gaussian-splat rasterizer (one JSON line on rank 0).
+
+Workload: the "plain forward at working size" shape -- a 740,000-Gaussian SH-degree-3 scene
+(seeded synthetic, 20x6x20 box) seen by 16 cameras on a radius-8 ring at 1280x720, f = 1100.
+A step renders the 16 views once. Metric: Gaussians/s forward = 16 * N / step time.
+
+    python bench.py [--steps K] [--warmup W] [--gpus N]          # this library
+    python bench.py --impl reference [--steps K] [--warmup W]    # the reference CPU renderer
+
+`value` is device-timed (CUDA events on the render stream, scene resident in HBM, images
+written to device memory). `e2e` renders the same views through the public C ABI call
+aniso_b200_render (the drop-in for GpuRenderer::render) into pinned host memory, so each view's
+device-to-host image copy is inside the timed region. Under torchrun each rank renders its own
+replica's 16 views (weak scaling, no collective); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "740k-Gaussian SH3 synthetic scene, 16 ring views 1280x720 (forward)"
+METRIC = "Gaussians/s fwd"
+UNIT = "Gaussians/s"
+N_GAUSS = 740_000
+# the reference's published GPU forward on the 0.74M-Gaussian *train* scene at
+# 1280 wide, 2.3 ms/frame on an RTX 5090 (README.md:28) = 741,883 / 2.3 ms.
+PUBLISHED_GAUSSIANS_PER_S = 741_883 / 2.3e-3
+# dram__bytes_read.sum + dram__bytes_write.sum of one blend launch on ring view 0 (ncu, see
+# profiles/); None until captured.
+BLEND_TRAFFIC_BYTES = None
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.rows = []
+        self.gpu = gpu_index
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        deadline = time.time() + 3
+        while not self.rows and time.time() < deadline:
+            time.sleep(0.01)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append((time.time(), [x.strip() for x in line.split(",")]))
+
+    def mark_begin(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
+    def stop(self):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t0, t1 = self.t0 or 0, self.t1 or time.time()
+        inside = [r for t, r in self.rows if t0 - 0.2 <= t <= t1 + 0.2] or [self.rows[-1][1]]
+        sm = [float(r[1]) for r in inside if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in inside if r[2].replace(".", "").isdigit()]
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in inside:
+            for k, nm in enumerate(names[1:], start=5):
+                if len(r) > k and r[k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(inside)}
+
+
+def load_workload():
+    from aniso_b200 import scenes
+
+    scs, cams = scenes.config(2)
+    gauss, sh = scenes.activate(scs[0])
+    return gauss, sh, cams[0]
+
+
+def reference_arm(args, rank):
+    """The reference's own CPU renderer (render.cpp), all host threads, one view per step."""
+    if rank != 0:
+        return
+    import oracle
+
+    gauss, sh, cams = load_workload()
+    if oracle.ReferenceCPU.available():
+        impl, kind = oracle.ReferenceCPU(), "reference"
+    else:
+        impl, kind = oracle.Restatement(), "port"
+    for k in range(args.warmup):
+        impl.render(gauss, sh, 3, cams[k % len(cams)])
+    t = time.perf_counter()
+    for k in range(args.steps):
+        impl.render(gauss, sh, 3, cams[k % len(cams)])
+    dt = time.perf_counter() - t
+    value = args.steps * N_GAUSS / dt
+    cores = os.cpu_count() if kind == "reference" else 1
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
+            "ms_per_frame": 1000 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded generator, 740k SH3)",
+            "config": {"workload": WORKLOAD + "; one ring view per step", "gaussians": N_GAUSS},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": "%d views of the 16 (one per step), reference render.cpp with "
+                                       "std::thread::hardware_concurrency() threads" % args.steps},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_leg(gauss, sh, cams, images):
+    """Reference CPU renderer on a bounded sample (2 views) and the image agreement there."""
+    import oracle
+
+    if oracle.ReferenceCPU.available():
+        impl, kind, cores = oracle.ReferenceCPU(), "reference", os.cpu_count()
+    else:
+        impl, kind, cores = oracle.Restatement(), "port", 1
+    views = [0, 8]
+    impl.render(gauss, sh, 3, cams[views[0]])  # warm-up
+    worst_abs, worst_psnr = 0, float("inf")
+    t = time.perf_counter()
+    refs = [impl.render(gauss, sh, 3, cams[v])[0] for v in views]
+    dt = time.perf_counter() - t
+    for v, ref in zip(views, refs):
+        d = np.abs(images[v].astype(np.int32) - ref.astype(np.int32))
+        worst_abs = max(worst_abs, int(d.max()))
+        worst_psnr = min(worst_psnr, oracle.psnr(images[v], ref))
+    base = {"value": len(views) * N_GAUSS / dt, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": "ring views 0 and 8 of the 16, 1 warm-up, %s" % ("reference render.cpp -O3, "
+                                                                     "hardware_concurrency threads" if kind == "reference"
+                                                                     else "C restatement, 1 thread")}
+    return base, {"max_abs_255": worst_abs, "psnr_db": worst_psnr, "views": views, "vs": "CPU renderer"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from aniso_b200 import GpuRenderer
+
+    gauss, sh, cams = load_workload()
+    r = GpuRenderer(gauss, sh, 3)
+    V = len(cams)
+    H, W = cams[0].height, cams[0].width
+
+    # Warm-up through the host API: sizes the pair buffers for every view, gives per-view counts.
+    images, counts = [], []
+    for cam in cams:
+        st = {}
+        images.append(r.render(cam, st).copy())
+        counts.append(st)
+    pairs_per_step = sum(c["tile_pairs"] for c in counts)
+
+    out = torch.empty(V, H, W, 3, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+
+    def step():
+        for v, cam in enumerate(cams):
+            r.render_device(cam, out[v].data_ptr(), stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    r.sync()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    r.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.mark_begin()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sampler.mark_end()
+    r.profile(False)
+    prof = r.profile_read()
+    r.sync()  # raises if any frame overflowed or a device wait gave up
+    if dist:
+        dist.barrier()
+    sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * V * N_GAUSS / (ms_step / 1000.0)
+
+    # Images written by the timed loop agree with the host-API renders.
+    same = bool(np.array_equal(out.cpu().numpy(), np.stack(images)))
+
+    # End to end through the public C ABI into pinned host memory.
+    pinned = torch.empty(V, H, W, 3, dtype=torch.uint8).pin_memory()
+    host = pinned.numpy()
+    for _ in range(args.warmup):
+        for v, cam in enumerate(cams):
+            r.render(cam, out=host[v])
+    if dist:
+        dist.barrier()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        for v, cam in enumerate(cams):
+            r.render(cam, out=host[v])
+    e2e_s = (time.perf_counter() - t) / args.steps
+    if dist:
+        tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_value = world * V * N_GAUSS / e2e_s
+
+    line = None
+    if rank == 0:
+        frames = max(prof["frames"], 1)
+        blend_ms = prof["blend_ms"] / frames
+        peak, peak_kind = measured_peaks()
+        # Algorithmic bytes of one blend launch (per view): P*4 index + P*36 splat record + W*H*3 out.
+        blend_bytes = pairs_per_step / V * 40 + W * H * 3
+        achieved = blend_bytes / (blend_ms / 1000.0) / 1e9
+        base, acc = cpu_baseline_leg(gauss, sh, cams, images)
+        kernels_per_frame = 11  # frame_begin, preprocess, 4 depth passes, duplicate, 2 tile passes, ranges, blend
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "ms_per_frame": ms_step / V,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / world / PUBLISHED_GAUSSIANS_PER_S,
+            "dtype": "fp32", "data": "synthetic: seeded 3DGS generator (uniform box, log-scale N(-4,0.5), "
+                                     "logit opacity N(0,1.5), SH3), no dataset",
+            "config": {"workload": WORKLOAD, "gaussians": N_GAUSS, "sh_degree": 3, "views_per_step": V,
+                       "resolution": "%dx%d" % (W, H), "tile": "16x16",
+                       "l2": "inputs larger than L2: scene %.0f MB (> 126 MB) re-read from HBM every view"
+                             % (N_GAUSS * 240 / 1e6),
+                       "parallelism": "replicas (views independent; no collective)" if world > 1 else "1 GPU",
+                       "vs_baseline_source": "BASELINE.md: 2.3 ms/frame, 0.74M train scene, RTX 5090"},
+            "stages_ms_per_frame": {k: prof[k] / frames for k in ("project_ms", "sort_ms", "blend_ms")},
+            "pairs_per_frame": pairs_per_step / V,
+            "roofline": {"kernel": "blend", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": BLEND_TRAFFIC_BYTES,
+                         "note": "blend is FP32/MUFU-issue bound, not HBM bound; bytes per launch = P*40 + W*H*3"},
+            "cpu_baseline": base,
+            "accuracy": acc,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": V * 136,
+                    "d2h_bytes_per_step": V * (H * W * 3 + 64),
+                    "path": "aniso_b200_render (GpuRenderer::render drop-in), pinned host output"},
+            "gpu_launches": kernels_per_frame * V * args.steps,
+            "timed_images_match_host_api": same,
+            "clocks": sampler.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -43,7 +43,7 @@ typedef struct aniso_b200_camera {
 
 /* aniso::RenderOptions (include/aniso/render.h:28-33). */
 typedef struct aniso_b200_options {
-    int32_t sh_degree;  /* colour up to this SH degree (0..3), clamped to the scene's */
+    int32_t sh_degree;  /* colour up to this SH degree (>= 0), clamped to the scene's and to 3 */
     float splat_scale;  /* multiplies every Gaussian's scale (1 = unchanged) */
 } aniso_b200_options;
 
@@ -63,7 +63,8 @@ int aniso_b200_available(int32_t* available);
 /* GpuRenderer::GpuRenderer(const Scene&) (gpu_render.h:24, gpu_render.cu:267-292).
  * gaussians: n x 11 floats, the memory of std::vector<aniso::Gaussian> (gaussian.h:21-26):
  *            position x y z, scale x y z, rotation w x y z, opacity -- already activated.
- * sh:        n x (sh_degree+1)^2 x 3 floats, [coefficient][channel] (Scene::sh, gaussian.h:33-35).
+ * sh:        n x (sh_degree+1)^2 x 3 floats, [coefficient][channel] (Scene::sh, gaussian.h:33-35);
+ *            sh_degree 0..4 (colour is evaluated up to degree 3).
  * The scene is copied to the device; the caller's arrays are not retained. */
 int aniso_b200_scene_create(const float* gaussians, const float* sh, int64_t n, int32_t sh_degree,
                             aniso_b200_scene** out);
@@ -97,6 +98,15 @@ int aniso_b200_render_device(aniso_b200_scene* scene, const aniso_b200_camera* c
  * returns ANISO_B200_ERR_ARGUMENT with message "pair capacity exceeded" if any frame since the
  * previous sync overflowed (the capacity has then been grown for the next render). */
 int aniso_b200_sync(aniso_b200_scene* scene, aniso_b200_stats* stats);
+
+/* Per-stage device timing of aniso_b200_render_device frames (no counterpart in gpu_render.h;
+ * GpuRenderer times only its synchronous render, gpu_render.cu:318-373). enable = 1 clears the
+ * totals and records CUDA events around each stage of every later frame on its own stream;
+ * enable = 0 stops. aniso_b200_profile_read waits for the scene's work and returns the summed
+ * stage times in ms and the number of frames they cover. */
+int aniso_b200_profile(aniso_b200_scene* scene, int32_t enable);
+int aniso_b200_profile_read(aniso_b200_scene* scene, double* project_ms, double* sort_ms, double* blend_ms,
+                            int64_t* frames);
 
 /* Copies the last error message (NUL-terminated, truncated to len) and returns its full length. */
 size_t aniso_b200_last_error(char* buf, size_t len);
