@@ -1,4 +1,4 @@
-// Step 5 of the rasterizer: front-to-back blending, one 256-thread block per 16x16 tile.
+// Step 5 of the rasterizer: front-to-back blending, one 128-thread block per 16x16 tile.
 //
 // Per pixel this is the blend of render.cpp:195-220 / gpu_render.cu:180-233:
 //   power = -(A dx^2 + C dy^2)/2 - B dx dy; skip if power > 0
@@ -6,114 +6,156 @@
 //   stop (without applying) once T (1 - alpha) < 1e-4; else C += rgb alpha T, T *= 1 - alpha
 // evaluated in base 2 on the pre-scaled conic of the SplatRecord (one MUFU ex2 per evaluation).
 //
-// B200 mapping:
-//   * each warp owns an 8x4 pixel block (lane -> pixel), so a tile is 2 x 4 warp blocks and every
-//     warp block lies inside one 8x8 tile of the CPU renderer;
-//   * the block stages 256 splat records per round in shared memory and, per splat, builds an
-//     8-bit mask of the warp blocks it can touch: its pixel bounds (the CPU 8x8-tile rectangle cut
-//     by the ellipse where alpha can reach 1/255) against each warp block. The 8x8 part makes every
-//     pixel see exactly the splat list the CPU renderer gives it; the ellipse part only drops splats
-//     that cannot pass the alpha test anywhere in the warp block, so it changes no result;
-//   * each warp walks only its set bits (ballot + ffs), exits as soon as all 32 pixels are opaque,
-//     and the block stops loading once all 256 pixels are done (__syncthreads_count).
+// B200 mapping (the kernel is FP32-issue bound, so the layout minimises instructions per pixel):
+//   * each warp owns one 8x8 pixel block -- exactly one tile of the CPU renderer -- with two
+//     horizontally adjacent pixels per lane; the row terms of the exponent (with log2(opacity)
+//     folded in) are shared, so each pixel's exponent is two FMAs;
+//   * the block stages 256 splat records per round in shared memory and, per splat, a 4-bit mask
+//     of the warp blocks it can touch: its pixel bounds (the CPU 8x8-tile rectangle cut by the
+//     ellipse where alpha can reach 1/255, with a margin) against each 8x8 block. The 8x8 part
+//     gives every pixel exactly the splat list of the CPU renderer; the ellipse part only drops
+//     splats that cannot pass the alpha test anywhere in the block, so it changes no result;
+//   * each warp walks only its set bits (ballot + ffs); a finished pixel holds T = 0 (T >= 1e-4
+//     while it is not finished), so no separate flag is carried; the warp leaves once all 64
+//     pixels are finished and the block stops loading once all four warps have (__syncthreads_or).
 #include "common.cuh"
 #include "kernels.h"
 
 namespace ab2 {
 namespace {
 
+constexpr int kThreads = 128;
+constexpr int kBatch = 256;
+
 __device__ __forceinline__ bool overlaps(int lo, int hi, int a, int b) { return lo <= b && hi >= a; }
 
+// One pixel's step for one splat. p is the base-2 exponent including log2(opacity) L, so
+// alpha = min(0.99, 2^p) and the reference's "power > 0" skip is p > L. The new transmittance is
+// T - alpha T (one instruction fewer than T (1 - alpha); it differs only in rounding).
+// In training mode tfin keeps the transmittance after the last applied splat (T itself is zeroed
+// when the pixel finishes) and last the list position one past that splat.
 template <bool kTrain>
-__global__ void __launch_bounds__(256) blend_kernel(const uint2* __restrict__ ranges,
-                                                    const unsigned* __restrict__ vals,
-                                                    const SplatRecord* __restrict__ rec, const Ctrl* ctrl, int width,
-                                                    int height, int tiles_x, BlendOut out) {
-    __shared__ float4 s_r0[256];
-    __shared__ float4 s_r1[256];
-    __shared__ float s_b[256];
-    __shared__ unsigned char s_mask[256];
+__device__ __forceinline__ void blend_px(float p, float L, float r, float g, float b, float& T, float& cr, float& cg,
+                                         float& cb, float& tfin, unsigned& last, unsigned pos) {
+    const float alpha = fminf(0.99f, ex2_approx(p));
+    if (!(p > L) && alpha >= 1.0f / 255.0f) {
+        const float w = alpha * T;
+        const float nt = T - w;
+        if (nt < 1e-4f) {
+            T = 0.f;  // finished (also keeps an already finished pixel finished)
+        } else {
+            cr = fmaf(r, w, cr);
+            cg = fmaf(g, w, cg);
+            cb = fmaf(b, w, cb);
+            T = nt;
+            if (kTrain) {
+                tfin = nt;
+                last = pos;
+            }
+        }
+    }
+}
+
+template <bool kTrain>
+__device__ __forceinline__ void store_px(const BlendOut& out, int x, int y, int width, int height, float tfin, float cr,
+                                         float cg, float cb, unsigned last) {
+    if (x >= width || y >= height) return;
+    const size_t p = static_cast<size_t>(y) * width + x;
+    if (out.rgb8) {
+        uint8_t* o = out.rgb8 + p * 3;
+        o[0] = static_cast<uint8_t>(fminf(fmaxf(cr, 0.f), 1.f) * 255.f + 0.5f);
+        o[1] = static_cast<uint8_t>(fminf(fmaxf(cg, 0.f), 1.f) * 255.f + 0.5f);
+        o[2] = static_cast<uint8_t>(fminf(fmaxf(cb, 0.f), 1.f) * 255.f + 0.5f);
+    }
+    if (kTrain) {
+        out.rgbf[p * 3 + 0] = cr;
+        out.rgbf[p * 3 + 1] = cg;
+        out.rgbf[p * 3 + 2] = cb;
+        out.t_final[p] = tfin;
+        out.n_contrib[p] = last;
+    }
+}
+
+template <bool kTrain>
+__global__ void __launch_bounds__(kThreads) blend_kernel(const uint2* __restrict__ ranges,
+                                                         const unsigned* __restrict__ vals,
+                                                         const SplatRecord* __restrict__ rec, const Ctrl* ctrl,
+                                                         int width, int height, int tiles_x, BlendOut out) {
+    __shared__ float4 s_r0[kBatch];
+    __shared__ float4 s_r1[kBatch];
+    __shared__ float s_b[kBatch];
+    __shared__ unsigned char s_mask[kBatch];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tile = blockIdx.x;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
     const int ox = tx * kTile, oy = ty * kTile;
-    const int pxi = ox + (warp & 1) * 8 + (lane & 7), pyi = oy + (warp >> 1) * 4 + (lane >> 3);
-    const bool inside = pxi < width && pyi < height;
-    const float px = pxi + 0.5f, py = pyi + 0.5f;
+    const int x0 = ox + (warp & 1) * 8 + 2 * (lane & 3), y = oy + (warp >> 1) * 8 + (lane >> 2);
+    const float px0 = x0 + 0.5f, py = y + 0.5f;
     const uint2 range = (ctrl->flags & kFlagOverflow) ? make_uint2(0, 0) : ranges[tile];
 
-    float T = 1.0f, cr = 0.f, cg = 0.f, cb = 0.f;
-    bool done = !inside;
-    unsigned last = range.x;
+    // Pixels outside the image start finished.
+    float T0 = (x0 < width && y < height) ? 1.0f : 0.f;
+    float T1 = (x0 + 1 < width && y < height) ? 1.0f : 0.f;
+    float r0 = 0.f, g0 = 0.f, b0c = 0.f, r1 = 0.f, g1 = 0.f, b1c = 0.f;
+    unsigned last0 = range.x, last1 = range.x;
+    float tf0 = 1.0f, tf1 = 1.0f;
 
-    for (unsigned b0 = range.x; b0 < range.y; b0 += 256) {
-        if (__syncthreads_count(done) == 256) break;
-        const unsigned j = b0 + tid;
-        unsigned m = 0;
-        if (j < range.y) {
-            const SplatRecord r = rec[vals[j]];
-            s_r0[tid] = r.r0;
-            s_r1[tid] = r.r1;
-            s_b[tid] = r.r2.x;
-            const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
-            const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
-            const unsigned cols = (overlaps(xlo, xhi, ox, ox + 7) ? 1u : 0u) | (overlaps(xlo, xhi, ox + 8, ox + 15) ? 2u : 0u);
+    for (unsigned base = range.x; base < range.y; base += kBatch) {
+        if (!__syncthreads_or(T0 + T1 > 0.f)) break;
 #pragma unroll
-            for (int row = 0; row < 4; ++row)
-                if (overlaps(ylo, yhi, oy + 4 * row, oy + 4 * row + 3)) m |= cols << (2 * row);
+        for (int h = 0; h < kBatch / kThreads; ++h) {
+            const int slot = tid + h * kThreads;
+            const unsigned j = base + slot;
+            unsigned m = 0;
+            if (j < range.y) {
+                const SplatRecord r = rec[vals[j]];
+                s_r0[slot] = r.r0;
+                s_r1[slot] = r.r1;
+                s_b[slot] = r.r2.x;
+                const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
+                const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
+                const unsigned cols =
+                    (overlaps(xlo, xhi, ox, ox + 7) ? 1u : 0u) | (overlaps(xlo, xhi, ox + 8, ox + 15) ? 2u : 0u);
+                if (overlaps(ylo, yhi, oy, oy + 7)) m |= cols;
+                if (overlaps(ylo, yhi, oy + 8, oy + 15)) m |= cols << 2;
+            }
+            s_mask[slot] = static_cast<unsigned char>(m);
         }
-        s_mask[tid] = static_cast<unsigned char>(m);
         __syncthreads();
-        const unsigned cnt = min(256u, range.y - b0);
-        bool warp_done = __all_sync(0xFFFFFFFFu, done);
+        const unsigned cnt = min(static_cast<unsigned>(kBatch), range.y - base);
+        bool warp_done = !__any_sync(0xFFFFFFFFu, T0 + T1 > 0.f);
         for (unsigned c = 0; c * 32 < cnt && !warp_done; ++c) {
             const unsigned idx = c * 32 + lane;
             unsigned bits = __ballot_sync(0xFFFFFFFFu, idx < cnt && ((s_mask[idx] >> warp) & 1u));
             while (bits) {
-                const unsigned jj = c * 32 + (__ffs(bits) - 1);
-                bits &= bits - 1;
-                const float4 a = s_r0[jj];
-                const float4 q1 = s_r1[jj];
-                const float dx = px - a.x, dy = py - a.y;
-                const float q = fmaf(dx, fmaf(a.z, dx, a.w * dy), q1.x * dy * dy);
-                const float alpha = fminf(0.99f, ex2_approx(q + q1.y));
-                if (!done && !(q > 0.f) && alpha >= 1.0f / 255.0f) {
-                    const float nt = T * (1.0f - alpha);
-                    if (nt < 1e-4f) {
-                        done = true;
-                    } else {
-                        const float w = alpha * T;
-                        cr = fmaf(q1.z, w, cr);
-                        cg = fmaf(q1.w, w, cg);
-                        cb = fmaf(s_b[jj], w, cb);
-                        T = nt;
-                        if (kTrain) last = b0 + jj + 1;
-                    }
+                // Up to two splats per vote on whether the warp is finished.
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    if (!bits) break;
+                    const unsigned jj = c * 32 + (__ffs(bits) - 1);
+                    bits &= bits - 1;
+                    const float4 a = s_r0[jj];
+                    const float4 k = s_r1[jj];
+                    const float bb = s_b[jj];
+                    const float dx0 = px0 - a.x, dy = py - a.y;
+                    const float t1 = a.w * dy, t3 = fmaf(k.x * dy, dy, k.y);
+                    const float p0 = fmaf(dx0, fmaf(a.z, dx0, t1), t3);
+                    const float dx1 = dx0 + 1.0f;
+                    const float p1 = fmaf(dx1, fmaf(a.z, dx1, t1), t3);
+                    const unsigned pos = base + jj + 1;
+                    blend_px<kTrain>(p0, k.y, k.z, k.w, bb, T0, r0, g0, b0c, tf0, last0, pos);
+                    blend_px<kTrain>(p1, k.y, k.z, k.w, bb, T1, r1, g1, b1c, tf1, last1, pos);
                 }
-                if (__all_sync(0xFFFFFFFFu, done)) {
+                if (!__any_sync(0xFFFFFFFFu, T0 + T1 > 0.f)) {
                     warp_done = true;
                     break;
                 }
             }
         }
     }
-    if (inside) {
-        const size_t p = static_cast<size_t>(pyi) * width + pxi;
-        if (out.rgb8) {
-            uint8_t* o = out.rgb8 + p * 3;
-            o[0] = static_cast<uint8_t>(fminf(fmaxf(cr, 0.f), 1.f) * 255.f + 0.5f);
-            o[1] = static_cast<uint8_t>(fminf(fmaxf(cg, 0.f), 1.f) * 255.f + 0.5f);
-            o[2] = static_cast<uint8_t>(fminf(fmaxf(cb, 0.f), 1.f) * 255.f + 0.5f);
-        }
-        if (kTrain) {
-            out.rgbf[p * 3 + 0] = cr;
-            out.rgbf[p * 3 + 1] = cg;
-            out.rgbf[p * 3 + 2] = cb;
-            out.t_final[p] = T;
-            out.n_contrib[p] = last;
-        }
-    }
+    store_px<kTrain>(out, x0, y, width, height, tf0, r0, g0, b0c, last0);
+    store_px<kTrain>(out, x0 + 1, y, width, height, tf1, r1, g1, b1c, last1);
 }
 
 }  // namespace
@@ -123,9 +165,9 @@ void launch_blend(const uint2* ranges, const unsigned* sorted_vals, const SplatR
     const unsigned blocks = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
     if (blocks == 0) return;
     if (out.rgbf)
-        blend_kernel<true><<<blocks, 256, 0, stream>>>(ranges, sorted_vals, rec, ctrl, width, height, tiles_x, out);
+        blend_kernel<true><<<blocks, kThreads, 0, stream>>>(ranges, sorted_vals, rec, ctrl, width, height, tiles_x, out);
     else
-        blend_kernel<false><<<blocks, 256, 0, stream>>>(ranges, sorted_vals, rec, ctrl, width, height, tiles_x, out);
+        blend_kernel<false><<<blocks, kThreads, 0, stream>>>(ranges, sorted_vals, rec, ctrl, width, height, tiles_x, out);
 }
 
 }  // namespace ab2

@@ -1,8 +1,8 @@
 // The C ABI (include/aniso_b200.h): scene upload, per-frame work buffers, the frame pipeline.
 //
 // A frame is a fixed, host-sync-free sequence of launches on one stream (capturable in a CUDA
-// graph): frame_begin, preprocess (+compaction), 4 depth onesweep passes, duplicate, 1-4 tile
-// onesweep passes, tile ranges, blend. Data-dependent sizes (visible count V, pair count P) stay
+// graph): frame_begin, preprocess (+compaction), 4 depth onesweep passes, pair scan, pair
+// expansion, 1-4 tile onesweep passes, tile ranges, blend. Data-dependent sizes (visible count V, pair count P) stay
 // on the device; grids are sized for capacity and surplus blocks exit at once. The reference
 // instead reads P back mid-frame (gpu_render.cu:329) to size its buffers; here a frame whose P
 // exceeds the pair capacity sets an overflow flag instead of writing, and the host grows the
@@ -87,11 +87,14 @@ struct Arena {
     uint64_t frames = 0;
     DevBuf<SplatRecord> rec;
     DevBuf<unsigned long long> rect16;
+    DevBuf<unsigned> depth_key;
     DevBuf<unsigned> vis_key[2], vis_idx[2];
     DevBuf<unsigned> pair_key[2], pair_val[2];
+    DevBuf<unsigned> offs, chunk_start;
+    DevBuf<unsigned long long> rect_sorted;
     DevBuf<uint2> ranges;
     DevBuf<Ctrl> ctrl;
-    DevBuf<unsigned long long> st_pre, st_depth, st_dup, st_tile;
+    DevBuf<unsigned long long> st_depth, st_dup, st_tile;
     DevBuf<uint8_t> image;
 
     unsigned depth_chunks() const { return chunks_of(static_cast<uint64_t>(std::max<int64_t>(n, 1)), onesweep_chunk_items()); }
@@ -102,14 +105,16 @@ struct Arena {
         const size_t nn = static_cast<size_t>(std::max<int64_t>(count, 1));
         AB_TRY(rec.reserve(nn));
         AB_TRY(rect16.reserve(nn));
+        AB_TRY(depth_key.reserve(nn));
         for (int k = 0; k < 2; ++k) {
             AB_TRY(vis_key[k].reserve(nn));
             AB_TRY(vis_idx[k].reserve(nn));
         }
         AB_TRY(ctrl.reserve(1, true));
-        AB_TRY(st_pre.reserve(chunks_of(nn, 256), true));
         AB_TRY(st_depth.reserve(static_cast<size_t>(kMaxPasses) * depth_chunks() * kRadix, true));
-        AB_TRY(st_dup.reserve(chunks_of(nn, duplicate_chunk_items()), true));
+        AB_TRY(st_dup.reserve(chunks_of(nn, pair_scan_chunk_items()), true));
+        AB_TRY(offs.reserve(nn));
+        AB_TRY(rect_sorted.reserve(nn));
         return grow_pairs(cap);
     }
 
@@ -120,6 +125,7 @@ struct Arena {
             AB_TRY(pair_val[k].reserve(cap));
         }
         pair_cap = cap;
+        AB_TRY(chunk_start.reserve(chunks_of(cap, expand_chunk_pairs()) + 2));
         st_tile.release();
         return st_tile.reserve(static_cast<size_t>(kMaxPasses) * tile_chunks() * kRadix, true);
     }
@@ -127,7 +133,6 @@ struct Arena {
     // Status words carry a 30-bit frame epoch; clear them long before it could wrap.
     int tick(cudaStream_t st) {
         if (++frames % (1ull << 29) == 0) {
-            AB_CUDA(cudaMemsetAsync(st_pre.p, 0, st_pre.cap * sizeof(unsigned long long), st));
             AB_CUDA(cudaMemsetAsync(st_depth.p, 0, st_depth.cap * sizeof(unsigned long long), st));
             AB_CUDA(cudaMemsetAsync(st_dup.p, 0, st_dup.cap * sizeof(unsigned long long), st));
             AB_CUDA(cudaMemsetAsync(st_tile.p, 0, st_tile.cap * sizeof(unsigned long long), st));
@@ -136,26 +141,29 @@ struct Arena {
     }
 };
 
-// Depth passes, duplication, tile passes and ranges, from the compacted visible list in
-// vis_key[0]/vis_idx[0]. Returns the buffer index holding the final sorted pairs.
+// Depth passes (the first one compacts the visible Gaussians out of depth_key), pair scan and
+// expansion, tile passes and ranges. Returns the buffer index holding the final sorted pairs.
 int enqueue_sort(Arena& A, int tiles_x, int tiles_y, cudaStream_t st, int* final_buf) {
     Ctrl* ctrl = A.ctrl.p;
     const unsigned nmax = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
     for (int p = 0; p < kMaxPasses; ++p) {
-        const int src = p & 1, dst = src ^ 1;
-        launch_onesweep(A.vis_key[src].p, A.vis_idx[src].p, p == kMaxPasses - 1 ? nullptr : A.vis_key[dst].p,
-                        A.vis_idx[dst].p, &ctrl->vis_count, nullptr, nmax, p * kRadixBits, &ctrl->depth_hist[p * kRadix],
-                        A.st_depth.p + static_cast<size_t>(p) * A.depth_chunks() * kRadix, &ctrl->chunk_ctr[kCtrDepth0 + p],
-                        ctrl, st);
+        const int src = (p + 1) & 1, dst = p & 1;  // pass 0 reads depth_key and writes buffer 0
+        launch_onesweep(p == 0 ? A.depth_key.p : A.vis_key[src].p, p == 0 ? nullptr : A.vis_idx[src].p,
+                        p == kMaxPasses - 1 ? nullptr : A.vis_key[dst].p, A.vis_idx[dst].p, p == 0 ? nmax : 0u, nmax,
+                        p * kRadixBits, &ctrl->depth_hist[p * kRadix],
+                        A.st_depth.p + static_cast<size_t>(p) * A.depth_chunks() * kRadix,
+                        &ctrl->chunk_ctr[kCtrDepth0 + p], ctrl, st);
     }
+    const int sorted = (kMaxPasses - 1) & 1;
     const unsigned tiles = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
     const int tile_passes = std::max(1, (bits_for(tiles - 1) + kRadixBits - 1) / kRadixBits);
-    launch_duplicate(A.vis_idx[0].p, A.rect16.p, ctrl, A.pair_cap, nmax, tiles_x, tile_passes, A.pair_key[0].p,
-                     A.pair_val[0].p, A.st_dup.p, st);
+    const DupBuffers dup{A.offs.p, A.rect_sorted.p, A.chunk_start.p};
+    launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, nmax, tiles_x, tile_passes, dup,
+                     A.pair_key[0].p, A.pair_val[0].p, A.st_dup.p, st);
     for (int p = 0; p < tile_passes; ++p) {
         const int src = p & 1, dst = src ^ 1;
-        launch_onesweep(A.pair_key[src].p, A.pair_val[src].p, A.pair_key[dst].p, A.pair_val[dst].p, nullptr,
-                        &ctrl->pair_total, A.pair_cap, p * kRadixBits, &ctrl->tile_hist[p * kRadix],
+        launch_onesweep(A.pair_key[src].p, A.pair_val[src].p, A.pair_key[dst].p, A.pair_val[dst].p, 0u, A.pair_cap,
+                        p * kRadixBits, &ctrl->tile_hist[p * kRadix],
                         A.st_tile.p + static_cast<size_t>(p) * A.tile_chunks() * kRadix,
                         &ctrl->chunk_ctr[kCtrTile0 + p], ctrl, st);
     }
@@ -221,7 +229,7 @@ __global__ void ingest_kernel(const float* __restrict__ gauss, const float* __re
         f.y = 4 * p + 1 < k3 ? s[4 * p + 1] : 0.f;
         f.z = 4 * p + 2 < k3 ? s[4 * p + 2] : 0.f;
         f.w = 4 * p + 3 < k3 ? s[4 * p + 3] : 0.f;
-        sh[static_cast<int64_t>(p) * n + i] = f;
+        sh[i * planes + p] = f;
     }
 }
 
@@ -251,7 +259,7 @@ __global__ void ingest_raw_kernel(const float* __restrict__ xyz, const float* __
             const int k = f / 3, c = f % 3;
             v[e] = k == 0 ? f_dc[3 * i + c] : f_rest[i * 3 * rest + c * rest + (k - 1)];
         }
-        sh[static_cast<int64_t>(p) * n + i] = make_float4(v[0], v[1], v[2], v[3]);
+        sh[i * planes + p] = make_float4(v[0], v[1], v[2], v[3]);
     }
 }
 
@@ -332,8 +340,7 @@ int enqueue_frame(aniso_b200_scene* s, const CamParams& cam, const BlendOut& out
     AB_TRY(A.tick(st));
     if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
     launch_frame_begin(A.ctrl.p, st);
-    launch_preprocess(s->view(), cam, A.ctrl.p, A.rec.p, A.rect16.p, A.vis_key[0].p, A.vis_idx[0].p, A.st_pre.p, dbg,
-                      st);
+    launch_preprocess(s->view(), cam, A.ctrl.p, A.rec.p, A.rect16.p, A.depth_key.p, dbg, st);
     if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
     int fin = 0;
     AB_TRY(enqueue_sort(A, cam.tilesX, cam.tilesY, st, &fin));
@@ -604,8 +611,7 @@ int aniso_b200_debug_projection(aniso_b200_scene* s, const aniso_b200_camera* ca
     Arena& A = s->arena;
     AB_TRY(A.tick(s->stream));
     launch_frame_begin(A.ctrl.p, s->stream);
-    launch_preprocess(s->view(), cam, A.ctrl.p, A.rec.p, A.rect16.p, A.vis_key[0].p, A.vis_idx[0].p, A.st_pre.p, &dbg,
-                      s->stream);
+    launch_preprocess(s->view(), cam, A.ctrl.p, A.rec.p, A.rect16.p, A.depth_key.p, &dbg, s->stream);
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaStreamSynchronize(s->stream));
     const size_t n = static_cast<size_t>(s->n);
@@ -672,8 +678,7 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     cudaStream_t st = nullptr;
     AB_TRY(A.tick(st));
     launch_frame_begin(A.ctrl.p, st);
-    launch_compact_projection(n, dtt.p, ddepth.p, drect.p, A.ctrl.p, A.vis_key[0].p, A.vis_idx[0].p, A.rect16.p,
-                              A.st_pre.p, st);
+    launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.ctrl.p, A.depth_key.p, A.rect16.p, st);
     int fin = 0;
     AB_TRY(enqueue_sort(A, tiles_x, tiles_y, st, &fin));
     AB_CUDA(cudaGetLastError());

@@ -4,12 +4,15 @@
 //   pos_op  float4[N]   x, y, z, opacity (activated)
 //   scale   float4[N]   sx, sy, sz, 0     (activated, i.e. exp of the PLY's log-scale)
 //   rot     float4[N]   w, x, y, z        (normalised)
-//   sh      float4[P][N]  P = ceil(3K/4) planes; plane p holds floats 4p..4p+3 of the
-//                         Gaussian's 3K SH floats in [coefficient][channel] order (gaussian.h:33-35)
+//   sh      float4[N][P]  P = ceil(3K/4): the Gaussian's 3K SH floats in [coefficient][channel]
+//                         order (gaussian.h:33-35), padded to 16 bytes. Per Gaussian, not planar:
+//                         only visible Gaussians read their SH, and a planar layout would pull the
+//                         sectors of culled neighbours from DRAM too.
 // Per view:
 //   rec     float4[3][N]  blend record of each visible Gaussian (see SplatRecord)
 //   rect    uint64[N]     16x16-tile rectangle x0 | y0 << 16 | x1 << 32 | y1 << 48
-//   vis_key / vis_idx     compacted visible list: depth bits and Gaussian index, index order
+//   depth_key uint32[N]   float bits of each Gaussian's depth, kCulledKey when culled
+//   vis_key / vis_idx     the visible list being depth-sorted: depth bits and Gaussian index
 //   pair_key / pair_val   one (tile, Gaussian) pair per tile a splat touches
 //   ranges  uint2[tiles]  [start, end) of each tile's run in the sorted pair list
 #pragma once
@@ -42,7 +45,7 @@ struct SceneView {
     const float4* pos_op;
     const float4* scale;
     const float4* rot;
-    const float4* sh;   // planes
+    const float4* sh;   // [n][sh_planes]
     int64_t n;
     int sh_planes;
 };
@@ -60,13 +63,17 @@ struct Ctrl {
     unsigned int tile_hist[kMaxPasses * kRadix];
 };
 
+// Depth key of a culled Gaussian. Visible depths are >= 0.2 (or a canonical NaN), so their float
+// bits never have the sign bit set.
+constexpr unsigned kCulledKey = 0xFFFFFFFFu;
+
 enum : unsigned {
     kFlagOverflow = 1u,  // pairs exceeded the pair capacity: nothing after duplication ran
     kFlagTimeout = 2u,   // a look-back wait hit kSpinLimit (never expected)
 };
 
 // Chunk counter slots.
-enum : int { kCtrPre = 0, kCtrDepth0 = 1, kCtrDup = 5, kCtrTile0 = 6, kCtrCompact = 10 };
+enum : int { kCtrDepth0 = 1, kCtrDup = 5, kCtrTile0 = 6 };
 
 // ---- look-back status words: [epoch:30][flag:2][value:32] ------------------------------------
 enum : unsigned { kStAgg = 1u, kStInc = 2u };

@@ -24,36 +24,43 @@ struct DebugProjection {
 void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
 
 void launch_preprocess(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
-                       unsigned long long* rect16, unsigned* vis_key, unsigned* vis_idx, unsigned long long* status,
-                       const DebugProjection* dbg, cudaStream_t stream);
+                       unsigned long long* rect16, unsigned* depth_key, const DebugProjection* dbg,
+                       cudaStream_t stream);
 
-// One stable onesweep LSD radix pass over (key, value) u32 pairs, 8-bit digit at `shift`.
-// `count` is read on the device; blocks beyond it exit. `hist` holds this digit's global
-// histogram; `status` has max_chunks * 256 words.
+// One stable onesweep LSD radix pass over (key, value) u32 pairs, 8-bit digit at `shift`; `hist` is
+// this digit's global histogram. masked_count > 0: the input is the N depth keys with culled ones
+// dropped and the index as value (the first depth pass); else the histogram total is the item
+// count. Grids are sized for `capacity` items; surplus blocks exit at once.
 int onesweep_items_per_thread();
 unsigned onesweep_chunk_items();
 void launch_onesweep(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
-                     const unsigned* count, const unsigned long long* count64, unsigned capacity, int shift,
-                     const unsigned* hist, unsigned long long* status, unsigned* chunk_ctr, Ctrl* ctrl,
-                     cudaStream_t stream);
+                     unsigned masked_count, unsigned capacity, int shift, const unsigned* hist,
+                     unsigned long long* status, unsigned* chunk_ctr, Ctrl* ctrl, cudaStream_t stream);
 
 // Expands the depth-sorted visible list into (tile, Gaussian) pairs in depth order, building the
-// tile-digit histograms; sets kFlagOverflow (and writes nothing) if the pairs exceed capacity.
-unsigned duplicate_chunk_items();
+// tile-digit histograms; sets kFlagOverflow (and writes no pairs) if they exceed capacity.
+// Two kernels: a pair-offset scan over the V Gaussians, then an expansion with a fixed number of
+// pairs per block.
+struct DupBuffers {
+    unsigned* offs;                   // [N] exclusive pair offset of each depth-sorted Gaussian
+    unsigned long long* rect_sorted;  // [N] its 16x16-tile rectangle, in sorted order
+    unsigned* chunk_start;            // [capacity / expand_chunk_pairs() + 2] first Gaussian per chunk
+};
+unsigned pair_scan_chunk_items();
+unsigned expand_chunk_pairs();
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
-                      unsigned max_visible, int tiles_x, int tile_passes, unsigned* pair_key, unsigned* pair_val,
-                      unsigned long long* status, cudaStream_t stream);
+                      unsigned max_visible, int tiles_x, int tile_passes, const DupBuffers& buf, unsigned* pair_key,
+                      unsigned* pair_val, unsigned long long* status, cudaStream_t stream);
 
 // ranges[tile] = [start, end) over the sorted tile keys (gpu_render.cu:164-177); ranges must be
 // zeroed before.
 void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capacity, uint2* ranges,
                    cudaStream_t stream);
 
-// Compacts an externally given projection (tiles_touched, depth) into the visible list, as the
-// preprocess kernel does, for sorting a projection computed elsewhere.
-void launch_compact_projection(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
-                               Ctrl* ctrl, unsigned* vis_key, unsigned* vis_idx, unsigned long long* rect16,
-                               unsigned long long* status, cudaStream_t stream);
+// Depth keys, rectangles and depth histograms of a projection computed elsewhere (tiles_touched,
+// rect, depth in the reference kernel's layout), as the preprocess kernel writes them.
+void launch_projection_keys(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
+                            Ctrl* ctrl, unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream);
 
 // Blend outputs.
 struct BlendOut {

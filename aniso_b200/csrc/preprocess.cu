@@ -4,10 +4,9 @@
 // order, compiled without fast-math, so depth, rectangle and conic come out bit-identical to the
 // reference kernel built without --use_fast_math), then, fused into the same kernel:
 //   * writes the blend record (SplatRecord) and the 16x16-tile rectangle of visible Gaussians;
-//   * compacts the visible Gaussians, in index order, into (depth bits, index) with a single-pass
-//     decoupled look-back -- the input of the stable depth sort;
-//   * builds the four 8-bit digit histograms of the depth bits for the onesweep passes and sums
-//     the pair count (tiles touched) of the frame.
+//   * writes every Gaussian's depth key (the float bits of its depth; a sentinel if culled) -- the
+//     first onesweep pass of the depth sort compacts the visible ones as it ranks them;
+//   * builds the four 8-bit digit histograms of the depth bits for the onesweep passes.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -146,25 +145,18 @@ __device__ __forceinline__ unsigned axis_bounds(float centre, float cov, float t
 }
 
 template <int D, bool kDebug>
-__global__ void __launch_bounds__(256) preprocess_kernel(SceneView sc, CamParams cam, Ctrl* __restrict__ ctrl,
+__global__ void __launch_bounds__(256, 3) preprocess_kernel(SceneView sc, CamParams cam, Ctrl* __restrict__ ctrl,
                                                          SplatRecord* __restrict__ rec,
                                                          unsigned long long* __restrict__ rect16,
-                                                         unsigned* __restrict__ vis_key,
-                                                         unsigned* __restrict__ vis_idx,
-                                                         unsigned long long* __restrict__ status, DebugProjection dbg) {
-    __shared__ unsigned s_chunk;
-    __shared__ unsigned s_tmp[8];
-    __shared__ unsigned s_base;
+                                                         unsigned* __restrict__ depth_key, DebugProjection dbg) {
     __shared__ unsigned s_hist[kMaxPasses * kRadix];
     const int tid = threadIdx.x;
     for (int k = tid; k < kMaxPasses * kRadix; k += 256) s_hist[k] = 0;
-    if (tid == 0) s_chunk = atomicAdd(&ctrl->chunk_ctr[kCtrPre], 1u);
     __syncthreads();
-    const unsigned chunk = s_chunk;
-    const int64_t i = static_cast<int64_t>(chunk) * 256 + tid;
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * 256 + tid;
 
     bool vis = false;
-    unsigned depth_bits = 0, count = 0;
+    unsigned depth_bits = 0;
     if (i < sc.n) {
         const float4 pg = sc.pos_op[i];
         const float4 sg = sc.scale[i];
@@ -178,7 +170,7 @@ __global__ void __launch_bounds__(256) preprocess_kernel(SceneView sc, CamParams
             float sh[planes * 4];
 #pragma unroll
             for (int k = 0; k < planes; ++k) {
-                const float4 f = sc.sh[static_cast<int64_t>(k) * sc.n + i];
+                const float4 f = sc.sh[i * sc.sh_planes + k];
                 sh[4 * k + 0] = f.x;
                 sh[4 * k + 1] = f.y;
                 sh[4 * k + 2] = f.z;
@@ -206,7 +198,6 @@ __global__ void __launch_bounds__(256) preprocess_kernel(SceneView sc, CamParams
             rect16[i] = static_cast<unsigned long long>(p.x0) | (static_cast<unsigned long long>(p.y0) << 16) |
                         (static_cast<unsigned long long>(p.x1) << 32) | (static_cast<unsigned long long>(p.y1) << 48);
             depth_bits = __float_as_uint(p.depth);
-            count = static_cast<unsigned>((p.x1 - p.x0 + 1) * (p.y1 - p.y0 + 1));
             if (kDebug) {
                 dbg.uv[i] = make_float2(p.u, p.v);
                 dbg.conic_opacity[i] = make_float4(p.conicA, p.conicB, p.conicC, opacity);
@@ -215,7 +206,7 @@ __global__ void __launch_bounds__(256) preprocess_kernel(SceneView sc, CamParams
                 dbg.rgb[3 * i + 1] = rgb.y;
                 dbg.rgb[3 * i + 2] = rgb.z;
                 dbg.rect[i] = make_uint4(p.x0, p.y0, p.x1, p.y1);
-                dbg.tiles_touched[i] = count;
+                dbg.tiles_touched[i] = static_cast<unsigned>((p.x1 - p.x0 + 1) * (p.y1 - p.y0 + 1));
             }
 #pragma unroll
             for (int pass = 0; pass < kMaxPasses; ++pass)
@@ -223,51 +214,37 @@ __global__ void __launch_bounds__(256) preprocess_kernel(SceneView sc, CamParams
         }
     }
 
-    // Stable compaction of the visible Gaussians (index order) with a decoupled look-back.
-    unsigned total = 0;
-    const unsigned local = block_excl_scan<256>(vis ? 1u : 0u, s_tmp, total);
-    unsigned pairs_total = 0;
-    block_excl_scan<256>(count, s_tmp, pairs_total);
-    if (tid < 32) {
-        const unsigned base = lookback_warp(status, chunk, total, ctrl->epoch, &ctrl->flags);
-        if (tid == 0) {
-            s_base = base;
-            if (total) atomicAdd(&ctrl->vis_count, total);
-            if (pairs_total) atomicAdd(&ctrl->pair_total, static_cast<unsigned long long>(pairs_total));
-        }
-    }
+    // The depth key of every Gaussian, kCulledKey for culled ones: visible depths are >= 0.2 (or
+    // the canonical NaN), so the sign bit never collides. The first depth pass compacts the list.
+    if (i < sc.n) depth_key[i] = vis ? depth_bits : kCulledKey;
     __syncthreads();
-    if (vis) {
-        vis_key[s_base + local] = depth_bits;
-        vis_idx[s_base + local] = static_cast<unsigned>(i);
-    }
     for (int k = tid; k < kMaxPasses * kRadix; k += 256)
         if (s_hist[k]) atomicAdd(&ctrl->depth_hist[k], s_hist[k]);
 }
 
 template <bool kDebug>
 void launch_preprocess_t(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
-                         unsigned long long* rect16, unsigned* vis_key, unsigned* vis_idx,
-                         unsigned long long* status, const DebugProjection& dbg, cudaStream_t stream) {
+                         unsigned long long* rect16, unsigned* depth_key, const DebugProjection& dbg,
+                         cudaStream_t stream) {
     const unsigned blocks = static_cast<unsigned>((sc.n + 255) / 256);
     if (blocks == 0) return;
     switch (cam.shDegree) {
-        case 0: preprocess_kernel<0, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, dbg); break;
-        case 1: preprocess_kernel<1, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, dbg); break;
-        case 2: preprocess_kernel<2, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, dbg); break;
-        default: preprocess_kernel<3, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, dbg); break;
+        case 0: preprocess_kernel<0, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
+        case 1: preprocess_kernel<1, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
+        case 2: preprocess_kernel<2, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
+        default: preprocess_kernel<3, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
     }
 }
 
 }  // namespace
 
 void launch_preprocess(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
-                       unsigned long long* rect16, unsigned* vis_key, unsigned* vis_idx, unsigned long long* status,
-                       const DebugProjection* dbg, cudaStream_t stream) {
+                       unsigned long long* rect16, unsigned* depth_key, const DebugProjection* dbg,
+                       cudaStream_t stream) {
     if (dbg)
-        launch_preprocess_t<true>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, *dbg, stream);
+        launch_preprocess_t<true>(sc, cam, ctrl, rec, rect16, depth_key, *dbg, stream);
     else
-        launch_preprocess_t<false>(sc, cam, ctrl, rec, rect16, vis_key, vis_idx, status, DebugProjection{}, stream);
+        launch_preprocess_t<false>(sc, cam, ctrl, rec, rect16, depth_key, DebugProjection{}, stream);
 }
 
 }  // namespace ab2
