@@ -33,6 +33,10 @@ EXPORTS = [
     "aniso_b200_sort_projection",
     "aniso_b200_profile",
     "aniso_b200_profile_read",
+    "aniso_b200_trainer_create",
+    "aniso_b200_trainer_destroy",
+    "aniso_b200_train_forward",
+    "aniso_b200_train_backward",
 ]
 
 
@@ -49,6 +53,17 @@ class Options(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("visible", ctypes.c_uint64), ("tile_pairs", ctypes.c_uint64), ("project_ms", ctypes.c_double),
                 ("sort_ms", ctypes.c_double), ("blend_ms", ctypes.c_double)]
+
+
+class RawParams(ctypes.Structure):
+    _fields_ = [("means", ctypes.c_void_p), ("log_scales", ctypes.c_void_p), ("quats", ctypes.c_void_p),
+                ("opacity_logits", ctypes.c_void_p), ("sh", ctypes.c_void_p), ("n", ctypes.c_int64),
+                ("sh_degree", ctypes.c_int32)]
+
+
+class RawGrads(ctypes.Structure):
+    _fields_ = [("means", ctypes.c_void_p), ("log_scales", ctypes.c_void_p), ("quats", ctypes.c_void_p),
+                ("opacity_logits", ctypes.c_void_p), ("sh", ctypes.c_void_p)]
 
 
 class AnisoError(RuntimeError):
@@ -76,6 +91,11 @@ def _load():
                                     ctypes.POINTER(U64)],
         "aniso_b200_sort_projection": [I64, P, P, P, I32, I32, P, P, U64, P, ctypes.POINTER(U64)],
         "aniso_b200_profile": [P, I32],
+        "aniso_b200_trainer_create": [ctypes.POINTER(P)],
+        "aniso_b200_trainer_destroy": [P],
+        "aniso_b200_train_forward": [P, ctypes.POINTER(RawParams), ctypes.POINTER(Camera), ctypes.POINTER(Options), P,
+                                     P],
+        "aniso_b200_train_backward": [P, P, ctypes.POINTER(RawGrads), P],
         "aniso_b200_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(I64)],
     }

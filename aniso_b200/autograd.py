@@ -1,0 +1,114 @@
+"""The differentiable path: a torch.autograd.Function over the C ABI's training entry points.
+
+    img = rasterize(means, log_scales, quats, opacity_logits, sh, camera, sh_degree=3)
+    loss = ((img - target) ** 2).sum(); loss.backward()
+
+The parameters are the raw optimizer tensors of pipeline/train_gsplat.py:85-92 (means, log-scales,
+quaternions, opacity logits, SH as (n, 16, 3) = sh0 ++ shN), float32 on one CUDA device; the
+activations (exp, sigmoid, normalise) run inside the kernels. The output is the (H, W, 3) float
+colour before the 8-bit rounding (unclamped, black background). The backward is the library's
+hand-written adjoint (deterministic; no atomics).
+
+PyTorch supplies the device memory and the stream; all arithmetic is in libaniso_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import check, lib
+from .renderer import RenderOptions, c_camera
+
+
+class Trainer:
+    """The work buffers of one forward and its backward (a C-ABI aniso_b200_trainer)."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        check(lib.aniso_b200_trainer_create(ctypes.byref(self._h)))
+
+    def close(self):
+        if self._h.value:
+            lib.aniso_b200_trainer_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_pool: list[Trainer] = []
+
+
+def _acquire() -> Trainer:
+    return _pool.pop() if _pool else Trainer()
+
+
+def _release(t: Trainer):
+    _pool.append(t)
+
+
+def _raw_params(means, log_scales, quats, opacity_logits, sh) -> _lib.RawParams:
+    n = means.shape[0]
+    k = sh.shape[1]
+    deg = {4: 1, 16: 3}.get(k)
+    if deg is None:
+        raise ValueError("sh must hold 4 or 16 coefficients per channel (pad lower degrees with zeros)")
+    for name, t, shape in (("means", means, (n, 3)), ("log_scales", log_scales, (n, 3)), ("quats", quats, (n, 4)),
+                           ("opacity_logits", opacity_logits, (n,)), ("sh", sh, (n, k, 3))):
+        if tuple(t.shape) != shape or t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous():
+            raise ValueError("%s must be a contiguous float32 CUDA tensor of shape %s" % (name, shape))
+    return _lib.RawParams(means.data_ptr(), log_scales.data_ptr(), quats.data_ptr(), opacity_logits.data_ptr(),
+                          sh.data_ptr(), n, deg)
+
+
+class RasterizeFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, means, log_scales, quats, opacity_logits, sh, camera, options):
+        means, log_scales, quats = means.contiguous(), log_scales.contiguous(), quats.contiguous()
+        opacity_logits, sh = opacity_logits.contiguous(), sh.contiguous()
+        params = _raw_params(means, log_scales, quats, opacity_logits, sh)
+        img = torch.empty(camera.height, camera.width, 3, dtype=torch.float32, device=means.device)
+        trainer = _acquire()
+        stream = torch.cuda.current_stream(means.device).cuda_stream
+        try:
+            check(lib.aniso_b200_train_forward(trainer._h, ctypes.byref(params), ctypes.byref(c_camera(camera)),
+                                               ctypes.byref(options.c()), ctypes.c_void_p(img.data_ptr()),
+                                               ctypes.c_void_p(stream)))
+        except Exception:
+            _release(trainer)
+            raise
+        if any(ctx.needs_input_grad[:5]):
+            ctx.trainer = trainer
+        else:
+            ctx.trainer = None
+            _release(trainer)  # no backward will come; the next forward on this stream is ordered after
+        ctx.save_for_backward(means, log_scales, quats, opacity_logits, sh)
+        return img
+
+    @staticmethod
+    def backward(ctx, grad_img):
+        means, log_scales, quats, opacity_logits, sh = ctx.saved_tensors
+        grads = [torch.zeros_like(t) for t in (means, log_scales, quats, opacity_logits, sh)]
+        g = _lib.RawGrads(*[t.data_ptr() for t in grads])
+        gi = grad_img.contiguous().float()
+        stream = torch.cuda.current_stream(means.device).cuda_stream
+        trainer = ctx.trainer
+        try:
+            check(lib.aniso_b200_train_backward(trainer._h, ctypes.c_void_p(gi.data_ptr()), ctypes.byref(g),
+                                                ctypes.c_void_p(stream)))
+        finally:
+            ctx.trainer = None
+            # The next forward on this trainer is ordered after the backward's kernels (same stream).
+            _release(trainer)
+        return (*grads, None, None)
+
+
+def rasterize(means, log_scales, quats, opacity_logits, sh, camera, sh_degree: int = 3, splat_scale: float = 1.0):
+    """Differentiable render of one view: (H, W, 3) float32 colour."""
+    return RasterizeFunction.apply(means, log_scales, quats, opacity_logits, sh, camera,
+                                   RenderOptions(sh_degree, splat_scale))

@@ -1,0 +1,485 @@
+// The adjoint of the rasterizer (no counterpart in the reference, which has no backward pass; the
+// forward it differentiates is render.cpp:39-104 / 195-220 on the GPU path's lists).
+//
+// blend_backward: one 128-thread block per 16x16 tile, the forward's pixel layout (8x8 per warp,
+//   two pixels per lane). Each pixel walks its tile list back to front from its last applied
+//   splat, replaying the forward's alpha tests bit for bit (same record, same exponent code) and
+//   recovering the transmittance in front of each splat by division (T_j = T_{j+1} / (1 - a_j));
+//   nothing per pixel is stored but the final T and the last contributor. Per splat, the gradient
+//   with respect to its nine record parameters (u, v, A2, B2, C2, L, r, g, b) is reduced over the
+//   warp (12 shuffles for the 9 values), summed over the four warps in a fixed order, and written
+//   to the pair's slot in the depth-ordered pair list -- no atomics, so the result does not depend
+//   on scheduling.
+// gauss_backward: one thread per visible Gaussian (depth order) sums its pairs' slots, which are
+//   contiguous and summed in list order, and applies the chain rule through the record
+//   (conic, log2 opacity, SH colour), the EWA projection (2D covariance, clamped Jacobian, camera
+//   transform), the 3D covariance M M^T with M = R(q) diag(s), and the activations (exp, sigmoid,
+//   quaternion normalisation) to the 59 raw parameters.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ab2 {
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kBatch = 128;
+constexpr int kG = 9;
+constexpr float kLn2 = 0.69314718055994530942f;
+constexpr float kHalfLog2e = -0.72134752044448170368f;  // A2 = kHalfLog2e * A, C2 likewise
+constexpr float kNegLog2e = -1.44269504088896340736f;   // B2 = kNegLog2e * B
+
+__device__ __forceinline__ bool overlaps(int lo, int hi, int a, int b) { return lo <= b && hi >= a; }
+
+// Sums v[0..8] over the warp; afterwards the even lanes hold one sum each: value index *k (-1 for
+// none). 12 shuffles: each step hands half of the values to the partner lane.
+__device__ __forceinline__ float warp_reduce9(const float v[kG], int lane, int& k) {
+    const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4, b2 = lane & 2;
+    float a[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const float lo = v[i], hi = i + 5 < kG ? v[i + 5] : 0.f;
+        a[i] = (b16 ? hi : lo) + __shfl_xor_sync(0xFFFFFFFFu, b16 ? lo : hi, 16);
+    }
+    float b[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float lo = a[i], hi = i + 3 < 5 ? a[i + 3] : 0.f;
+        b[i] = (b8 ? hi : lo) + __shfl_xor_sync(0xFFFFFFFFu, b8 ? lo : hi, 8);
+    }
+    float c[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const float lo = b[i], hi = i + 2 < 3 ? b[i + 2] : 0.f;
+        c[i] = (b4 ? hi : lo) + __shfl_xor_sync(0xFFFFFFFFu, b4 ? lo : hi, 4);
+    }
+    const float d = (b2 ? c[1] : c[0]) + __shfl_xor_sync(0xFFFFFFFFu, b2 ? c[0] : c[1], 2);
+    const float e = d + __shfl_xor_sync(0xFFFFFFFFu, d, 1);
+    const int ci = b2 ? 1 : 0;
+    const int bi = ci + (b4 ? 2 : 0);
+    const int ai = bi + (b8 ? 3 : 0);
+    const int vi = ai + (b16 ? 5 : 0);
+    k = ((lane & 1) == 0 && bi < 3 && ai < 5 && vi < kG) ? vi : -1;
+    return e;
+}
+
+struct PixelState {
+    float T;                 // transmittance behind the splat being visited (starts at the final T)
+    float ar, ag, ab;        // colour accumulated from the splats behind it
+    float gr, gg, gb;        // dL/dC of the pixel
+    unsigned last;           // list position one past the last applied splat
+};
+
+// One pixel's adjoint step for splat j (list position pos); adds to g[0..8].
+__device__ __forceinline__ void pixel_step(PixelState& s, unsigned pos, float p, float dx, float dy, const float4& r0,
+                                           const float4& r1, float rb, float g[kG]) {
+    if (pos >= s.last) return;
+    const float e = ex2_approx(p);
+    const float alpha = fminf(0.99f, e);  // the same bits as the forward's splat_alpha
+    if (!(!(p > r1.y) && alpha >= 1.0f / 255.0f)) return;
+    const float om = 1.0f - alpha;
+    const float Tb = s.T / om;  // transmittance in front of the splat
+    const float w = alpha * Tb;
+    g[6] = fmaf(s.gr, w, g[6]);
+    g[7] = fmaf(s.gg, w, g[7]);
+    g[8] = fmaf(s.gb, w, g[8]);
+    const float inv_om = 1.0f / om;
+    const float dalpha = s.gr * (r1.z * Tb - s.ar * inv_om) + s.gg * (r1.w * Tb - s.ag * inv_om) +
+                         s.gb * (rb * Tb - s.ab * inv_om);
+    s.ar = fmaf(r1.z, w, s.ar);
+    s.ag = fmaf(r1.w, w, s.ag);
+    s.ab = fmaf(rb, w, s.ab);
+    s.T = Tb;
+    const float dp = e > 0.99f ? 0.f : dalpha * alpha * kLn2;  // d alpha / d p = alpha ln 2 unless clamped
+    g[0] -= dp * (2.0f * r0.z * dx + r0.w * dy);
+    g[1] -= dp * (2.0f * r1.x * dy + r0.w * dx);
+    g[2] = fmaf(dp, dx * dx, g[2]);
+    g[3] = fmaf(dp, dx * dy, g[3]);
+    g[4] = fmaf(dp, dy * dy, g[4]);
+    g[5] += dp;
+}
+
+__global__ void __launch_bounds__(kThreads) blend_backward_kernel(BackwardIn in, float* __restrict__ grad_pair) {
+    __shared__ float4 s_r0[kBatch];
+    __shared__ float4 s_r1[kBatch];
+    __shared__ float s_b[kBatch];
+    __shared__ unsigned s_pos[kBatch];
+    __shared__ unsigned char s_mask[kBatch];
+    __shared__ unsigned s_hit[kBatch];
+    __shared__ float s_grad[4][kBatch][kG];
+    __shared__ unsigned s_maxlast;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tile = blockIdx.x;
+    const int tx = tile % in.tiles_x, ty = tile / in.tiles_x;
+    const int ox = tx * kTile, oy = ty * kTile;
+    const int x0 = ox + (warp & 1) * 8 + 2 * (lane & 3), y = oy + (warp >> 1) * 8 + (lane >> 2);
+    const float px0 = x0 + 0.5f, py = y + 0.5f;
+    const uint2 range = (in.ctrl->flags & kFlagOverflow) ? make_uint2(0, 0) : in.ranges[tile];
+
+    PixelState s0{1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, range.x}, s1{1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, range.x};
+    if (x0 < in.width && y < in.height) {
+        const size_t p = static_cast<size_t>(y) * in.width + x0;
+        s0.T = in.t_final[p];
+        s0.last = in.n_contrib[p];
+        s0.gr = in.grad_img[3 * p];
+        s0.gg = in.grad_img[3 * p + 1];
+        s0.gb = in.grad_img[3 * p + 2];
+    }
+    if (x0 + 1 < in.width && y < in.height) {
+        const size_t p = static_cast<size_t>(y) * in.width + x0 + 1;
+        s1.T = in.t_final[p];
+        s1.last = in.n_contrib[p];
+        s1.gr = in.grad_img[3 * p];
+        s1.gg = in.grad_img[3 * p + 1];
+        s1.gb = in.grad_img[3 * p + 2];
+    }
+    if (tid == 0) s_maxlast = range.x;
+    __syncthreads();
+    const unsigned mylast = max(s0.last, s1.last);
+    const unsigned wlast = __reduce_max_sync(0xFFFFFFFFu, mylast);
+    if (lane == 0) atomicMax(&s_maxlast, wlast);
+    __syncthreads();
+    const unsigned end = s_maxlast;
+
+    // Pairs behind every pixel's last applied splat get zero gradient.
+    for (unsigned q = end + tid; q < range.y; q += kThreads) {
+        const unsigned g = in.vals[q];
+        const unsigned j = in.rank[g];
+        const unsigned long long rc = in.rect_sorted[j];
+        const unsigned rx0 = rc & 0xFFFFu, ry0 = (rc >> 16) & 0xFFFFu, rx1 = (rc >> 32) & 0xFFFFu;
+        float* out = grad_pair +
+                     static_cast<size_t>(in.offs[j] + (static_cast<unsigned>(ty) - ry0) * (rx1 - rx0 + 1) +
+                                         (static_cast<unsigned>(tx) - rx0)) * kG;
+#pragma unroll
+        for (int k = 0; k < kG; ++k) out[k] = 0.f;
+    }
+
+    for (unsigned top = end; top > range.x;) {
+        const unsigned start = top > range.x + kBatch ? top - kBatch : range.x;
+        const unsigned cnt = top - start;
+        // Stage the batch [start, top): records, warp masks and each pair's slot in the
+        // depth-ordered pair list (the slot of (Gaussian g, tile t) is offs[rank[g]] plus t's
+        // row-major index in g's rectangle).
+        for (unsigned slot = tid; slot < cnt; slot += kThreads) {
+            const unsigned g = in.vals[start + slot];
+            const SplatRecord r = in.rec[g];
+            s_r0[slot] = r.r0;
+            s_r1[slot] = r.r1;
+            s_b[slot] = r.r2.x;
+            const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
+            const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
+            const unsigned cols =
+                (overlaps(xlo, xhi, ox, ox + 7) ? 1u : 0u) | (overlaps(xlo, xhi, ox + 8, ox + 15) ? 2u : 0u);
+            unsigned m = 0;
+            if (overlaps(ylo, yhi, oy, oy + 7)) m |= cols;
+            if (overlaps(ylo, yhi, oy + 8, oy + 15)) m |= cols << 2;
+            s_mask[slot] = static_cast<unsigned char>(m);
+            s_hit[slot] = 0;
+            const unsigned j = in.rank[g];
+            const unsigned long long rc = in.rect_sorted[j];
+            const unsigned rx0 = rc & 0xFFFFu, ry0 = (rc >> 16) & 0xFFFFu, rx1 = (rc >> 32) & 0xFFFFu;
+            s_pos[slot] = in.offs[j] + (static_cast<unsigned>(ty) - ry0) * (rx1 - rx0 + 1) + (static_cast<unsigned>(tx) - rx0);
+        }
+        __syncthreads();
+        if (__any_sync(0xFFFFFFFFu, start < mylast)) {
+            for (int c = static_cast<int>((cnt - 1) / 32); c >= 0; --c) {
+                const unsigned idx = c * 32 + lane;
+                unsigned bits = __ballot_sync(0xFFFFFFFFu, idx < cnt && ((s_mask[idx] >> warp) & 1u));
+                while (bits) {
+                    const int b = 31 - __clz(bits);
+                    bits &= ~(1u << b);
+                    const unsigned jj = c * 32 + b;
+                    const unsigned pos = start + jj;
+                    if (!__any_sync(0xFFFFFFFFu, pos < mylast)) continue;
+                    const float4 r0 = s_r0[jj];
+                    const float4 r1 = s_r1[jj];
+                    const float rb = s_b[jj];
+                    const float dx0 = __fsub_rn(px0, r0.x), dy = __fsub_rn(py, r0.y);
+                    float p0, p1;
+                    splat_exponents(r0, r1, dx0, dy, p0, p1);
+                    float g[kG] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                    pixel_step(s0, pos, p0, dx0, dy, r0, r1, rb, g);
+                    pixel_step(s1, pos, p1, __fadd_rn(dx0, 1.0f), dy, r0, r1, rb, g);
+                    int k;
+                    const float sum = warp_reduce9(g, lane, k);
+                    if (k >= 0) s_grad[warp][jj][k] = sum;
+                    if (lane == 0) atomicOr(&s_hit[jj], 1u << warp);
+                }
+            }
+        }
+        __syncthreads();
+        // Fixed-order sum over the warps; every staged pair's slot is written.
+        for (unsigned slot = tid; slot < cnt; slot += kThreads) {
+            const unsigned hit = s_hit[slot];
+            float acc[kG];
+#pragma unroll
+            for (int k = 0; k < kG; ++k) acc[k] = 0.f;
+#pragma unroll
+            for (int w = 0; w < 4; ++w)
+                if (hit & (1u << w))
+#pragma unroll
+                    for (int k = 0; k < kG; ++k) acc[k] += s_grad[w][slot][k];
+            float* out = grad_pair + static_cast<size_t>(s_pos[slot]) * kG;
+#pragma unroll
+            for (int k = 0; k < kG; ++k) out[k] = acc[k];
+        }
+        __syncthreads();
+        top = start;
+    }
+}
+
+// SH basis (sh.cpp:18-58 order) and its derivatives along x, y, z, for degree D.
+template <int D>
+__device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16], float bx[16], float by[16],
+                                         float bz[16]) {
+    const float C0 = 0.28209479177387814f, C1 = 0.4886025119029199f;
+    const float C20 = 1.0925484305920792f, C21 = -1.0925484305920792f, C22 = 0.31539156525252005f,
+                C23 = -1.0925484305920792f, C24 = 0.5462742152960396f;
+    const float C30 = -0.5900435899266435f, C31 = 2.890611442640554f, C32 = -0.4570457994644658f,
+                C33 = 0.3731763325901154f, C34 = -0.4570457994644658f, C35 = 1.445305721320277f,
+                C36 = -0.5900435899266435f;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) b[k] = bx[k] = by[k] = bz[k] = 0.f;
+    b[0] = C0;
+    if (D >= 1) {
+        b[1] = -C1 * y; by[1] = -C1;
+        b[2] = C1 * z; bz[2] = C1;
+        b[3] = -C1 * x; bx[3] = -C1;
+    }
+    if (D >= 2) {
+        const float xx = x * x, yy = y * y, zz = z * z;
+        b[4] = C20 * x * y; bx[4] = C20 * y; by[4] = C20 * x;
+        b[5] = C21 * y * z; by[5] = C21 * z; bz[5] = C21 * y;
+        b[6] = C22 * (2 * zz - xx - yy); bx[6] = -2 * C22 * x; by[6] = -2 * C22 * y; bz[6] = 4 * C22 * z;
+        b[7] = C23 * x * z; bx[7] = C23 * z; bz[7] = C23 * x;
+        b[8] = C24 * (xx - yy); bx[8] = 2 * C24 * x; by[8] = -2 * C24 * y;
+        if (D >= 3) {
+            b[9] = C30 * y * (3 * xx - yy); bx[9] = C30 * 6 * x * y; by[9] = C30 * (3 * xx - 3 * yy);
+            b[10] = C31 * x * y * z; bx[10] = C31 * y * z; by[10] = C31 * x * z; bz[10] = C31 * x * y;
+            b[11] = C32 * y * (4 * zz - xx - yy); bx[11] = -2 * C32 * x * y; by[11] = C32 * (4 * zz - xx - 3 * yy);
+            bz[11] = 8 * C32 * y * z;
+            b[12] = C33 * z * (2 * zz - 3 * xx - 3 * yy); bx[12] = -6 * C33 * x * z; by[12] = -6 * C33 * y * z;
+            bz[12] = C33 * (6 * zz - 3 * xx - 3 * yy);
+            b[13] = C34 * x * (4 * zz - xx - yy); bx[13] = C34 * (4 * zz - 3 * xx - yy); by[13] = -2 * C34 * x * y;
+            bz[13] = 8 * C34 * x * z;
+            b[14] = C35 * z * (xx - yy); bx[14] = 2 * C35 * x * z; by[14] = -2 * C35 * y * z; bz[14] = C35 * (xx - yy);
+            b[15] = C36 * x * (xx - 3 * yy); bx[15] = C36 * (3 * xx - 3 * yy); by[15] = -6 * C36 * x * y;
+        }
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamParams cam, const Ctrl* ctrl,
+                                                             const unsigned* __restrict__ sorted_idx,
+                                                             const unsigned* __restrict__ offs,
+                                                             const unsigned long long* __restrict__ rect_sorted,
+                                                             const float* __restrict__ grad_pair, RawGrads out) {
+    const unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ctrl->flags & kFlagOverflow) return;
+    if (j >= ctrl->vis_count) return;
+    const unsigned i = sorted_idx[j];
+    const unsigned long long rc = rect_sorted[j];
+    const unsigned cnt = ((rc >> 32 & 0xFFFFu) - (rc & 0xFFFFu) + 1) * ((rc >> 48) - (rc >> 16 & 0xFFFFu) + 1);
+    float g9[kG] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float* gp = grad_pair + static_cast<size_t>(offs[j]) * kG;
+    for (unsigned k = 0; k < cnt; ++k)
+#pragma unroll
+        for (int c = 0; c < kG; ++c) g9[c] += gp[k * kG + c];
+
+    // ---- forward quantities (the preprocess kernel's, in the same order) ----
+    float4 pg, sg, qn;
+    raw.load(i, pg, sg, qn);
+    const float4 qraw = raw.quats[i];
+    const float qlen = sqrtf(qraw.x * qraw.x + qraw.y * qraw.y + qraw.z * qraw.z + qraw.w * qraw.w);
+    const float gx = pg.x, gy = pg.y, gz = pg.z, o = pg.w;
+    const float* W = cam.R;
+    const float px = W[0] * gx + W[1] * gy + W[2] * gz + cam.t[0];
+    const float py = W[3] * gx + W[4] * gy + W[5] * gz + cam.t[1];
+    const float pz = W[6] * gx + W[7] * gy + W[8] * gz + cam.t[2];
+    const float qw = qn.x, qx = qn.y, qy = qn.z, qz = qn.w;
+    const float Rq[3][3] = {{1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy)},
+                            {2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx)},
+                            {2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)}};
+    const float s[3] = {sg.x * cam.splatScale, sg.y * cam.splatScale, sg.z * cam.splatScale};
+    float M[3][3], S[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) M[r][c] = Rq[r][c] * s[c];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) S[r][c] = M[r][0] * M[c][0] + M[r][1] * M[c][1] + M[r][2] * M[c][2];
+    const float limX = 1.3f * 0.5f * cam.width / cam.fx, limY = 1.3f * 0.5f * cam.height / cam.fy;
+    const float rx = px / pz, ry = py / pz;
+    const bool clx = rx < -limX || rx > limX, cly = ry < -limY || ry > limY;
+    const float tx = fminf(limX, fmaxf(-limX, rx)) * pz;
+    const float ty = fminf(limY, fmaxf(-limY, ry)) * pz;
+    const float iz = 1.0f / pz, iz2 = iz * iz;
+    const float J[2][3] = {{cam.fx * iz, 0.f, -cam.fx * tx * iz2}, {0.f, cam.fy * iz, -cam.fy * ty * iz2}};
+    float T[2][3];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) T[r][c] = J[r][0] * W[c] + J[r][1] * W[3 + c] + J[r][2] * W[6 + c];
+    float ST[2][3];  // S T_r^T for r = 0, 1 (S symmetric)
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ST[r][c] = S[c][0] * T[r][0] + S[c][1] * T[r][1] + S[c][2] * T[r][2];
+    const float a = T[0][0] * ST[0][0] + T[0][1] * ST[0][1] + T[0][2] * ST[0][2] + 0.3f;
+    const float b = T[1][0] * ST[0][0] + T[1][1] * ST[0][1] + T[1][2] * ST[0][2];
+    const float c = T[1][0] * ST[1][0] + T[1][1] * ST[1][1] + T[1][2] * ST[1][2] + 0.3f;
+    const float det = a * c - b * b;
+
+    // ---- record parameters -> conic, opacity, colour ----
+    const float gu = g9[0], gv = g9[1];
+    const float gA = g9[2] * kHalfLog2e, gB = g9[3] * kNegLog2e, gC = g9[4] * kHalfLog2e;
+    const float go = g9[5] / (o * kLn2);  // L = log2(o)
+    float* gsh = out.sh + static_cast<size_t>(i) * raw.sh_planes * 4;
+    float gm[3] = {0.f, 0.f, 0.f};
+    {
+        float3 d = make_float3(gx - cam.eye[0], gy - cam.eye[1], gz - cam.eye[2]);
+        const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+        const float ux = d.x / len, uy = d.y / len, uz = d.z / len;
+        float bs[16], bxs[16], bys[16], bzs[16];
+        sh_basis<D>(ux, uy, uz, bs, bxs, bys, bzs);
+        constexpr int count = (D + 1) * (D + 1);
+        const float4* shp = raw.sh + static_cast<size_t>(i) * raw.sh_planes;
+        float shv[48];
+#pragma unroll
+        for (int k = 0; k < (count * 3 + 3) / 4; ++k) {
+            const float4 f = shp[k];
+            shv[4 * k] = f.x;
+            if (4 * k + 1 < 48) shv[4 * k + 1] = f.y;
+            if (4 * k + 2 < 48) shv[4 * k + 2] = f.z;
+            if (4 * k + 3 < 48) shv[4 * k + 3] = f.w;
+        }
+        float gdir[3] = {0.f, 0.f, 0.f};
+        const float grgb[3] = {g9[6], g9[7], g9[8]};
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            float pre = 0.5f;
+#pragma unroll
+            for (int k = 0; k < count; ++k) pre += bs[k] * shv[k * 3 + ch];
+            const float gc = pre > 0.f ? grgb[ch] : 0.f;  // rgb = max(0, pre)
+#pragma unroll
+            for (int k = 0; k < count; ++k) {
+                gsh[k * 3 + ch] = bs[k] * gc;
+                gdir[0] += shv[k * 3 + ch] * bxs[k] * gc;
+                gdir[1] += shv[k * 3 + ch] * bys[k] * gc;
+                gdir[2] += shv[k * 3 + ch] * bzs[k] * gc;
+            }
+        }
+        const float dd = ux * gdir[0] + uy * gdir[1] + uz * gdir[2];
+        gm[0] += (gdir[0] - ux * dd) / len;
+        gm[1] += (gdir[1] - uy * dd) / len;
+        gm[2] += (gdir[2] - uz * dd) / len;
+    }
+    out.logits[i] = go * o * (1.0f - o);
+
+    // ---- conic (A, B, C) = (c, -b, a) / det -> 2D covariance (a, b, c) ----
+    const float id2 = 1.0f / (det * det);
+    const float ga = (-c * c * gA + b * c * gB - b * b * gC) * id2;
+    const float gb = (2.0f * b * c * gA - (det + 2.0f * b * b) * gB + 2.0f * a * b * gC) * id2;
+    const float gc2 = (-b * b * gA + a * b * gB - a * a * gC) * id2;
+
+    // ---- covariance = T S T^T + 0.3 I -> S, T ----
+    float gS[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            gS[r][q] = ga * T[0][r] * T[0][q] + gb * T[0][r] * T[1][q] + gc2 * T[1][r] * T[1][q];
+    float gT[2][3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        gT[0][q] = 2.0f * ga * ST[0][q] + gb * ST[1][q];
+        gT[1][q] = gb * ST[0][q] + 2.0f * gc2 * ST[1][q];
+    }
+    // ---- T = J W -> J -> camera-space position ----
+    float gJ[2][3];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) gJ[r][k] = gT[r][0] * W[3 * k] + gT[r][1] * W[3 * k + 1] + gT[r][2] * W[3 * k + 2];
+    float gpx = gu * cam.fx * iz, gpy = gv * cam.fy * iz;
+    float gpz = -(gu * cam.fx * px + gv * cam.fy * py) * iz2;
+    gpz += -(gJ[0][0] * cam.fx + gJ[1][1] * cam.fy) * iz2;
+    const float iz3 = iz2 * iz;
+    if (!clx) {
+        gpx += gJ[0][2] * (-cam.fx * iz2);
+        gpz += gJ[0][2] * (2.0f * cam.fx * tx * iz3);
+    } else {
+        gpz += gJ[0][2] * (cam.fx * (tx * iz) * iz2);  // tx = lim pz: J02 = -fx lim / pz
+    }
+    if (!cly) {
+        gpy += gJ[1][2] * (-cam.fy * iz2);
+        gpz += gJ[1][2] * (2.0f * cam.fy * ty * iz3);
+    } else {
+        gpz += gJ[1][2] * (cam.fy * (ty * iz) * iz2);
+    }
+    // camera transform p_cam = W p + t
+    gm[0] += W[0] * gpx + W[3] * gpy + W[6] * gpz;
+    gm[1] += W[1] * gpx + W[4] * gpy + W[7] * gpz;
+    gm[2] += W[2] * gpx + W[5] * gpy + W[8] * gpz;
+    out.means[3 * i] = gm[0];
+    out.means[3 * i + 1] = gm[1];
+    out.means[3 * i + 2] = gm[2];
+
+    // ---- S = M M^T -> M = R(q) diag(s) -> s, R(q) ----
+    float gM[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            gM[r][k] = (gS[r][0] + gS[0][r]) * M[0][k] + (gS[r][1] + gS[1][r]) * M[1][k] + (gS[r][2] + gS[2][r]) * M[2][k];
+    float gR[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float gs = 0.f;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            gR[r][k] = gM[r][k] * s[k];
+            gs += gM[r][k] * Rq[r][k];
+        }
+        out.log_scales[3 * i + k] = gs * s[k];  // s = exp(log s) * splat_scale
+    }
+    const float gqw = 2.0f * (-qz * gR[0][1] + qy * gR[0][2] + qz * gR[1][0] - qx * gR[1][2] - qy * gR[2][0] + qx * gR[2][1]);
+    const float gqx = 2.0f * (qy * gR[0][1] + qz * gR[0][2] + qy * gR[1][0] - 2.0f * qx * gR[1][1] - qw * gR[1][2] +
+                              qz * gR[2][0] + qw * gR[2][1] - 2.0f * qx * gR[2][2]);
+    const float gqy = 2.0f * (-2.0f * qy * gR[0][0] + qx * gR[0][1] + qw * gR[0][2] + qx * gR[1][0] + qz * gR[1][2] -
+                              qw * gR[2][0] + qz * gR[2][1] - 2.0f * qy * gR[2][2]);
+    const float gqz = 2.0f * (-2.0f * qz * gR[0][0] - qw * gR[0][1] + qx * gR[0][2] + qw * gR[1][0] -
+                              2.0f * qz * gR[1][1] + qy * gR[1][2] + qx * gR[2][0] + qy * gR[2][1]);
+    // q_n = q / |q|
+    const float dq = qw * gqw + qx * gqx + qy * gqy + qz * gqz;
+    const float il = qlen > 0 ? 1.0f / qlen : 0.f;
+    out.quats[4 * i] = (gqw - qw * dq) * il;
+    out.quats[4 * i + 1] = (gqx - qx * dq) * il;
+    out.quats[4 * i + 2] = (gqy - qy * dq) * il;
+    out.quats[4 * i + 3] = (gqz - qz * dq) * il;
+}
+
+}  // namespace
+
+void launch_blend_backward(const BackwardIn& in, int tiles_y, float* grad_pair, cudaStream_t stream) {
+    const unsigned blocks = static_cast<unsigned>(in.tiles_x) * static_cast<unsigned>(tiles_y);
+    if (blocks == 0) return;
+    blend_backward_kernel<<<blocks, kThreads, 0, stream>>>(in, grad_pair);
+}
+
+void launch_gauss_backward(const RawParams& raw, const CamParams& cam, const Ctrl* ctrl, const unsigned* sorted_idx,
+                           const unsigned* offs, const unsigned long long* rect_sorted, const float* grad_pair,
+                           unsigned max_visible, const RawGrads& out, cudaStream_t stream) {
+    const unsigned blocks = (max_visible + 127) / 128;
+    if (blocks == 0) return;
+    switch (cam.shDegree) {
+        case 0: gauss_backward_kernel<0><<<blocks, 128, 0, stream>>>(raw, cam, ctrl, sorted_idx, offs, rect_sorted, grad_pair, out); break;
+        case 1: gauss_backward_kernel<1><<<blocks, 128, 0, stream>>>(raw, cam, ctrl, sorted_idx, offs, rect_sorted, grad_pair, out); break;
+        case 2: gauss_backward_kernel<2><<<blocks, 128, 0, stream>>>(raw, cam, ctrl, sorted_idx, offs, rect_sorted, grad_pair, out); break;
+        default: gauss_backward_kernel<3><<<blocks, 128, 0, stream>>>(raw, cam, ctrl, sorted_idx, offs, rect_sorted, grad_pair, out); break;
+    }
+}
+
+}  // namespace ab2

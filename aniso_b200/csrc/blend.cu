@@ -37,8 +37,9 @@ __device__ __forceinline__ bool overlaps(int lo, int hi, int a, int b) { return 
 template <bool kTrain>
 __device__ __forceinline__ void blend_px(float p, float L, float r, float g, float b, float& T, float& cr, float& cg,
                                          float& cb, float& tfin, unsigned& last, unsigned pos) {
-    const float alpha = fminf(0.99f, ex2_approx(p));
-    if (!(p > L) && alpha >= 1.0f / 255.0f) {
+    bool valid;
+    const float alpha = splat_alpha(p, L, valid);
+    if (valid) {
         const float w = alpha * T;
         const float nt = T - w;
         if (nt < 1e-4f) {
@@ -138,11 +139,8 @@ __global__ void __launch_bounds__(kThreads) blend_kernel(const uint2* __restrict
                     const float4 a = s_r0[jj];
                     const float4 k = s_r1[jj];
                     const float bb = s_b[jj];
-                    const float dx0 = px0 - a.x, dy = py - a.y;
-                    const float t1 = a.w * dy, t3 = fmaf(k.x * dy, dy, k.y);
-                    const float p0 = fmaf(dx0, fmaf(a.z, dx0, t1), t3);
-                    const float dx1 = dx0 + 1.0f;
-                    const float p1 = fmaf(dx1, fmaf(a.z, dx1, t1), t3);
+                    float p0, p1;
+                    splat_exponents(a, k, __fsub_rn(px0, a.x), __fsub_rn(py, a.y), p0, p1);
                     const unsigned pos = base + jj + 1;
                     blend_px<kTrain>(p0, k.y, k.z, k.w, bb, T0, r0, g0, b0c, tf0, last0, pos);
                     blend_px<kTrain>(p1, k.y, k.z, k.w, bb, T1, r1, g1, b1c, tf1, last1, pos);

@@ -90,7 +90,7 @@ struct Arena {
     DevBuf<unsigned> depth_key;
     DevBuf<unsigned> vis_key[2], vis_idx[2];
     DevBuf<unsigned> pair_key[2], pair_val[2];
-    DevBuf<unsigned> offs, chunk_start;
+    DevBuf<unsigned> offs, rank, chunk_start;
     DevBuf<unsigned long long> rect_sorted;
     DevBuf<uint2> ranges;
     DevBuf<Ctrl> ctrl;
@@ -99,6 +99,8 @@ struct Arena {
 
     unsigned depth_chunks() const { return chunks_of(static_cast<uint64_t>(std::max<int64_t>(n, 1)), onesweep_chunk_items()); }
     unsigned tile_chunks() const { return chunks_of(std::max(pair_cap, 1u), onesweep_chunk_items()); }
+    // The vis_idx buffer that holds the depth-sorted visible list after the depth passes.
+    static int sorted_buf() { return (kMaxPasses - 1) & 1; }
 
     int init(int64_t count, unsigned cap) {
         n = count;
@@ -114,6 +116,7 @@ struct Arena {
         AB_TRY(st_depth.reserve(static_cast<size_t>(kMaxPasses) * depth_chunks() * kRadix, true));
         AB_TRY(st_dup.reserve(chunks_of(nn, pair_scan_chunk_items()), true));
         AB_TRY(offs.reserve(nn));
+        AB_TRY(rank.reserve(nn));
         AB_TRY(rect_sorted.reserve(nn));
         return grow_pairs(cap);
     }
@@ -154,10 +157,10 @@ int enqueue_sort(Arena& A, int tiles_x, int tiles_y, cudaStream_t st, int* final
                         A.st_depth.p + static_cast<size_t>(p) * A.depth_chunks() * kRadix,
                         &ctrl->chunk_ctr[kCtrDepth0 + p], ctrl, st);
     }
-    const int sorted = (kMaxPasses - 1) & 1;
+    const int sorted = A.sorted_buf();
     const unsigned tiles = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
     const int tile_passes = std::max(1, (bits_for(tiles - 1) + kRadixBits - 1) / kRadixBits);
-    const DupBuffers dup{A.offs.p, A.rect_sorted.p, A.chunk_start.p};
+    const DupBuffers dup{A.offs.p, A.rank.p, A.rect_sorted.p, A.chunk_start.p};
     launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, nmax, tiles_x, tile_passes, dup,
                      A.pair_key[0].p, A.pair_val[0].p, A.st_dup.p, st);
     for (int p = 0; p < tile_passes; ++p) {
@@ -302,7 +305,7 @@ int new_scene(int64_t n, int degree, aniso_b200_scene** out, aniso_b200_scene** 
 
 // The per-view constants, packed as gpu_render.cu:301-316 packs them (doubles cast to float; the
 // eye is Camera::centre(), camera.cpp:19-23, computed in double).
-int pack_camera(const aniso_b200_scene* s, const aniso_b200_camera* c, const aniso_b200_options* o, CamParams& cp) {
+int pack_camera_deg(int scene_degree, const aniso_b200_camera* c, const aniso_b200_options* o, CamParams& cp) {
     if (!c) return fail(ANISO_B200_ERR_ARGUMENT, "camera is NULL");
     if (c->width <= 0 || c->height <= 0 || c->width > 32767 || c->height > 32767)
         return fail(ANISO_B200_ERR_ARGUMENT, "camera size must be in [1, 32767]");
@@ -326,10 +329,14 @@ int pack_camera(const aniso_b200_scene* s, const aniso_b200_camera* c, const ani
     cp.height = c->height;
     cp.tilesX = (c->width + kTile - 1) / kTile;
     cp.tilesY = (c->height + kTile - 1) / kTile;
-    cp.shDegree = std::min(std::min(opt_degree, s->degree), 3);
-    cp.shCoeffs = (s->degree + 1) * (s->degree + 1);
+    cp.shDegree = std::min(std::min(opt_degree, scene_degree), 3);
+    cp.shCoeffs = (scene_degree + 1) * (scene_degree + 1);
     cp.splatScale = o ? o->splat_scale : 1.0f;
     return 0;
+}
+
+int pack_camera(const aniso_b200_scene* s, const aniso_b200_camera* c, const aniso_b200_options* o, CamParams& cp) {
+    return pack_camera_deg(s->degree, c, o, cp);
 }
 
 // Enqueues one frame; ev (4 events, may be NULL) brackets the stages. With stop_after_sort, the
@@ -379,6 +386,21 @@ int read_ctrl(aniso_b200_scene* s, cudaStream_t st) {
 }
 
 }  // namespace
+
+struct aniso_b200_trainer {
+    Arena arena;
+    Ctrl* host_ctrl = nullptr;  // pinned
+    DevBuf<float> t_final, grad_pair;
+    DevBuf<unsigned> n_contrib;
+    // The state of the last forward, for its backward.
+    bool has_forward = false;
+    RawParams raw{};
+    CamParams cam{};
+    int fin = 0;
+    ~aniso_b200_trainer() {
+        if (host_ctrl) cudaFreeHost(host_ctrl);
+    }
+};
 
 extern "C" {
 
@@ -692,6 +714,147 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     if (ranges)
         AB_CUDA(cudaMemcpy(ranges, A.ranges.p, static_cast<size_t>(tiles_x) * tiles_y * sizeof(uint2),
                            cudaMemcpyDeviceToHost));
+    return ANISO_B200_OK;
+}
+
+int aniso_b200_trainer_create(aniso_b200_trainer** out) {
+    if (!out) return fail(ANISO_B200_ERR_ARGUMENT, "out is NULL");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(ANISO_B200_ERR_NO_DEVICE, "no CUDA device");
+    }
+    aniso_b200_trainer* t = new (std::nothrow) aniso_b200_trainer();
+    if (!t) return fail(ANISO_B200_ERR_OUT_OF_MEMORY, "host allocation failed");
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&t->host_ctrl), sizeof(Ctrl));
+    if (e != cudaSuccess) {
+        delete t;
+        return cuda_fail(e, "cudaMallocHost");
+    }
+    std::memset(t->host_ctrl, 0, sizeof(Ctrl));
+    *out = t;
+    return ANISO_B200_OK;
+}
+
+int aniso_b200_trainer_destroy(aniso_b200_trainer* t) {
+    if (t) cudaDeviceSynchronize();
+    delete t;
+    return ANISO_B200_OK;
+}
+
+int aniso_b200_train_forward(aniso_b200_trainer* t, const aniso_b200_raw_params* params, const aniso_b200_camera* camera,
+                             const aniso_b200_options* options, float* image_device, void* stream) {
+    if (!t || !params || !image_device) return fail(ANISO_B200_ERR_ARGUMENT, "trainer/params/image is NULL");
+    const aniso_b200_raw_params& P = *params;
+    if (P.n < 0 || P.n >= (int64_t(1) << 31)) return fail(ANISO_B200_ERR_ARGUMENT, "n must be in [0, 2^31)");
+    if (P.sh_degree != 1 && P.sh_degree != 3)
+        return fail(ANISO_B200_ERR_ARGUMENT, "stored SH degree must be 1 or 3 (whole 16-byte words per Gaussian)");
+    if (P.n > 0 && (!P.means || !P.log_scales || !P.quats || !P.opacity_logits || !P.sh))
+        return fail(ANISO_B200_ERR_ARGUMENT, "a parameter pointer is NULL");
+    if ((reinterpret_cast<uintptr_t>(P.quats) | reinterpret_cast<uintptr_t>(P.sh)) & 15)
+        return fail(ANISO_B200_ERR_ARGUMENT, "quats and sh must be 16-byte aligned");
+    CamParams cam;
+    AB_TRY(pack_camera_deg(P.sh_degree, camera, options, cam));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Arena& A = t->arena;
+    if (A.n < P.n) {
+        const uint64_t cap = std::max<uint64_t>(1u << 20, 4ull * static_cast<uint64_t>(P.n));
+        A.~Arena();
+        new (&A) Arena();
+        AB_TRY(A.init(P.n, static_cast<unsigned>(std::min<uint64_t>(cap, 0x3FFFFFFFull))));
+    }
+    const size_t pixels = static_cast<size_t>(cam.width) * cam.height;
+    AB_TRY(t->t_final.reserve(pixels));
+    AB_TRY(t->n_contrib.reserve(pixels));
+    RawParams raw;
+    raw.means = P.means;
+    raw.log_scales = P.log_scales;
+    raw.quats = reinterpret_cast<const float4*>(P.quats);
+    raw.logits = P.opacity_logits;
+    raw.sh = reinterpret_cast<const float4*>(P.sh);
+    raw.n = P.n;
+    raw.sh_planes = (P.sh_degree + 1) * (P.sh_degree + 1) * 3 / 4;
+    BlendOut out;
+    out.rgbf = image_device;
+    out.t_final = t->t_final.p;
+    out.n_contrib = t->n_contrib.p;
+    const int64_t saved_n = A.n;
+    A.n = P.n;  // grids follow this frame's Gaussian count
+    int rc = ANISO_B200_OK;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        rc = A.tick(st);
+        if (rc) break;
+        launch_frame_begin(A.ctrl.p, st);
+        launch_preprocess_raw(raw, cam, A.ctrl.p, A.rec.p, A.rect16.p, A.depth_key.p, st);
+        int fin = 0;
+        rc = enqueue_sort(A, cam.tilesX, cam.tilesY, st, &fin);
+        if (rc) break;
+        launch_blend(A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, cam.width, cam.height, cam.tilesX, cam.tilesY,
+                     out, st);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(t->host_ctrl, A.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "train forward");
+            break;
+        }
+        const Ctrl& h = *t->host_ctrl;
+        if (h.flags & kFlagTimeout) {
+            rc = fail(ANISO_B200_ERR_DEVICE_WAIT, "a device-side look-back wait gave up");
+            break;
+        }
+        if (h.flags & kFlagOverflow) {
+            const uint64_t need = h.pair_total + h.pair_total / 4 + 1024;
+            if (need > 0x3FFFFFFFull) {
+                rc = fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 splat-tile pairs");
+                break;
+            }
+            rc = A.grow_pairs(static_cast<unsigned>(need));
+            if (rc) break;
+            rc = fail(ANISO_B200_ERR_ARGUMENT, "pair capacity kept overflowing");
+            continue;
+        }
+        t->has_forward = true;
+        t->raw = raw;
+        t->cam = cam;
+        t->fin = fin;
+        rc = ANISO_B200_OK;
+        break;
+    }
+    A.n = std::max(A.n, saved_n);
+    if (rc != ANISO_B200_OK) t->has_forward = false;
+    return rc;
+}
+
+int aniso_b200_train_backward(aniso_b200_trainer* t, const float* grad_image_device, const aniso_b200_raw_grads* grads,
+                              void* stream) {
+    if (!t || !grad_image_device || !grads) return fail(ANISO_B200_ERR_ARGUMENT, "trainer/grad_image/grads is NULL");
+    if (!t->has_forward) return fail(ANISO_B200_ERR_ARGUMENT, "no forward to differentiate");
+    if (t->raw.n > 0 && (!grads->means || !grads->log_scales || !grads->quats || !grads->opacity_logits || !grads->sh))
+        return fail(ANISO_B200_ERR_ARGUMENT, "a gradient pointer is NULL");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Arena& A = t->arena;
+    const Ctrl& h = *t->host_ctrl;
+    AB_TRY(t->grad_pair.reserve(std::max<uint64_t>(h.pair_total, 1) * 9));
+    BackwardIn in;
+    in.ranges = A.ranges.p;
+    in.vals = A.pair_val[t->fin].p;
+    in.rec = A.rec.p;
+    in.ctrl = A.ctrl.p;
+    in.t_final = t->t_final.p;
+    in.n_contrib = t->n_contrib.p;
+    in.grad_img = grad_image_device;
+    in.rank = A.rank.p;
+    in.offs = A.offs.p;
+    in.rect_sorted = A.rect_sorted.p;
+    in.width = t->cam.width;
+    in.height = t->cam.height;
+    in.tiles_x = t->cam.tilesX;
+    launch_blend_backward(in, t->cam.tilesY, t->grad_pair.p, st);
+    RawGrads g{grads->means, grads->log_scales, grads->quats, grads->opacity_logits, grads->sh};
+    launch_gauss_backward(t->raw, t->cam, A.ctrl.p, A.vis_idx[A.sorted_buf()].p, A.offs.p, A.rect_sorted.p,
+                          t->grad_pair.p, h.vis_count, g, st);
+    AB_CUDA(cudaGetLastError());
     return ANISO_B200_OK;
 }
 

@@ -48,6 +48,35 @@ struct SceneView {
     const float4* sh;   // [n][sh_planes]
     int64_t n;
     int sh_planes;
+
+    // Activated position + opacity, scale and rotation of Gaussian i.
+    __device__ __forceinline__ void load(int64_t i, float4& pg, float4& sg, float4& q) const {
+        pg = pos_op[i];
+        sg = scale[i];
+        q = rot[i];
+    }
+};
+
+// The optimizer's raw per-Gaussian tensors (device memory, row-major): means n x 3, log-scales
+// n x 3, quaternions n x 4 (w first, any norm), opacity logits n, SH n x K x 3 with 3K a multiple
+// of 4 (sh_planes = 3K / 4). Activated on the fly as the reference loader activates a PLY
+// (ply_loader.cpp:124-131): exp, sigmoid, normalise.
+struct RawParams {
+    const float* means;
+    const float* log_scales;
+    const float4* quats;
+    const float* logits;
+    const float4* sh;
+    int64_t n;
+    int sh_planes;
+
+    __device__ __forceinline__ void load(int64_t i, float4& pg, float4& sg, float4& q) const {
+        pg = make_float4(means[3 * i], means[3 * i + 1], means[3 * i + 2], 1.0f / (1.0f + expf(-logits[i])));
+        sg = make_float4(expf(log_scales[3 * i]), expf(log_scales[3 * i + 1]), expf(log_scales[3 * i + 2]), 0.f);
+        const float4 r = quats[i];
+        const float nrm = sqrtf(r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w);
+        q = nrm > 0 ? make_float4(r.x / nrm, r.y / nrm, r.z / nrm, r.w / nrm) : make_float4(1.f, 0.f, 0.f, 0.f);
+    }
 };
 
 // Control block of one frame. Zeroed (except epoch, which advances) by frame_begin.
@@ -197,6 +226,27 @@ __device__ __forceinline__ float ex2_approx(float x) {
 struct SplatRecord {
     float4 r0, r1, r2;
 };
+
+// The base-2 exponents of a splat at two horizontally adjacent pixel centres (dx0, dy) and
+// (dx0 + 1, dy): A2 dx^2 + B2 dx dy + C2 dy^2 + L from the record (r0 = u, v, A2, B2; r1 = C2, L, ..).
+// Written with explicit roundings so the forward and backward blends compute the same bits (the
+// backward replays the forward's alpha tests).
+__device__ __forceinline__ void splat_exponents(const float4& r0, const float4& r1, float dx0, float dy, float& p0,
+                                                float& p1) {
+    const float t1 = __fmul_rn(r0.w, dy);
+    const float t3 = __fmaf_rn(__fmul_rn(r1.x, dy), dy, r1.y);
+    p0 = __fmaf_rn(dx0, __fmaf_rn(r0.z, dx0, t1), t3);
+    const float dx1 = __fadd_rn(dx0, 1.0f);
+    p1 = __fmaf_rn(dx1, __fmaf_rn(r0.z, dx1, t1), t3);
+}
+
+// alpha of a splat from its exponent; valid = the reference's tests pass (power <= 0 is p <= L,
+// alpha >= 1/255).
+__device__ __forceinline__ float splat_alpha(float p, float L, bool& valid) {
+    const float alpha = fminf(0.99f, ex2_approx(p));
+    valid = !(p > L) && alpha >= 1.0f / 255.0f;
+    return alpha;
+}
 
 __device__ __forceinline__ unsigned pack_i16x2(int lo, int hi) {
     return (static_cast<unsigned>(lo) & 0xFFFFu) | (static_cast<unsigned>(hi) << 16);

@@ -26,6 +26,9 @@ void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
 void launch_preprocess(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
                        unsigned long long* rect16, unsigned* depth_key, const DebugProjection* dbg,
                        cudaStream_t stream);
+// The same projection of the optimizer's raw tensors (activated in the kernel).
+void launch_preprocess_raw(const RawParams& params, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
+                           unsigned long long* rect16, unsigned* depth_key, cudaStream_t stream);
 
 // One stable onesweep LSD radix pass over (key, value) u32 pairs, 8-bit digit at `shift`; `hist` is
 // this digit's global histogram. masked_count > 0: the input is the N depth keys with culled ones
@@ -43,6 +46,7 @@ void launch_onesweep(const unsigned* keys_in, const unsigned* vals_in, unsigned*
 // pairs per block.
 struct DupBuffers {
     unsigned* offs;                   // [N] exclusive pair offset of each depth-sorted Gaussian
+    unsigned* rank;                   // [N] depth-sorted position of each visible Gaussian index
     unsigned long long* rect_sorted;  // [N] its 16x16-tile rectangle, in sorted order
     unsigned* chunk_start;            // [capacity / expand_chunk_pairs() + 2] first Gaussian per chunk
 };
@@ -72,5 +76,34 @@ struct BlendOut {
 
 void launch_blend(const uint2* ranges, const unsigned* sorted_vals, const SplatRecord* rec, const Ctrl* ctrl,
                   int width, int height, int tiles_x, int tiles_y, const BlendOut& out, cudaStream_t stream);
+
+// ---- the adjoint ----------------------------------------------------------------------------
+struct BackwardIn {
+    const uint2* ranges;
+    const unsigned* vals;                // sorted pair values (Gaussian indices)
+    const SplatRecord* rec;
+    const Ctrl* ctrl;
+    const float* t_final;                // H x W, from the training forward
+    const unsigned* n_contrib;           // H x W
+    const float* grad_img;               // H x W x 3, dL/d(colour)
+    const unsigned* rank;                // depth-sorted position of each Gaussian
+    const unsigned* offs;                // pair offset of each depth-sorted Gaussian
+    const unsigned long long* rect_sorted;
+    int width, height, tiles_x;
+};
+// Gradients of the raw parameters (device, the layout of RawParams; overwritten for visible
+// Gaussians, left untouched for culled ones -- callers zero them).
+struct RawGrads {
+    float* means;
+    float* log_scales;
+    float* quats;
+    float* logits;
+    float* sh;
+};
+// grad_pair: 9 floats per pair, at the pair's depth-ordered slot.
+void launch_blend_backward(const BackwardIn& in, int tiles_y, float* grad_pair, cudaStream_t stream);
+void launch_gauss_backward(const RawParams& raw, const CamParams& cam, const Ctrl* ctrl, const unsigned* sorted_idx,
+                           const unsigned* offs, const unsigned long long* rect_sorted, const float* grad_pair,
+                           unsigned max_visible, const RawGrads& out, cudaStream_t stream);
 
 }  // namespace ab2

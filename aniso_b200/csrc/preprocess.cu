@@ -144,8 +144,8 @@ __device__ __forceinline__ unsigned axis_bounds(float centre, float cov, float t
     return pack_i16x2(lo, hi);
 }
 
-template <int D, bool kDebug>
-__global__ void __launch_bounds__(256, 3) preprocess_kernel(SceneView sc, CamParams cam, Ctrl* __restrict__ ctrl,
+template <int D, bool kDebug, class Src>
+__global__ void __launch_bounds__(256, 3) preprocess_kernel(Src sc, CamParams cam, Ctrl* __restrict__ ctrl,
                                                          SplatRecord* __restrict__ rec,
                                                          unsigned long long* __restrict__ rect16,
                                                          unsigned* __restrict__ depth_key, DebugProjection dbg) {
@@ -158,9 +158,8 @@ __global__ void __launch_bounds__(256, 3) preprocess_kernel(SceneView sc, CamPar
     bool vis = false;
     unsigned depth_bits = 0;
     if (i < sc.n) {
-        const float4 pg = sc.pos_op[i];
-        const float4 sg = sc.scale[i];
-        const float4 q = sc.rot[i];
+        float4 pg, sg, q;
+        sc.load(i, pg, sg, q);
         Projected p;
         vis = project(pg, sg, q, cam, p);
         if (kDebug) dbg.tiles_touched[i] = 0;
@@ -222,17 +221,16 @@ __global__ void __launch_bounds__(256, 3) preprocess_kernel(SceneView sc, CamPar
         if (s_hist[k]) atomicAdd(&ctrl->depth_hist[k], s_hist[k]);
 }
 
-template <bool kDebug>
-void launch_preprocess_t(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
-                         unsigned long long* rect16, unsigned* depth_key, const DebugProjection& dbg,
-                         cudaStream_t stream) {
+template <bool kDebug, class Src>
+void launch_preprocess_t(const Src& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec, unsigned long long* rect16,
+                         unsigned* depth_key, const DebugProjection& dbg, cudaStream_t stream) {
     const unsigned blocks = static_cast<unsigned>((sc.n + 255) / 256);
     if (blocks == 0) return;
     switch (cam.shDegree) {
-        case 0: preprocess_kernel<0, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
-        case 1: preprocess_kernel<1, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
-        case 2: preprocess_kernel<2, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
-        default: preprocess_kernel<3, kDebug><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
+        case 0: preprocess_kernel<0, kDebug, Src><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
+        case 1: preprocess_kernel<1, kDebug, Src><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
+        case 2: preprocess_kernel<2, kDebug, Src><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
+        default: preprocess_kernel<3, kDebug, Src><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
     }
 }
 
@@ -245,6 +243,11 @@ void launch_preprocess(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, Sp
         launch_preprocess_t<true>(sc, cam, ctrl, rec, rect16, depth_key, *dbg, stream);
     else
         launch_preprocess_t<false>(sc, cam, ctrl, rec, rect16, depth_key, DebugProjection{}, stream);
+}
+
+void launch_preprocess_raw(const RawParams& params, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
+                           unsigned long long* rect16, unsigned* depth_key, cudaStream_t stream) {
+    launch_preprocess_t<false>(params, cam, ctrl, rec, rect16, depth_key, DebugProjection{}, stream);
 }
 
 }  // namespace ab2

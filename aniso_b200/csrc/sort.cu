@@ -195,6 +195,7 @@ __global__ void __launch_bounds__(kOsThreads) onesweep_kernel(const unsigned* __
 __global__ void __launch_bounds__(256) pair_scan_kernel(const unsigned* __restrict__ sorted_idx,
                                                         const unsigned long long* __restrict__ rect16, Ctrl* ctrl,
                                                         unsigned capacity, unsigned* __restrict__ offs,
+                                                        unsigned* __restrict__ rank,
                                                         unsigned long long* __restrict__ rect_sorted,
                                                         unsigned* __restrict__ chunk_start,
                                                         unsigned long long* status) {
@@ -217,7 +218,9 @@ __global__ void __launch_bounds__(256) pair_scan_kernel(const unsigned* __restri
         unsigned c = 0;
         unsigned long long r = 0;
         if (j < V) {
-            r = rect16[sorted_idx[j]];
+            const unsigned g = sorted_idx[j];
+            rank[g] = j;
+            r = rect16[g];
             const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu, y1 = r >> 48;
             c = (x1 - x0 + 1) * (y1 - y0 + 1);
         }
@@ -385,8 +388,8 @@ void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect
                       unsigned* pair_val, unsigned long long* status, cudaStream_t stream) {
     const unsigned scan_blocks = (max_visible + kScanChunk - 1) / kScanChunk;
     if (scan_blocks == 0) return;
-    pair_scan_kernel<<<scan_blocks, 256, 0, stream>>>(sorted_idx, rect16, ctrl, capacity, buf.offs, buf.rect_sorted,
-                                                      buf.chunk_start, status);
+    pair_scan_kernel<<<scan_blocks, 256, 0, stream>>>(sorted_idx, rect16, ctrl, capacity, buf.offs, buf.rank,
+                                                      buf.rect_sorted, buf.chunk_start, status);
     const unsigned expand_blocks = (capacity + kExpandChunk - 1) / kExpandChunk;
     expand_kernel<<<expand_blocks, 256, 0, stream>>>(sorted_idx, buf.rect_sorted, buf.offs, buf.chunk_start, ctrl,
                                                      capacity, tiles_x, tile_passes, pair_key, pair_val);

@@ -111,6 +111,54 @@ int aniso_b200_profile_read(aniso_b200_scene* scene, double* project_ms, double*
 /* Copies the last error message (NUL-terminated, truncated to len) and returns its full length. */
 size_t aniso_b200_last_error(char* buf, size_t len);
 
+/* ---- the differentiable path (no counterpart in the reference: it has no backward pass; the
+ * training pipeline it drives calls the third-party gsplat rasterizer instead,
+ * pipeline/train_gsplat.py:96-102) ----------------------------------------------------------- */
+
+/* Opaque: the work buffers of one forward and its backward. */
+typedef struct aniso_b200_trainer aniso_b200_trainer;
+
+/* The optimizer's raw tensors, DEVICE pointers, row-major float32, as train_gsplat.py:85-92 keeps
+ * them: means n x 3, log-scales n x 3, quaternions n x 4 (w first, any norm), opacity logits n,
+ * SH n x (sh_degree+1)^2 x 3. sh_degree is the STORED degree and must be 1 or 3 (so each
+ * Gaussian's SH is whole 16-byte words); quats and sh 16-byte aligned. Activations (exp, sigmoid,
+ * normalise) are applied inside the kernels. */
+typedef struct aniso_b200_raw_params {
+    const float* means;
+    const float* log_scales;
+    const float* quats;
+    const float* opacity_logits;
+    const float* sh;
+    int64_t n;
+    int32_t sh_degree;
+} aniso_b200_raw_params;
+
+/* Gradient outputs, DEVICE pointers with the shapes of aniso_b200_raw_params. The caller zeroes
+ * them; entries of Gaussians culled in the view are left untouched. */
+typedef struct aniso_b200_raw_grads {
+    float* means;
+    float* log_scales;
+    float* quats;
+    float* opacity_logits;
+    float* sh;
+} aniso_b200_raw_grads;
+
+int aniso_b200_trainer_create(aniso_b200_trainer** out);
+int aniso_b200_trainer_destroy(aniso_b200_trainer* trainer);
+
+/* Renders the float colour image (width*height*3, unclamped, the sum before the 8-bit rounding of
+ * gpu_render.cu:229-231) into image_device on `stream` and keeps what the backward needs. Returns
+ * after the frame has run (it reads the frame's pair count to size its buffers). */
+int aniso_b200_train_forward(aniso_b200_trainer* trainer, const aniso_b200_raw_params* params,
+                             const aniso_b200_camera* camera, const aniso_b200_options* options, float* image_device,
+                             void* stream);
+
+/* The adjoint of the last train_forward: given dL/d(image) (device, width*height*3), writes the
+ * gradients of the 59 raw parameters per Gaussian. The params of that forward must be unchanged.
+ * Deterministic: no atomics; every sum runs in a fixed order. Enqueued on `stream`. */
+int aniso_b200_train_backward(aniso_b200_trainer* trainer, const float* grad_image_device,
+                              const aniso_b200_raw_grads* grads, void* stream);
+
 /* ---- introspection used by the parity tests (no counterpart in gpu_render.h) ---------------- */
 
 /* Runs the projection only and copies, per Gaussian, what the reference preprocess kernel

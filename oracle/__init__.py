@@ -61,6 +61,11 @@ class Restatement:
         L.orc_render.restype = _I
         L.orc_sort_keys.argtypes = [_I64, _P, _P, _P, _I, _I, _P, _P, _I64, _P]
         L.orc_sort_keys.restype = _I64
+        L.orc_train_forward_f64.argtypes = [_I64, _P, _P, _P, _P, _P, _I, _P, _I, _I, _I, ctypes.c_double, _P]
+        L.orc_train_forward_f64.restype = _I
+        L.orc_train_backward_f64.argtypes = [_I64, _P, _P, _P, _P, _P, _I, _P, _I, _I, _I, ctypes.c_double, _P,
+                                             _P, _P, _P, _P, _P]
+        L.orc_train_backward_f64.restype = _I
 
     def activate(self, raw):
         n = raw.n
@@ -121,6 +126,34 @@ class Restatement:
                                      _ptr(values), keys.shape[0], _ptr(ranges))
         assert got == total
         return keys[:total], values[:total], ranges
+
+
+    # ---- FP64 gradient oracle: raw parameters as float64 arrays (means n x 3, log_scales n x 3,
+    # quats n x 4, logits n, sh n x K x 3) ----
+    @staticmethod
+    def _f64(params):
+        return [np.ascontiguousarray(p, dtype=np.float64) for p in params]
+
+    def train_forward_f64(self, params, cam, sh_degree=3, splat_scale=1.0):
+        means, ls, q, lg, sh = self._f64(params)
+        img = np.zeros((cam.height, cam.width, 3), np.float64)
+        c = _cam(cam)
+        rc = self.lib.orc_train_forward_f64(means.shape[0], _ptr(means), _ptr(ls), _ptr(q), _ptr(lg), _ptr(sh),
+                                            sh.shape[1], _ptr(c), cam.width, cam.height, sh_degree, splat_scale,
+                                            _ptr(img))
+        assert rc == 0, rc
+        return img
+
+    def train_backward_f64(self, params, cam, grad_img, sh_degree=3, splat_scale=1.0):
+        means, ls, q, lg, sh = self._f64(params)
+        gi = np.ascontiguousarray(grad_img, np.float64)
+        grads = [np.zeros_like(a) for a in (means, ls, q, lg, sh)]
+        c = _cam(cam)
+        rc = self.lib.orc_train_backward_f64(means.shape[0], _ptr(means), _ptr(ls), _ptr(q), _ptr(lg), _ptr(sh),
+                                             sh.shape[1], _ptr(c), cam.width, cam.height, sh_degree, splat_scale,
+                                             _ptr(gi), *[_ptr(g) for g in grads])
+        assert rc == 0, rc
+        return grads
 
 
 class ReferenceCPU:

@@ -381,3 +381,362 @@ int64_t orc_sort_keys(int64_t n, const uint32_t* tiles_touched, const uint32_t* 
     }
     return total;
 }
+
+/* ==== FP64 forward and adjoint of the training render (the gradient oracle) ====================
+ *
+ * The same algorithm as the CPU renderer (render.cpp:39-104 projection, 8x8-tile lists from the
+ * 3-sigma rectangles render.cpp:166-171, depth order with index ties, render.cpp:195-220 blending
+ * and thresholds), evaluated in double from the optimizer's raw parameters (exp scale, sigmoid
+ * opacity, normalised quaternion), producing the unclamped colour. The adjoint is derived by hand
+ * from the same equations. Camera values are rounded to float first, as the GPU path packs them
+ * (gpu_render.cu:301-316), so both evaluate the same function.
+ * params: means n x 3, log_scales n x 3, quats n x 4 (w first), logits n, sh n x K x 3. */
+
+typedef struct {
+    double R[9], t[3], eye[3], fx, fy, cx, cy;
+    int w, h;
+} orc_cam64;
+
+static orc_cam64 cam64(const double* cam, int w, int h) {
+    orc_cam64 c;
+    for (int k = 0; k < 9; ++k) c.R[k] = (float)cam[k];
+    for (int k = 0; k < 3; ++k) c.t[k] = (float)cam[9 + k];
+    float e[3];
+    orc_camera_centre(cam, e);
+    for (int k = 0; k < 3; ++k) c.eye[k] = e[k];
+    c.fx = (float)cam[12]; c.fy = (float)cam[13]; c.cx = (float)cam[14]; c.cy = (float)cam[15];
+    c.w = w; c.h = h;
+    return c;
+}
+
+typedef struct {
+    int alive, x0, y0, x1, y1;      /* 8x8-tile rectangle */
+    float depth32;                   /* ordering key */
+    double u, v, A, B, C, o, rgb[3], pre[3];
+    /* intermediates for the adjoint */
+    double p[3], pc[3], qn[4], qlen, s[3], Rq[9], M[9], S[9], T[6], a, b, c, det, dir[3], len;
+    int clx, cly;
+} orc_sp64;
+
+static void sh_basis64(double x, double y, double z, int D, double* b, double* bx, double* by, double* bz) {
+    const double C0 = 0.28209479177387814, C1 = 0.4886025119029199;
+    const double C20 = 1.0925484305920792, C21 = -1.0925484305920792, C22 = 0.31539156525252005,
+                 C23 = -1.0925484305920792, C24 = 0.5462742152960396;
+    const double C30 = -0.5900435899266435, C31 = 2.890611442640554, C32 = -0.4570457994644658,
+                 C33 = 0.3731763325901154, C34 = -0.4570457994644658, C35 = 1.445305721320277,
+                 C36 = -0.5900435899266435;
+    for (int k = 0; k < 16; ++k) b[k] = bx[k] = by[k] = bz[k] = 0;
+    b[0] = C0;
+    if (D >= 1) { b[1] = -C1 * y; by[1] = -C1; b[2] = C1 * z; bz[2] = C1; b[3] = -C1 * x; bx[3] = -C1; }
+    if (D >= 2) {
+        const double xx = x * x, yy = y * y, zz = z * z;
+        b[4] = C20 * x * y; bx[4] = C20 * y; by[4] = C20 * x;
+        b[5] = C21 * y * z; by[5] = C21 * z; bz[5] = C21 * y;
+        b[6] = C22 * (2 * zz - xx - yy); bx[6] = -2 * C22 * x; by[6] = -2 * C22 * y; bz[6] = 4 * C22 * z;
+        b[7] = C23 * x * z; bx[7] = C23 * z; bz[7] = C23 * x;
+        b[8] = C24 * (xx - yy); bx[8] = 2 * C24 * x; by[8] = -2 * C24 * y;
+        if (D >= 3) {
+            b[9] = C30 * y * (3 * xx - yy); bx[9] = 6 * C30 * x * y; by[9] = C30 * (3 * xx - 3 * yy);
+            b[10] = C31 * x * y * z; bx[10] = C31 * y * z; by[10] = C31 * x * z; bz[10] = C31 * x * y;
+            b[11] = C32 * y * (4 * zz - xx - yy); bx[11] = -2 * C32 * x * y; by[11] = C32 * (4 * zz - xx - 3 * yy);
+            bz[11] = 8 * C32 * y * z;
+            b[12] = C33 * z * (2 * zz - 3 * xx - 3 * yy); bx[12] = -6 * C33 * x * z; by[12] = -6 * C33 * y * z;
+            bz[12] = C33 * (6 * zz - 3 * xx - 3 * yy);
+            b[13] = C34 * x * (4 * zz - xx - yy); bx[13] = C34 * (4 * zz - 3 * xx - yy); by[13] = -2 * C34 * x * y;
+            bz[13] = 8 * C34 * x * z;
+            b[14] = C35 * z * (xx - yy); bx[14] = 2 * C35 * x * z; by[14] = -2 * C35 * y * z; bz[14] = C35 * (xx - yy);
+            b[15] = C36 * x * (xx - 3 * yy); bx[15] = C36 * (3 * xx - 3 * yy); by[15] = -6 * C36 * x * y;
+        }
+    }
+}
+
+static void splat64(const orc_cam64* cam, const double* means, const double* log_scales, const double* quats,
+                    const double* logits, const double* sh, int K, int D, double splat_scale, int64_t i,
+                    orc_sp64* s) {
+    memset(s, 0, sizeof *s);
+    const double* R = cam->R;
+    for (int k = 0; k < 3; ++k) s->p[k] = means[3 * i + k];
+    for (int r = 0; r < 3; ++r)
+        s->pc[r] = R[3 * r] * s->p[0] + R[3 * r + 1] * s->p[1] + R[3 * r + 2] * s->p[2] + cam->t[r];
+    const double px = s->pc[0], py = s->pc[1], pz = s->pc[2];
+    if (pz < 0.2) return;
+    const double* q = quats + 4 * i;
+    s->qlen = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    for (int k = 0; k < 4; ++k) s->qn[k] = s->qlen > 0 ? q[k] / s->qlen : (k == 0);
+    const double w = s->qn[0], x = s->qn[1], y = s->qn[2], z = s->qn[3];
+    double* Rq = s->Rq;
+    Rq[0] = 1 - 2 * (y * y + z * z); Rq[1] = 2 * (x * y - w * z); Rq[2] = 2 * (x * z + w * y);
+    Rq[3] = 2 * (x * y + w * z); Rq[4] = 1 - 2 * (x * x + z * z); Rq[5] = 2 * (y * z - w * x);
+    Rq[6] = 2 * (x * z - w * y); Rq[7] = 2 * (y * z + w * x); Rq[8] = 1 - 2 * (x * x + y * y);
+    for (int k = 0; k < 3; ++k) s->s[k] = exp(log_scales[3 * i + k]) * splat_scale;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) s->M[3 * r + c] = Rq[3 * r + c] * s->s[c];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            s->S[3 * r + c] = s->M[3 * r] * s->M[3 * c] + s->M[3 * r + 1] * s->M[3 * c + 1] + s->M[3 * r + 2] * s->M[3 * c + 2];
+    const double limX = 1.3 * 0.5 * cam->w / cam->fx, limY = 1.3 * 0.5 * cam->h / cam->fy;
+    double rx = px / pz, ry = py / pz;
+    s->clx = rx < -limX || rx > limX;
+    s->cly = ry < -limY || ry > limY;
+    rx = rx < -limX ? -limX : (rx > limX ? limX : rx);
+    ry = ry < -limY ? -limY : (ry > limY ? limY : ry);
+    const double tx = rx * pz, ty = ry * pz;
+    const double J[6] = {cam->fx / pz, 0, -cam->fx * tx / (pz * pz), 0, cam->fy / pz, -cam->fy * ty / (pz * pz)};
+    for (int r = 0; r < 2; ++r)
+        for (int c = 0; c < 3; ++c) s->T[3 * r + c] = J[3 * r] * R[c] + J[3 * r + 1] * R[3 + c] + J[3 * r + 2] * R[6 + c];
+    double ST[6];
+    for (int r = 0; r < 2; ++r)
+        for (int c = 0; c < 3; ++c)
+            ST[3 * r + c] = s->S[3 * c] * s->T[3 * r] + s->S[3 * c + 1] * s->T[3 * r + 1] + s->S[3 * c + 2] * s->T[3 * r + 2];
+    s->a = s->T[0] * ST[0] + s->T[1] * ST[1] + s->T[2] * ST[2] + 0.3;
+    s->b = s->T[3] * ST[0] + s->T[4] * ST[1] + s->T[5] * ST[2];
+    s->c = s->T[3] * ST[3] + s->T[4] * ST[4] + s->T[5] * ST[5] + 0.3;
+    s->det = s->a * s->c - s->b * s->b;
+    if (s->det <= 0) return;
+    s->A = s->c / s->det; s->B = -s->b / s->det; s->C = s->a / s->det;
+    const double mid = 0.5 * (s->a + s->c);
+    const double m2 = mid * mid - s->det;
+    const int radius = (int)ceil(3.0 * sqrt(mid + sqrt(m2 > 0.1 ? m2 : 0.1)));
+    s->u = cam->fx * px / pz + cam->cx;
+    s->v = cam->fy * py / pz + cam->cy;
+    if (s->u + radius < 0 || s->v + radius < 0 || s->u - radius >= cam->w || s->v - radius >= cam->h) return;
+    const int tx8 = (cam->w + 7) / 8, ty8 = (cam->h + 7) / 8;
+    int a;
+    a = (int)(s->u - radius) / 8; s->x0 = a > 0 ? a : 0;
+    a = (int)(s->v - radius) / 8; s->y0 = a > 0 ? a : 0;
+    a = (int)(s->u + radius) / 8; s->x1 = a < tx8 - 1 ? a : tx8 - 1;
+    a = (int)(s->v + radius) / 8; s->y1 = a < ty8 - 1 ? a : ty8 - 1;
+    s->depth32 = (float)pz;
+    s->o = 1.0 / (1.0 + exp(-logits[i]));
+    double d[3] = {s->p[0] - cam->eye[0], s->p[1] - cam->eye[1], s->p[2] - cam->eye[2]};
+    s->len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int k = 0; k < 3; ++k) s->dir[k] = d[k] / s->len;
+    double b[16], bx[16], by[16], bz[16];
+    sh_basis64(s->dir[0], s->dir[1], s->dir[2], D, b, bx, by, bz);
+    const int count = (D + 1) * (D + 1);
+    for (int ch = 0; ch < 3; ++ch) {
+        double v = 0.5;
+        for (int k = 0; k < count; ++k) v += b[k] * sh[(i * K + k) * 3 + ch];
+        s->pre[ch] = v;
+        s->rgb[ch] = v > 0 ? v : 0;
+    }
+    s->alive = 1;
+}
+
+static const orc_sp64* g_sort_sp;
+static int cmp_depth_index(const void* a, const void* b) {
+    const uint32_t i = *(const uint32_t*)a, j = *(const uint32_t*)b;
+    const float di = g_sort_sp[i].depth32, dj = g_sort_sp[j].depth32;
+    if (di < dj) return -1;
+    if (di > dj) return 1;
+    return i < j ? -1 : (i > j);
+}
+
+/* Shared by forward and adjoint: splats, depth order, per-8x8-tile lists. */
+typedef struct {
+    orc_sp64* sp;
+    uint32_t* order;
+    size_t visible;
+} orc_frame64;
+
+static int frame64(const orc_cam64* cam, int64_t n, const double* means, const double* log_scales, const double* quats,
+                   const double* logits, const double* sh, int K, int D, double splat_scale, orc_frame64* f) {
+    f->sp = (orc_sp64*)calloc(n ? (size_t)n : 1, sizeof(orc_sp64));
+    f->order = (uint32_t*)malloc((n ? (size_t)n : 1) * sizeof(uint32_t));
+    if (!f->sp || !f->order) return 1;
+    f->visible = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        splat64(cam, means, log_scales, quats, logits, sh, K, D, splat_scale, i, &f->sp[i]);
+        if (f->sp[i].alive) f->order[f->visible++] = (uint32_t)i;
+    }
+    g_sort_sp = f->sp;
+    qsort(f->order, f->visible, sizeof(uint32_t), cmp_depth_index);
+    return 0;
+}
+
+/* Applied contributors of one pixel, front to back: (index, alpha, T before, e^power, clamped). */
+typedef struct { uint32_t idx; double alpha, T, ep, dx, dy; int clamped; } orc_contrib;
+
+static size_t pixel64(const orc_frame64* f, int x, int y, orc_contrib* out, double* col) {
+    const double px = x + 0.5, py = y + 0.5;
+    const int sx = x / 8, sy = y / 8;
+    double T = 1.0;
+    size_t n = 0;
+    col[0] = col[1] = col[2] = 0;
+    for (size_t k = 0; k < f->visible; ++k) {
+        const orc_sp64* s = &f->sp[f->order[k]];
+        if (sx < s->x0 || sx > s->x1 || sy < s->y0 || sy > s->y1) continue;
+        const double dx = px - s->u, dy = py - s->v;
+        const double power = -0.5 * (s->A * dx * dx + s->C * dy * dy) - s->B * dx * dy;
+        if (power > 0) continue;
+        const double ep = exp(power);
+        const double e = s->o * ep;
+        const double alpha = e < 0.99 ? e : 0.99;
+        if (alpha < 1.0 / 255.0) continue;
+        const double nt = T * (1 - alpha);
+        if (nt < 1e-4) break;
+        for (int c = 0; c < 3; ++c) col[c] += s->rgb[c] * alpha * T;
+        if (out) {
+            out[n].idx = f->order[k]; out[n].alpha = alpha; out[n].T = T; out[n].ep = ep;
+            out[n].dx = dx; out[n].dy = dy; out[n].clamped = !(e < 0.99);
+        }
+        ++n;
+        T = nt;
+    }
+    return n;
+}
+
+int orc_train_forward_f64(int64_t n, const double* means, const double* log_scales, const double* quats,
+                          const double* logits, const double* sh, int K, const double* camd, int w, int h,
+                          int sh_degree, double splat_scale, double* out_img) {
+    const orc_cam64 cam = cam64(camd, w, h);
+    int D = sh_degree;
+    if (D > 3) D = 3;
+    if ((D + 1) * (D + 1) > K) return 2;
+    orc_frame64 f;
+    if (frame64(&cam, n, means, log_scales, quats, logits, sh, K, D, splat_scale, &f)) return 1;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) pixel64(&f, x, y, NULL, out_img + ((size_t)y * w + x) * 3);
+    free(f.sp);
+    free(f.order);
+    return 0;
+}
+
+int orc_train_backward_f64(int64_t n, const double* means, const double* log_scales, const double* quats,
+                           const double* logits, const double* sh, int K, const double* camd, int w, int h,
+                           int sh_degree, double splat_scale, const double* grad_img, double* g_means,
+                           double* g_log_scales, double* g_quats, double* g_logits, double* g_sh) {
+    const orc_cam64 cam = cam64(camd, w, h);
+    int D = sh_degree;
+    if (D > 3) D = 3;
+    if ((D + 1) * (D + 1) > K) return 2;
+    orc_frame64 f;
+    if (frame64(&cam, n, means, log_scales, quats, logits, sh, K, D, splat_scale, &f)) return 1;
+    /* per-splat 2D gradients: u, v, A, B, C, o, r, g, b */
+    double* g2 = (double*)calloc((n ? (size_t)n : 1) * 9, sizeof(double));
+    orc_contrib* cl = (orc_contrib*)malloc((f.visible ? f.visible : 1) * sizeof(orc_contrib));
+    if (!g2 || !cl) return 1;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            double col[3];
+            const size_t m = pixel64(&f, x, y, cl, col);
+            const double* gc = grad_img + ((size_t)y * w + x) * 3;
+            double acc[3] = {0, 0, 0};
+            for (size_t q = m; q-- > 0;) {
+                const orc_contrib* c = &cl[q];
+                const orc_sp64* s = &f.sp[c->idx];
+                double* g = g2 + (size_t)c->idx * 9;
+                const double wgt = c->alpha * c->T;
+                double dalpha = 0;
+                for (int ch = 0; ch < 3; ++ch) {
+                    g[6 + ch] += gc[ch] * wgt;
+                    dalpha += gc[ch] * (s->rgb[ch] * c->T - acc[ch] / (1 - c->alpha));
+                    acc[ch] += s->rgb[ch] * wgt;
+                }
+                if (c->clamped) continue;
+                /* alpha = o e^power */
+                g[5] += dalpha * c->ep;
+                const double dpow = dalpha * c->alpha;
+                const double dx = c->dx, dy = c->dy;
+                g[2] += dpow * (-0.5 * dx * dx);
+                g[3] += dpow * (-dx * dy);
+                g[4] += dpow * (-0.5 * dy * dy);
+                g[0] += dpow * (s->A * dx + s->B * dy);  /* d power / d u */
+                g[1] += dpow * (s->C * dy + s->B * dx);
+            }
+        }
+    const int count = (D + 1) * (D + 1);
+    for (size_t k = 0; k < f.visible; ++k) {
+        const uint32_t i = f.order[k];
+        const orc_sp64* s = &f.sp[i];
+        const double* g = g2 + (size_t)i * 9;
+        /* colour and SH */
+        double b[16], bx[16], by[16], bz[16];
+        sh_basis64(s->dir[0], s->dir[1], s->dir[2], D, b, bx, by, bz);
+        double gdir[3] = {0, 0, 0};
+        for (int ch = 0; ch < 3; ++ch) {
+            const double gcol = s->pre[ch] > 0 ? g[6 + ch] : 0;
+            for (int q = 0; q < count; ++q) {
+                const double shv = sh[((size_t)i * K + q) * 3 + ch];
+                g_sh[((size_t)i * K + q) * 3 + ch] = b[q] * gcol;
+                gdir[0] += shv * bx[q] * gcol;
+                gdir[1] += shv * by[q] * gcol;
+                gdir[2] += shv * bz[q] * gcol;
+            }
+        }
+        const double dd = s->dir[0] * gdir[0] + s->dir[1] * gdir[1] + s->dir[2] * gdir[2];
+        double gm[3];
+        for (int q = 0; q < 3; ++q) gm[q] = (gdir[q] - s->dir[q] * dd) / s->len;
+        g_logits[i] = g[5] * s->o * (1 - s->o);
+        /* conic -> 2D covariance */
+        const double a = s->a, bb = s->b, c = s->c, det = s->det, id2 = 1.0 / (det * det);
+        const double gA = g[2], gB = g[3], gC = g[4];
+        const double ga = (-c * c * gA + bb * c * gB - bb * bb * gC) * id2;
+        const double gb = (2 * bb * c * gA - (det + 2 * bb * bb) * gB + 2 * a * bb * gC) * id2;
+        const double gc2 = (-bb * bb * gA + a * bb * gB - a * a * gC) * id2;
+        const double* T = s->T;
+        const double* S = s->S;
+        double ST[6];
+        for (int r = 0; r < 2; ++r)
+            for (int q = 0; q < 3; ++q) ST[3 * r + q] = S[3 * q] * T[3 * r] + S[3 * q + 1] * T[3 * r + 1] + S[3 * q + 2] * T[3 * r + 2];
+        double gS[9], gT[6], gJ[6];
+        for (int r = 0; r < 3; ++r)
+            for (int q = 0; q < 3; ++q)
+                gS[3 * r + q] = ga * T[r] * T[q] + gb * T[r] * T[3 + q] + gc2 * T[3 + r] * T[3 + q];
+        for (int q = 0; q < 3; ++q) {
+            gT[q] = 2 * ga * ST[q] + gb * ST[3 + q];
+            gT[3 + q] = gb * ST[q] + 2 * gc2 * ST[3 + q];
+        }
+        const double* W = cam.R;
+        for (int r = 0; r < 2; ++r)
+            for (int kk = 0; kk < 3; ++kk) gJ[3 * r + kk] = gT[3 * r] * W[3 * kk] + gT[3 * r + 1] * W[3 * kk + 1] + gT[3 * r + 2] * W[3 * kk + 2];
+        const double px = s->pc[0], py = s->pc[1], pz = s->pc[2], iz = 1 / pz, iz2 = iz * iz, iz3 = iz2 * iz;
+        const double limX = 1.3 * 0.5 * cam.w / cam.fx, limY = 1.3 * 0.5 * cam.h / cam.fy;
+        double rx = px / pz, ry = py / pz;
+        rx = rx < -limX ? -limX : (rx > limX ? limX : rx);
+        ry = ry < -limY ? -limY : (ry > limY ? limY : ry);
+        const double tx = rx * pz, ty = ry * pz;
+        double gpx = g[0] * cam.fx * iz, gpy = g[1] * cam.fy * iz;
+        double gpz = -(g[0] * cam.fx * px + g[1] * cam.fy * py) * iz2 - (gJ[0] * cam.fx + gJ[4] * cam.fy) * iz2;
+        if (!s->clx) { gpx += gJ[2] * (-cam.fx * iz2); gpz += gJ[2] * (2 * cam.fx * tx * iz3); }
+        else gpz += gJ[2] * (cam.fx * rx * iz2);
+        if (!s->cly) { gpy += gJ[5] * (-cam.fy * iz2); gpz += gJ[5] * (2 * cam.fy * ty * iz3); }
+        else gpz += gJ[5] * (cam.fy * ry * iz2);
+        for (int q = 0; q < 3; ++q) gm[q] += W[q] * gpx + W[3 + q] * gpy + W[6 + q] * gpz;
+        for (int q = 0; q < 3; ++q) g_means[3 * i + q] = gm[q];
+        /* S = M M^T, M = R(q) diag(s) */
+        const double* M = s->M;
+        const double* Rq = s->Rq;
+        double gM[9], gR[9];
+        for (int r = 0; r < 3; ++r)
+            for (int kk = 0; kk < 3; ++kk) {
+                double v = 0;
+                for (int q = 0; q < 3; ++q) v += (gS[3 * r + q] + gS[3 * q + r]) * M[3 * q + kk];
+                gM[3 * r + kk] = v;
+            }
+        for (int kk = 0; kk < 3; ++kk) {
+            double gsv = 0;
+            for (int r = 0; r < 3; ++r) {
+                gR[3 * r + kk] = gM[3 * r + kk] * s->s[kk];
+                gsv += gM[3 * r + kk] * Rq[3 * r + kk];
+            }
+            g_log_scales[3 * i + kk] = gsv * s->s[kk];
+        }
+        const double qw = s->qn[0], qx = s->qn[1], qy = s->qn[2], qz = s->qn[3];
+        const double gqw = 2 * (-qz * gR[1] + qy * gR[2] + qz * gR[3] - qx * gR[5] - qy * gR[6] + qx * gR[7]);
+        const double gqx = 2 * (qy * gR[1] + qz * gR[2] + qy * gR[3] - 2 * qx * gR[4] - qw * gR[5] + qz * gR[6] + qw * gR[7] - 2 * qx * gR[8]);
+        const double gqy = 2 * (-2 * qy * gR[0] + qx * gR[1] + qw * gR[2] + qx * gR[3] + qz * gR[5] - qw * gR[6] + qz * gR[7] - 2 * qy * gR[8]);
+        const double gqz = 2 * (-2 * qz * gR[0] - qw * gR[1] + qx * gR[2] + qw * gR[3] - 2 * qz * gR[4] + qy * gR[5] + qx * gR[6] + qy * gR[7]);
+        const double dq = qw * gqw + qx * gqx + qy * gqy + qz * gqz;
+        const double il = s->qlen > 0 ? 1 / s->qlen : 0;
+        g_quats[4 * i] = (gqw - qw * dq) * il;
+        g_quats[4 * i + 1] = (gqx - qx * dq) * il;
+        g_quats[4 * i + 2] = (gqy - qy * dq) * il;
+        g_quats[4 * i + 3] = (gqz - qz * dq) * il;
+    }
+    free(g2);
+    free(cl);
+    free(f.sp);
+    free(f.order);
+    return 0;
+}
