@@ -5,4 +5,4 @@ Importing the package loads libaniso_b200.so and fails if it is missing; there i
 """
 from . import scenes  # noqa: F401  (pure numpy, no library needed)
 from ._lib import AnisoError, LIB_PATH  # noqa: F401
-from .renderer import GpuRenderer, RenderOptions, keys_of, sort_projection  # noqa: F401
+from .renderer import BatchOptions, BatchRenderer, GpuRenderer, RenderOptions, keys_of, sort_projection  # noqa: F401

@@ -37,6 +37,12 @@ EXPORTS = [
     "aniso_b200_trainer_destroy",
     "aniso_b200_train_forward",
     "aniso_b200_train_backward",
+    "aniso_b200_batch_create",
+    "aniso_b200_batch_render",
+    "aniso_b200_batch_sync",
+    "aniso_b200_batch_destroy",
+    "aniso_b200_train_batch_forward",
+    "aniso_b200_train_batch_backward",
 ]
 
 
@@ -48,6 +54,11 @@ class Camera(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("sh_degree", ctypes.c_int32), ("splat_scale", ctypes.c_float)]
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("sh_degree", ctypes.c_int32), ("splat_scale", ctypes.c_float), ("tile_w", ctypes.c_int32),
+                ("tile_h", ctypes.c_int32), ("blend_batch", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):
@@ -96,6 +107,12 @@ def _load():
         "aniso_b200_train_forward": [P, ctypes.POINTER(RawParams), ctypes.POINTER(Camera), ctypes.POINTER(Options), P,
                                      P],
         "aniso_b200_train_backward": [P, P, ctypes.POINTER(RawGrads), P],
+        "aniso_b200_batch_create": [P, I32, P, I32, ctypes.POINTER(BatchOptions), ctypes.POINTER(P)],
+        "aniso_b200_batch_render": [P, P, P, P],
+        "aniso_b200_batch_sync": [P, ctypes.POINTER(Stats)],
+        "aniso_b200_batch_destroy": [P],
+        "aniso_b200_train_batch_forward": [P, P, I32, P, P, I32, ctypes.POINTER(BatchOptions), P, P],
+        "aniso_b200_train_batch_backward": [P, P, P, P],
         "aniso_b200_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(I64)],
     }

@@ -2,6 +2,7 @@
 
     img = rasterize(means, log_scales, quats, opacity_logits, sh, camera, sh_degree=3)
     loss = ((img - target) ** 2).sum(); loss.backward()
+    imgs = rasterize_batch([(means, log_scales, quats, opacity_logits, sh), ...], cameras, view_scene)
 
 The parameters are the raw optimizer tensors of pipeline/train_gsplat.py:85-92 (means, log-scales,
 quaternions, opacity logits, SH as (n, 16, 3) = sh0 ++ shN), float32 on one CUDA device; the
@@ -19,7 +20,7 @@ import torch
 
 from . import _lib
 from ._lib import check, lib
-from .renderer import RenderOptions, c_camera
+from .renderer import BatchOptions, RenderOptions, c_camera, c_cameras
 
 
 class Trainer:
@@ -112,3 +113,66 @@ def rasterize(means, log_scales, quats, opacity_logits, sh, camera, sh_degree: i
     """Differentiable render of one view: (H, W, 3) float32 colour."""
     return RasterizeFunction.apply(means, log_scales, quats, opacity_logits, sh, camera,
                                    RenderOptions(sh_degree, splat_scale))
+
+
+class RasterizeBatchFunction(torch.autograd.Function):
+    """Views of several scenes in one forward and one backward (aniso_b200_train_batch_*)."""
+
+    @staticmethod
+    def forward(ctx, meta, *tensors):
+        cameras, view_scene, options = meta
+        S = len(tensors) // 5
+        tensors = [t.contiguous() for t in tensors]
+        params = (_lib.RawParams * S)(*[_raw_params(*tensors[5 * s:5 * s + 5]) for s in range(S)])
+        device = tensors[0].device
+        imgs = [torch.empty(c.height, c.width, 3, dtype=torch.float32, device=device) for c in cameras]
+        vs = (ctypes.c_int32 * len(view_scene))(*view_scene)
+        cams = c_cameras(cameras)
+        ptrs = (ctypes.c_void_p * len(imgs))(*[t.data_ptr() for t in imgs])
+        stream = torch.cuda.current_stream(device).cuda_stream
+        trainer = _acquire()
+        try:
+            check(lib.aniso_b200_train_batch_forward(trainer._h, params, S, vs, cams, len(cameras),
+                                                     ctypes.byref(options.c()), ptrs, ctypes.c_void_p(stream)))
+        except Exception:
+            _release(trainer)
+            raise
+        if any(ctx.needs_input_grad[1:]):
+            ctx.trainer = trainer
+        else:
+            ctx.trainer = None
+            _release(trainer)
+        ctx.n_scenes = S
+        ctx.save_for_backward(*tensors)
+        return tuple(imgs)
+
+    @staticmethod
+    def backward(ctx, *grad_imgs):
+        tensors = ctx.saved_tensors
+        S = ctx.n_scenes
+        grads = [torch.zeros_like(t) for t in tensors]
+        g = (_lib.RawGrads * S)(*[_lib.RawGrads(*[t.data_ptr() for t in grads[5 * s:5 * s + 5]]) for s in range(S)])
+        # Views outside the loss arrive as zero images (autograd materialises unused outputs' grads).
+        gi = [gimg.contiguous().float() for gimg in grad_imgs]
+        ptrs = (ctypes.c_void_p * len(gi))(*[t.data_ptr() for t in gi])
+        stream = torch.cuda.current_stream(tensors[0].device).cuda_stream
+        trainer = ctx.trainer
+        try:
+            check(lib.aniso_b200_train_batch_backward(trainer._h, ptrs, g, ctypes.c_void_p(stream)))
+        finally:
+            ctx.trainer = None
+            _release(trainer)
+        return (None, *grads)
+
+
+def rasterize_batch(scenes, cameras, view_scene, sh_degree: int = 3, splat_scale: float = 1.0,
+                    tile: tuple[int, int] = (16, 16), blend_batch: int = 256):
+    """Differentiable render of many views of several scenes in one forward/backward.
+
+    scenes: a list of (means, log_scales, quats, opacity_logits, sh) tuples; view k shows scene
+    view_scene[k] (the views of a scene consecutive). Returns one (H, W, 3) image per view. The
+    gradient of a scene is the sum over its views, added in view order (deterministic).
+    """
+    flat = [t for s in scenes for t in s]
+    opts = BatchOptions(sh_degree, splat_scale, tuple(tile), blend_batch, False)
+    return RasterizeBatchFunction.apply((list(cameras), [int(v) for v in view_scene], opts), *flat)

@@ -1,8 +1,8 @@
 // The adjoint of the rasterizer (no counterpart in the reference, which has no backward pass; the
 // forward it differentiates is render.cpp:39-104 / 195-220 on the GPU path's lists).
 //
-// blend_backward: one 128-thread block per 16x16 tile, the forward's pixel layout (8x8 per warp,
-//   two pixels per lane). Each pixel walks its tile list back to front from its last applied
+// blend_backward: one block per tile of a batch, the forward's pixel layout (8x8 per warp, two
+//   pixels per lane). Each pixel walks its tile list back to front from its last applied
 //   splat, replaying the forward's alpha tests bit for bit (same record, same exponent code) and
 //   recovering the transmittance in front of each splat by division (T_j = T_{j+1} / (1 - a_j));
 //   nothing per pixel is stored but the final T and the last contributor. Per splat, the gradient
@@ -10,18 +10,19 @@
 //   warp (12 shuffles for the 9 values), summed over the four warps in a fixed order, and written
 //   to the pair's slot in the depth-ordered pair list -- no atomics, so the result does not depend
 //   on scheduling.
-// gauss_backward: one thread per visible Gaussian (depth order) sums its pairs' slots, which are
-//   contiguous and summed in list order, and applies the chain rule through the record
+// gauss_backward: one launch per view, one thread per Gaussian of its scene; a Gaussian visible in
+//   the view sums its pairs' slots, which are contiguous and summed in list order, applies the
+//   chain rule through the record
 //   (conic, log2 opacity, SH colour), the EWA projection (2D covariance, clamped Jacobian, camera
 //   transform), the 3D covariance M M^T with M = R(q) diag(s), and the activations (exp, sigmoid,
-//   quaternion normalisation) to the 59 raw parameters.
+//   quaternion normalisation) to the 59 raw parameters, and adds them to the scene's gradients.
+//   Views are launched one after another, so the sum over views also runs in a fixed order.
 #include "common.cuh"
 #include "kernels.h"
 
 namespace ab2 {
 namespace {
 
-constexpr int kThreads = 128;
 constexpr int kBatch = 128;
 constexpr int kG = 9;
 constexpr float kLn2 = 0.69314718055994530942f;
@@ -98,40 +99,48 @@ __device__ __forceinline__ void pixel_step(PixelState& s, unsigned pos, float p,
     g[5] += dp;
 }
 
-__global__ void __launch_bounds__(kThreads) blend_backward_kernel(BackwardIn in, float* __restrict__ grad_pair) {
+template <int TW, int TH>
+__global__ void __launch_bounds__(TW * TH / 2) blend_backward_kernel(BackwardIn in, float* __restrict__ grad_pair) {
+    constexpr int kThreads = TW * TH / 2;
+    constexpr int kWarps = kThreads / 32;
+    constexpr int kWarpsX = TW / 8;
     __shared__ float4 s_r0[kBatch];
     __shared__ float4 s_r1[kBatch];
     __shared__ float s_b[kBatch];
     __shared__ unsigned s_pos[kBatch];
     __shared__ unsigned char s_mask[kBatch];
     __shared__ unsigned s_hit[kBatch];
-    __shared__ float s_grad[4][kBatch][kG];
+    __shared__ float s_grad[kWarps][kBatch][kG];
     __shared__ unsigned s_maxlast;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tile = blockIdx.x;
-    const int tx = tile % in.tiles_x, ty = tile / in.tiles_x;
-    const int ox = tx * kTile, oy = ty * kTile;
-    const int x0 = ox + (warp & 1) * 8 + 2 * (lane & 3), y = oy + (warp >> 1) * 8 + (lane >> 2);
+    const unsigned gtile = blockIdx.x;
+    const unsigned v = find_segment(in.tables.tile_base, in.tables.n_views, gtile);
+    const ViewInfo& vi = in.views[v];
+    const unsigned local = gtile - vi.tile_base;
+    const int tx = static_cast<int>(local % vi.cam.tilesX), ty = static_cast<int>(local / vi.cam.tilesX);
+    const int ox = tx * TW, oy = ty * TH;
+    const int x0 = ox + (warp % kWarpsX) * 8 + 2 * (lane & 3), y = oy + (warp / kWarpsX) * 8 + (lane >> 2);
+    const int width = vi.cam.width, height = vi.cam.height;
     const float px0 = x0 + 0.5f, py = y + 0.5f;
-    const uint2 range = (in.ctrl->flags & kFlagOverflow) ? make_uint2(0, 0) : in.ranges[tile];
+    const uint2 range = (in.ctrl->flags & kFlagOverflow) ? make_uint2(0, 0) : in.ranges[gtile];
 
     PixelState s0{1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, range.x}, s1{1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, range.x};
-    if (x0 < in.width && y < in.height) {
-        const size_t p = static_cast<size_t>(y) * in.width + x0;
-        s0.T = in.t_final[p];
-        s0.last = in.n_contrib[p];
-        s0.gr = in.grad_img[3 * p];
-        s0.gg = in.grad_img[3 * p + 1];
-        s0.gb = in.grad_img[3 * p + 2];
+    if (x0 < width && y < height) {
+        const size_t p = static_cast<size_t>(y) * width + x0;
+        s0.T = vi.t_final[p];
+        s0.last = vi.n_contrib[p];
+        s0.gr = vi.grad_img[3 * p];
+        s0.gg = vi.grad_img[3 * p + 1];
+        s0.gb = vi.grad_img[3 * p + 2];
     }
-    if (x0 + 1 < in.width && y < in.height) {
-        const size_t p = static_cast<size_t>(y) * in.width + x0 + 1;
-        s1.T = in.t_final[p];
-        s1.last = in.n_contrib[p];
-        s1.gr = in.grad_img[3 * p];
-        s1.gg = in.grad_img[3 * p + 1];
-        s1.gb = in.grad_img[3 * p + 2];
+    if (x0 + 1 < width && y < height) {
+        const size_t p = static_cast<size_t>(y) * width + x0 + 1;
+        s1.T = vi.t_final[p];
+        s1.last = vi.n_contrib[p];
+        s1.gr = vi.grad_img[3 * p];
+        s1.gg = vi.grad_img[3 * p + 1];
+        s1.gb = vi.grad_img[3 * p + 2];
     }
     if (tid == 0) s_maxlast = range.x;
     __syncthreads();
@@ -168,11 +177,13 @@ __global__ void __launch_bounds__(kThreads) blend_backward_kernel(BackwardIn in,
             s_b[slot] = r.r2.x;
             const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
             const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
-            const unsigned cols =
-                (overlaps(xlo, xhi, ox, ox + 7) ? 1u : 0u) | (overlaps(xlo, xhi, ox + 8, ox + 15) ? 2u : 0u);
-            unsigned m = 0;
-            if (overlaps(ylo, yhi, oy, oy + 7)) m |= cols;
-            if (overlaps(ylo, yhi, oy + 8, oy + 15)) m |= cols << 2;
+            unsigned cols = 0, m = 0;
+#pragma unroll
+            for (int c = 0; c < kWarpsX; ++c)
+                if (overlaps(xlo, xhi, ox + 8 * c, ox + 8 * c + 7)) cols |= 1u << c;
+#pragma unroll
+            for (int rr = 0; rr < TH / 8; ++rr)
+                if (overlaps(ylo, yhi, oy + 8 * rr, oy + 8 * rr + 7)) m |= cols << (kWarpsX * rr);
             s_mask[slot] = static_cast<unsigned char>(m);
             s_hit[slot] = 0;
             const unsigned j = in.rank[g];
@@ -215,7 +226,7 @@ __global__ void __launch_bounds__(kThreads) blend_backward_kernel(BackwardIn in,
 #pragma unroll
             for (int k = 0; k < kG; ++k) acc[k] = 0.f;
 #pragma unroll
-            for (int w = 0; w < 4; ++w)
+            for (int w = 0; w < kWarps; ++w)
                 if (hit & (1u << w))
 #pragma unroll
                     for (int k = 0; k < kG; ++k) acc[k] += s_grad[w][slot][k];
@@ -229,6 +240,10 @@ __global__ void __launch_bounds__(kThreads) blend_backward_kernel(BackwardIn in,
 }
 
 // SH basis (sh.cpp:18-58 order) and its derivatives along x, y, z, for degree D.
+// Adds one view's gradient to the caller's buffer. The add is rounded on its own (never fused with
+// the product that formed v), so accumulating views here equals summing per-view gradients.
+__device__ __forceinline__ void accumulate(float* p, float v) { *p = __fadd_rn(*p, v); }
+
 template <int D>
 __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16], float bx[16], float by[16],
                                          float bz[16]) {
@@ -269,15 +284,18 @@ __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16],
 }
 
 template <int D>
-__global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamParams cam, const Ctrl* ctrl,
-                                                             const unsigned* __restrict__ sorted_idx,
+__global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamParams cam, unsigned entry_base,
+                                                             const Ctrl* ctrl, const unsigned* __restrict__ depth_key,
+                                                             const unsigned* __restrict__ rank,
                                                              const unsigned* __restrict__ offs,
                                                              const unsigned long long* __restrict__ rect_sorted,
                                                              const float* __restrict__ grad_pair, RawGrads out) {
-    const unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
-    if (j >= ctrl->vis_count) return;
-    const unsigned i = sorted_idx[j];
+    if (i >= raw.n) return;
+    const unsigned e = entry_base + static_cast<unsigned>(i);
+    if (depth_key[e] == kCulledKey) return;  // culled in this view: no gradient from it
+    const unsigned j = rank[e];
     const unsigned long long rc = rect_sorted[j];
     const unsigned cnt = ((rc >> 32 & 0xFFFFu) - (rc & 0xFFFFu) + 1) * ((rc >> 48) - (rc >> 16 & 0xFFFFu) + 1);
     float g9[kG] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -365,7 +383,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
             const float gc = pre > 0.f ? grgb[ch] : 0.f;  // rgb = max(0, pre)
 #pragma unroll
             for (int k = 0; k < count; ++k) {
-                gsh[k * 3 + ch] = bs[k] * gc;
+                accumulate(&gsh[k * 3 + ch], bs[k] * gc);
                 gdir[0] += shv[k * 3 + ch] * bxs[k] * gc;
                 gdir[1] += shv[k * 3 + ch] * bys[k] * gc;
                 gdir[2] += shv[k * 3 + ch] * bzs[k] * gc;
@@ -376,7 +394,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
         gm[1] += (gdir[1] - uy * dd) / len;
         gm[2] += (gdir[2] - uz * dd) / len;
     }
-    out.logits[i] = go * o * (1.0f - o);
+    accumulate(&out.logits[i], go * o * (1.0f - o));
 
     // ---- conic (A, B, C) = (c, -b, a) / det -> 2D covariance (a, b, c) ----
     const float id2 = 1.0f / (det * det);
@@ -423,9 +441,9 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
     gm[0] += W[0] * gpx + W[3] * gpy + W[6] * gpz;
     gm[1] += W[1] * gpx + W[4] * gpy + W[7] * gpz;
     gm[2] += W[2] * gpx + W[5] * gpy + W[8] * gpz;
-    out.means[3 * i] = gm[0];
-    out.means[3 * i + 1] = gm[1];
-    out.means[3 * i + 2] = gm[2];
+    accumulate(&out.means[3 * i], gm[0]);
+    accumulate(&out.means[3 * i + 1], gm[1]);
+    accumulate(&out.means[3 * i + 2], gm[2]);
 
     // ---- S = M M^T -> M = R(q) diag(s) -> s, R(q) ----
     float gM[3][3];
@@ -443,7 +461,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
             gR[r][k] = gM[r][k] * s[k];
             gs += gM[r][k] * Rq[r][k];
         }
-        out.log_scales[3 * i + k] = gs * s[k];  // s = exp(log s) * splat_scale
+        accumulate(&out.log_scales[3 * i + k], gs * s[k]);  // s = exp(log s) * splat_scale
     }
     const float gqw = 2.0f * (-qz * gR[0][1] + qy * gR[0][2] + qz * gR[1][0] - qx * gR[1][2] - qy * gR[2][0] + qx * gR[2][1]);
     const float gqx = 2.0f * (qy * gR[0][1] + qz * gR[0][2] + qy * gR[1][0] - 2.0f * qx * gR[1][1] - qw * gR[1][2] +
@@ -455,30 +473,33 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
     // q_n = q / |q|
     const float dq = qw * gqw + qx * gqx + qy * gqy + qz * gqz;
     const float il = qlen > 0 ? 1.0f / qlen : 0.f;
-    out.quats[4 * i] = (gqw - qw * dq) * il;
-    out.quats[4 * i + 1] = (gqx - qx * dq) * il;
-    out.quats[4 * i + 2] = (gqy - qy * dq) * il;
-    out.quats[4 * i + 3] = (gqz - qz * dq) * il;
+    accumulate(&out.quats[4 * i], (gqw - qw * dq) * il);
+    accumulate(&out.quats[4 * i + 1], (gqx - qx * dq) * il);
+    accumulate(&out.quats[4 * i + 2], (gqy - qy * dq) * il);
+    accumulate(&out.quats[4 * i + 3], (gqz - qz * dq) * il);
 }
 
 }  // namespace
 
-void launch_blend_backward(const BackwardIn& in, int tiles_y, float* grad_pair, cudaStream_t stream) {
-    const unsigned blocks = static_cast<unsigned>(in.tiles_x) * static_cast<unsigned>(tiles_y);
-    if (blocks == 0) return;
-    blend_backward_kernel<<<blocks, kThreads, 0, stream>>>(in, grad_pair);
+void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int tile_h, float* grad_pair,
+                           cudaStream_t stream) {
+    if (tiles == 0) return;
+    if (tile_w == 8) blend_backward_kernel<8, 8><<<tiles, 32, 0, stream>>>(in, grad_pair);
+    else if (tile_h == 32) blend_backward_kernel<16, 32><<<tiles, 256, 0, stream>>>(in, grad_pair);
+    else blend_backward_kernel<16, 16><<<tiles, 128, 0, stream>>>(in, grad_pair);
 }
 
-void launch_gauss_backward(const RawParams& raw, const CamParams& cam, const Ctrl* ctrl, const unsigned* sorted_idx,
-                           const unsigned* offs, const unsigned long long* rect_sorted, const float* grad_pair,
-                           unsigned max_visible, const RawGrads& out, cudaStream_t stream) {
-    const unsigned blocks = (max_visible + 127) / 128;
+void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
+                           const unsigned* depth_key, const unsigned* rank, const unsigned* offs,
+                           const unsigned long long* rect_sorted, const float* grad_pair, const RawGrads& out,
+                           cudaStream_t stream) {
+    const unsigned blocks = static_cast<unsigned>((raw.n + 127) / 128);
     if (blocks == 0) return;
     switch (cam.shDegree) {
-        case 0: gauss_backward_kernel<0><<<blocks, 128, 0, stream>>>(raw, cam, ctrl, sorted_idx, offs, rect_sorted, grad_pair, out); break;
-        case 1: gauss_backward_kernel<1><<<blocks, 128, 0, stream>>>(raw, cam, ctrl, sorted_idx, offs, rect_sorted, grad_pair, out); break;
-        case 2: gauss_backward_kernel<2><<<blocks, 128, 0, stream>>>(raw, cam, ctrl, sorted_idx, offs, rect_sorted, grad_pair, out); break;
-        default: gauss_backward_kernel<3><<<blocks, 128, 0, stream>>>(raw, cam, ctrl, sorted_idx, offs, rect_sorted, grad_pair, out); break;
+        case 0: gauss_backward_kernel<0><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, depth_key, rank, offs, rect_sorted, grad_pair, out); break;
+        case 1: gauss_backward_kernel<1><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, depth_key, rank, offs, rect_sorted, grad_pair, out); break;
+        case 2: gauss_backward_kernel<2><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, depth_key, rank, offs, rect_sorted, grad_pair, out); break;
+        default: gauss_backward_kernel<3><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, depth_key, rank, offs, rect_sorted, grad_pair, out); break;
     }
 }
 

@@ -1,4 +1,5 @@
-// Step 5 of the rasterizer: front-to-back blending, one 128-thread block per 16x16 tile.
+// Step 5 of the rasterizer: front-to-back blending, one block per tile of a batch (any view),
+// for tile shapes TW x TH of 8x8, 16x16 (the reference's) and 16x32 pixels.
 //
 // Per pixel this is the blend of render.cpp:195-220 / gpu_render.cu:180-233:
 //   power = -(A dx^2 + C dy^2)/2 - B dx dy; skip if power > 0
@@ -10,22 +11,20 @@
 //   * each warp owns one 8x8 pixel block -- exactly one tile of the CPU renderer -- with two
 //     horizontally adjacent pixels per lane; the row terms of the exponent (with log2(opacity)
 //     folded in) are shared, so each pixel's exponent is two FMAs;
-//   * the block stages 256 splat records per round in shared memory and, per splat, a 4-bit mask
-//     of the warp blocks it can touch: its pixel bounds (the CPU 8x8-tile rectangle cut by the
+//   * the block stages kBatch splat records per round in shared memory and, per splat, a mask of
+//     the warp blocks it can touch: its pixel bounds (the CPU 8x8-tile rectangle cut by the
 //     ellipse where alpha can reach 1/255, with a margin) against each 8x8 block. The 8x8 part
-//     gives every pixel exactly the splat list of the CPU renderer; the ellipse part only drops
-//     splats that cannot pass the alpha test anywhere in the block, so it changes no result;
+//     gives every pixel exactly the splat list of the CPU renderer whatever the tile shape (so the
+//     image does not depend on it); the ellipse part only drops splats that cannot pass the alpha
+//     test anywhere in the block, so it changes no result;
 //   * each warp walks only its set bits (ballot + ffs); a finished pixel holds T = 0 (T >= 1e-4
 //     while it is not finished), so no separate flag is carried; the warp leaves once all 64
-//     pixels are finished and the block stops loading once all four warps have (__syncthreads_or).
+//     pixels are finished and the block stops loading once all its warps have (__syncthreads_or).
 #include "common.cuh"
 #include "kernels.h"
 
 namespace ab2 {
 namespace {
-
-constexpr int kThreads = 128;
-constexpr int kBatch = 256;
 
 __device__ __forceinline__ bool overlaps(int lo, int hi, int a, int b) { return lo <= b && hi >= a; }
 
@@ -58,42 +57,49 @@ __device__ __forceinline__ void blend_px(float p, float L, float r, float g, flo
 }
 
 template <bool kTrain>
-__device__ __forceinline__ void store_px(const BlendOut& out, int x, int y, int width, int height, float tfin, float cr,
-                                         float cg, float cb, unsigned last) {
-    if (x >= width || y >= height) return;
+__device__ __forceinline__ void store_px(const ViewInfo& vi, int x, int y, float tfin, float cr, float cg, float cb,
+                                         unsigned last) {
+    const int width = vi.cam.width;
+    if (x >= width || y >= vi.cam.height) return;
     const size_t p = static_cast<size_t>(y) * width + x;
-    if (out.rgb8) {
-        uint8_t* o = out.rgb8 + p * 3;
+    if (vi.rgb8) {
+        uint8_t* o = vi.rgb8 + p * 3;
         o[0] = static_cast<uint8_t>(fminf(fmaxf(cr, 0.f), 1.f) * 255.f + 0.5f);
         o[1] = static_cast<uint8_t>(fminf(fmaxf(cg, 0.f), 1.f) * 255.f + 0.5f);
         o[2] = static_cast<uint8_t>(fminf(fmaxf(cb, 0.f), 1.f) * 255.f + 0.5f);
     }
     if (kTrain) {
-        out.rgbf[p * 3 + 0] = cr;
-        out.rgbf[p * 3 + 1] = cg;
-        out.rgbf[p * 3 + 2] = cb;
-        out.t_final[p] = tfin;
-        out.n_contrib[p] = last;
+        vi.rgbf[p * 3 + 0] = cr;
+        vi.rgbf[p * 3 + 1] = cg;
+        vi.rgbf[p * 3 + 2] = cb;
+        vi.t_final[p] = tfin;
+        vi.n_contrib[p] = last;
     }
 }
 
-template <bool kTrain>
-__global__ void __launch_bounds__(kThreads) blend_kernel(const uint2* __restrict__ ranges,
-                                                         const unsigned* __restrict__ vals,
-                                                         const SplatRecord* __restrict__ rec, const Ctrl* ctrl,
-                                                         int width, int height, int tiles_x, BlendOut out) {
+template <int TW, int TH, int kBatch, bool kTrain>
+__global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restrict__ ranges,
+                                                            const unsigned* __restrict__ vals,
+                                                            const SplatRecord* __restrict__ rec, const Ctrl* ctrl,
+                                                            const ViewInfo* __restrict__ views, BatchTables tables) {
+    constexpr int kThreads = TW * TH / 2;  // two pixels per lane
+    constexpr int kWarpsX = TW / 8;
     __shared__ float4 s_r0[kBatch];
     __shared__ float4 s_r1[kBatch];
     __shared__ float s_b[kBatch];
     __shared__ unsigned char s_mask[kBatch];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tile = blockIdx.x;
-    const int tx = tile % tiles_x, ty = tile / tiles_x;
-    const int ox = tx * kTile, oy = ty * kTile;
-    const int x0 = ox + (warp & 1) * 8 + 2 * (lane & 3), y = oy + (warp >> 1) * 8 + (lane >> 2);
+    const unsigned gtile = blockIdx.x;
+    const unsigned v = find_segment(tables.tile_base, tables.n_views, gtile);
+    const ViewInfo& vi = views[v];
+    const int tiles_x = vi.cam.tilesX;
+    const unsigned local = gtile - vi.tile_base;
+    const int ox = static_cast<int>(local % tiles_x) * TW, oy = static_cast<int>(local / tiles_x) * TH;
+    const int x0 = ox + (warp % kWarpsX) * 8 + 2 * (lane & 3), y = oy + (warp / kWarpsX) * 8 + (lane >> 2);
+    const int width = vi.cam.width, height = vi.cam.height;
     const float px0 = x0 + 0.5f, py = y + 0.5f;
-    const uint2 range = (ctrl->flags & kFlagOverflow) ? make_uint2(0, 0) : ranges[tile];
+    const uint2 range = (ctrl->flags & kFlagOverflow) ? make_uint2(0, 0) : ranges[gtile];
 
     // Pixels outside the image start finished.
     float T0 = (x0 < width && y < height) ? 1.0f : 0.f;
@@ -116,10 +122,13 @@ __global__ void __launch_bounds__(kThreads) blend_kernel(const uint2* __restrict
                 s_b[slot] = r.r2.x;
                 const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
                 const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
-                const unsigned cols =
-                    (overlaps(xlo, xhi, ox, ox + 7) ? 1u : 0u) | (overlaps(xlo, xhi, ox + 8, ox + 15) ? 2u : 0u);
-                if (overlaps(ylo, yhi, oy, oy + 7)) m |= cols;
-                if (overlaps(ylo, yhi, oy + 8, oy + 15)) m |= cols << 2;
+                unsigned cols = 0;
+#pragma unroll
+                for (int c = 0; c < kWarpsX; ++c)
+                    if (overlaps(xlo, xhi, ox + 8 * c, ox + 8 * c + 7)) cols |= 1u << c;
+#pragma unroll
+                for (int rr = 0; rr < TH / 8; ++rr)
+                    if (overlaps(ylo, yhi, oy + 8 * rr, oy + 8 * rr + 7)) m |= cols << (kWarpsX * rr);
             }
             s_mask[slot] = static_cast<unsigned char>(m);
         }
@@ -152,20 +161,40 @@ __global__ void __launch_bounds__(kThreads) blend_kernel(const uint2* __restrict
             }
         }
     }
-    store_px<kTrain>(out, x0, y, width, height, tf0, r0, g0, b0c, last0);
-    store_px<kTrain>(out, x0 + 1, y, width, height, tf1, r1, g1, b1c, last1);
+    store_px<kTrain>(vi, x0, y, tf0, r0, g0, b0c, last0);
+    store_px<kTrain>(vi, x0 + 1, y, tf1, r1, g1, b1c, last1);
+}
+
+template <int TW, int TH, int kBatch>
+void launch_shape(unsigned tiles, const uint2* ranges, const unsigned* vals, const SplatRecord* rec, const Ctrl* ctrl,
+                  const ViewInfo* views, const BatchTables& tables, bool train, cudaStream_t stream) {
+    if (train)
+        blend_kernel<TW, TH, kBatch, true><<<tiles, TW * TH / 2, 0, stream>>>(ranges, vals, rec, ctrl, views, tables);
+    else
+        blend_kernel<TW, TH, kBatch, false><<<tiles, TW * TH / 2, 0, stream>>>(ranges, vals, rec, ctrl, views, tables);
 }
 
 }  // namespace
 
-void launch_blend(const uint2* ranges, const unsigned* sorted_vals, const SplatRecord* rec, const Ctrl* ctrl,
-                  int width, int height, int tiles_x, int tiles_y, const BlendOut& out, cudaStream_t stream) {
-    const unsigned blocks = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
-    if (blocks == 0) return;
-    if (out.rgbf)
-        blend_kernel<true><<<blocks, kThreads, 0, stream>>>(ranges, sorted_vals, rec, ctrl, width, height, tiles_x, out);
-    else
-        blend_kernel<false><<<blocks, kThreads, 0, stream>>>(ranges, sorted_vals, rec, ctrl, width, height, tiles_x, out);
+bool blend_shape_supported(int tile_w, int tile_h) {
+    return (tile_w == 8 && tile_h == 8) || (tile_w == 16 && tile_h == 16) || (tile_w == 16 && tile_h == 32);
+}
+
+void launch_blend(unsigned tiles, const uint2* ranges, const unsigned* sorted_vals, const SplatRecord* rec,
+                  const Ctrl* ctrl, const ViewInfo* views, const BatchTables& tables, int tile_w, int tile_h,
+                  int batch, bool train, cudaStream_t stream) {
+    if (tiles == 0) return;
+    const bool big = batch >= 256;
+    if (tile_w == 8) {
+        if (big) launch_shape<8, 8, 256>(tiles, ranges, sorted_vals, rec, ctrl, views, tables, train, stream);
+        else launch_shape<8, 8, 128>(tiles, ranges, sorted_vals, rec, ctrl, views, tables, train, stream);
+    } else if (tile_h == 32) {
+        if (big) launch_shape<16, 32, 512>(tiles, ranges, sorted_vals, rec, ctrl, views, tables, train, stream);
+        else launch_shape<16, 32, 256>(tiles, ranges, sorted_vals, rec, ctrl, views, tables, train, stream);
+    } else {
+        if (big) launch_shape<16, 16, 256>(tiles, ranges, sorted_vals, rec, ctrl, views, tables, train, stream);
+        else launch_shape<16, 16, 128>(tiles, ranges, sorted_vals, rec, ctrl, views, tables, train, stream);
+    }
 }
 
 }  // namespace ab2

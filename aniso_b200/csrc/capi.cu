@@ -1,11 +1,12 @@
-// The C ABI (include/aniso_b200.h): scene upload, per-frame work buffers, the frame pipeline.
+// The C ABI (include/aniso_b200.h): scenes, batches, the differentiable path.
 //
-// A frame is a fixed, host-sync-free sequence of launches on one stream (capturable in a CUDA
-// graph): frame_begin, preprocess (+compaction), 4 depth onesweep passes, pair scan, pair
-// expansion, 1-4 tile onesweep passes, tile ranges, blend. Data-dependent sizes (visible count V, pair count P) stay
-// on the device; grids are sized for capacity and surplus blocks exit at once. The reference
-// instead reads P back mid-frame (gpu_render.cu:329) to size its buffers; here a frame whose P
-// exceeds the pair capacity sets an overflow flag instead of writing, and the host grows the
+// Everything renders through one plan: V views of S scenes. A frame is a fixed, host-sync-free
+// sequence of launches on one stream (capturable in a CUDA graph): upload of the plan's view
+// table, frame_begin, preprocess, 4 depth onesweep passes, pair scan, pair expansion, 1-4 tile
+// onesweep passes, tile ranges, blend. Data-dependent sizes (visible entries, pairs) stay on the
+// device; grids are sized for capacity and surplus blocks exit at once. The reference instead reads
+// the pair count back mid-frame (gpu_render.cu:329) to size its buffers; here a frame whose pairs
+// exceed the capacity sets an overflow flag instead of writing them, and the host grows the
 // buffers and renders it again.
 #include "aniso_b200.h"
 #include "common.cuh"
@@ -55,6 +56,10 @@ struct DevBuf {
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), cap(o.cap) {
+        o.p = nullptr;
+        o.cap = 0;
+    }
     ~DevBuf() { release(); }
     void release() {
         if (p) cudaFree(p);
@@ -80,7 +85,10 @@ int bits_for(uint32_t v) {  // bits needed to hold v
     return b;
 }
 
-// Work buffers of one frame at a time, sized for N Gaussians and a pair capacity.
+constexpr uint64_t kMaxEntries = 0xFFFFFFFFull;  // entry and tile indices are 32-bit
+constexpr uint64_t kMaxPairs = 0x3FFFFFFFull;    // look-back status values are 32-bit; keep headroom
+
+// Work buffers of one frame at a time, sized for `n` entries and a pair capacity.
 struct Arena {
     int64_t n = -1;
     unsigned pair_cap = 0;
@@ -95,7 +103,6 @@ struct Arena {
     DevBuf<uint2> ranges;
     DevBuf<Ctrl> ctrl;
     DevBuf<unsigned long long> st_depth, st_dup, st_tile;
-    DevBuf<uint8_t> image;
 
     unsigned depth_chunks() const { return chunks_of(static_cast<uint64_t>(std::max<int64_t>(n, 1)), onesweep_chunk_items()); }
     unsigned tile_chunks() const { return chunks_of(std::max(pair_cap, 1u), onesweep_chunk_items()); }
@@ -121,6 +128,16 @@ struct Arena {
         return grow_pairs(cap);
     }
 
+    // Makes room for at least `entries` entries (re-initialising when it grows).
+    int ensure(int64_t entries) {
+        if (n >= entries) return 0;
+        const uint64_t cap = std::max<uint64_t>(
+            std::max<uint64_t>(1u << 20, 2ull * static_cast<uint64_t>(entries)), pair_cap);
+        this->~Arena();
+        new (this) Arena();
+        return init(entries, static_cast<unsigned>(std::min<uint64_t>(cap, kMaxPairs)));
+    }
+
     int grow_pairs(unsigned cap) {
         if (cap <= pair_cap && pair_key[0].p) return 0;
         for (int k = 0; k < 2; ++k) {
@@ -144,24 +161,25 @@ struct Arena {
     }
 };
 
-// Depth passes (the first one compacts the visible Gaussians out of depth_key), pair scan and
-// expansion, tile passes and ranges. Returns the buffer index holding the final sorted pairs.
-int enqueue_sort(Arena& A, int tiles_x, int tiles_y, cudaStream_t st, int* final_buf) {
+// Depth passes over `entries` depth keys (the first compacts the visible ones), pair scan and
+// expansion, tile passes over `tiles` global tiles, and ranges. *final_buf = the pair buffer that
+// holds the sorted pairs.
+int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, cudaStream_t st,
+                 int* final_buf) {
     Ctrl* ctrl = A.ctrl.p;
-    const unsigned nmax = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
+    const unsigned cap = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
     for (int p = 0; p < kMaxPasses; ++p) {
         const int src = (p + 1) & 1, dst = p & 1;  // pass 0 reads depth_key and writes buffer 0
         launch_onesweep(p == 0 ? A.depth_key.p : A.vis_key[src].p, p == 0 ? nullptr : A.vis_idx[src].p,
-                        p == kMaxPasses - 1 ? nullptr : A.vis_key[dst].p, A.vis_idx[dst].p, p == 0 ? nmax : 0u, nmax,
-                        p * kRadixBits, &ctrl->depth_hist[p * kRadix],
+                        p == kMaxPasses - 1 ? nullptr : A.vis_key[dst].p, A.vis_idx[dst].p, p == 0 ? entries : 0u,
+                        p == 0 ? entries : cap, p * kRadixBits, &ctrl->depth_hist[p * kRadix],
                         A.st_depth.p + static_cast<size_t>(p) * A.depth_chunks() * kRadix,
                         &ctrl->chunk_ctr[kCtrDepth0 + p], ctrl, st);
     }
-    const int sorted = A.sorted_buf();
-    const unsigned tiles = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
+    const int sorted = Arena::sorted_buf();
     const int tile_passes = std::max(1, (bits_for(tiles - 1) + kRadixBits - 1) / kRadixBits);
     const DupBuffers dup{A.offs.p, A.rank.p, A.rect_sorted.p, A.chunk_start.p};
-    launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, nmax, tiles_x, tile_passes, dup,
+    launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, tile_passes, dup,
                      A.pair_key[0].p, A.pair_val[0].p, A.st_dup.p, st);
     for (int p = 0; p < tile_passes; ++p) {
         const int src = p & 1, dst = src ^ 1;
@@ -178,14 +196,282 @@ int enqueue_sort(Arena& A, int tiles_x, int tiles_y, cudaStream_t st, int* final
     return 0;
 }
 
+// The per-view constants, packed as gpu_render.cu:301-316 packs them (doubles cast to float; the
+// eye is Camera::centre(), camera.cpp:19-23, computed in double); tiles in the plan's shape.
+int pack_camera(int scene_degree, int rendered_degree, const aniso_b200_camera* c, float splat_scale, int tile_w,
+                int tile_h, CamParams& cp) {
+    if (!c) return fail(ANISO_B200_ERR_ARGUMENT, "camera is NULL");
+    if (c->width <= 0 || c->height <= 0 || c->width > 32767 || c->height > 32767)
+        return fail(ANISO_B200_ERR_ARGUMENT, "camera size must be in [1, 32767]");
+    std::memset(&cp, 0, sizeof cp);
+    for (int r = 0; r < 3; ++r) {
+        for (int k = 0; k < 3; ++k) cp.R[r * 3 + k] = static_cast<float>(c->R[r * 3 + k]);
+        cp.t[r] = static_cast<float>(c->t[r]);
+    }
+    const double* R = c->R;
+    const double* t = c->t;
+    cp.eye[0] = static_cast<float>(-(R[0] * t[0] + R[3] * t[1] + R[6] * t[2]));
+    cp.eye[1] = static_cast<float>(-(R[1] * t[0] + R[4] * t[1] + R[7] * t[2]));
+    cp.eye[2] = static_cast<float>(-(R[2] * t[0] + R[5] * t[1] + R[8] * t[2]));
+    cp.fx = static_cast<float>(c->fx);
+    cp.fy = static_cast<float>(c->fy);
+    cp.cx = static_cast<float>(c->cx);
+    cp.cy = static_cast<float>(c->cy);
+    cp.width = c->width;
+    cp.height = c->height;
+    cp.tilesX = (c->width + tile_w - 1) / tile_w;
+    cp.tilesY = (c->height + tile_h - 1) / tile_h;
+    cp.shDegree = rendered_degree;
+    cp.shCoeffs = (scene_degree + 1) * (scene_degree + 1);
+    cp.splatScale = splat_scale;
+    return 0;
+}
+
+// ---- plans ---------------------------------------------------------------------------------
+
+struct PlanShape {
+    int tile_w = kTile, tile_h = kTile, blend_batch = 256, sh_degree = 3;
+    float splat_scale = 1.0f;
+};
+
+int check_options(const aniso_b200_batch_options* o, PlanShape& shape) {
+    if (!o) return 0;
+    shape.sh_degree = o->sh_degree;
+    shape.splat_scale = o->splat_scale;
+    shape.tile_w = o->tile_w ? o->tile_w : kTile;
+    shape.tile_h = o->tile_h ? o->tile_h : kTile;
+    shape.blend_batch = o->blend_batch ? o->blend_batch : 256;
+    if (shape.sh_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
+    if (!blend_shape_supported(shape.tile_w, shape.tile_h))
+        return fail(ANISO_B200_ERR_ARGUMENT, "tile shape must be 8x8, 16x16 or 16x32");
+    return 0;
+}
+
+// V views of S scenes: host tables, uploaded as one blob to a slot before each frame.
+template <class Src>
+struct Plan {
+    PlanShape shape;
+    std::vector<ViewInfo> views;
+    std::vector<BatchScene<Src>> scenes;
+    std::vector<unsigned> entry_base, tile_base, tiles_x;
+    uint64_t entries = 0, tiles = 0;
+    unsigned pre_blocks = 0;
+
+    // srcs[s], stored degree deg[s]; view k of scene view_scene[k] (consecutive per scene).
+    int build(const std::vector<Src>& srcs, const std::vector<int>& deg, const int32_t* view_scene, int n_views,
+              const aniso_b200_camera* cameras, const PlanShape& sh) {
+        shape = sh;
+        const int S = static_cast<int>(srcs.size());
+        if (S <= 0 || n_views <= 0 || !view_scene || !cameras)
+            return fail(ANISO_B200_ERR_ARGUMENT, "a batch needs at least one scene and one view");
+        int rendered = std::min(sh.sh_degree, 3);
+        for (int s = 0; s < S; ++s) rendered = std::min(rendered, deg[s]);
+        views.assign(n_views, ViewInfo{});
+        scenes.assign(S, BatchScene<Src>{});
+        entry_base.assign(n_views, 0);
+        tile_base.assign(n_views, 0);
+        tiles_x.assign(n_views, 0);
+        std::vector<int> first(S, -1), last(S, -1);
+        entries = tiles = 0;
+        for (int k = 0; k < n_views; ++k) {
+            const int s = view_scene[k];
+            if (s < 0 || s >= S) return fail(ANISO_B200_ERR_ARGUMENT, "view_scene out of range");
+            if (first[s] < 0) first[s] = k;
+            else if (last[s] != k - 1) return fail(ANISO_B200_ERR_ARGUMENT, "the views of a scene must be consecutive");
+            last[s] = k;
+            ViewInfo& v = views[k];
+            AB_TRY(pack_camera(deg[s], rendered, &cameras[k], sh.splat_scale, sh.tile_w, sh.tile_h, v.cam));
+            v.scene = static_cast<unsigned>(s);
+            v.n = static_cast<unsigned>(srcs[s].n);
+            v.entry_base = static_cast<unsigned>(entries);
+            v.tile_base = static_cast<unsigned>(tiles);
+            entry_base[k] = v.entry_base;
+            tile_base[k] = v.tile_base;
+            tiles_x[k] = static_cast<unsigned>(v.cam.tilesX);
+            entries += static_cast<uint64_t>(srcs[s].n);
+            tiles += static_cast<uint64_t>(v.cam.tilesX) * v.cam.tilesY;
+            if (entries > kMaxEntries || tiles > kMaxEntries)
+                return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^32 entries or tiles in one batch");
+        }
+        pre_blocks = 0;
+        for (int s = 0; s < S; ++s) {
+            scenes[s].src = srcs[s];
+            scenes[s].view_begin = first[s] < 0 ? 0u : static_cast<unsigned>(first[s]);
+            scenes[s].view_end = first[s] < 0 ? 0u : static_cast<unsigned>(last[s] + 1);
+            scenes[s].block_base = pre_blocks;
+            if (first[s] >= 0) pre_blocks += chunks_of(static_cast<uint64_t>(srcs[s].n), 256);
+        }
+        return 0;
+    }
+
+    int rendered_degree() const { return views.empty() ? 0 : views[0].cam.shDegree; }
+    size_t blob_bytes() const {
+        return views.size() * sizeof(ViewInfo) + scenes.size() * sizeof(BatchScene<Src>) +
+               3 * views.size() * sizeof(unsigned);
+    }
+    // Same launch geometry (the only thing a recorded graph fixes besides the slot).
+    bool same_geometry(const Plan& o) const {
+        if (views.size() != o.views.size() || scenes.size() != o.scenes.size() || entries != o.entries ||
+            tiles != o.tiles)
+            return false;
+        for (size_t k = 0; k < views.size(); ++k)
+            if (views[k].cam.width != o.views[k].cam.width || views[k].cam.height != o.views[k].cam.height)
+                return false;
+        return shape.tile_w == o.shape.tile_w && shape.tile_h == o.shape.tile_h &&
+               shape.blend_batch == o.shape.blend_batch && rendered_degree() == o.rendered_degree();
+    }
+};
+
+// Device copy of a plan's tables, filled from a pinned staging blob by one async copy on the
+// render stream. A slot is reused only after the frame that read it has run (its event).
+struct Slot {
+    DevBuf<unsigned char> dev;
+    unsigned char* pinned = nullptr;
+    size_t cap = 0;
+    cudaEvent_t done = nullptr;
+    bool pending = false;
+    Slot() = default;
+    Slot(const Slot&) = delete;
+    Slot& operator=(const Slot&) = delete;
+    ~Slot() {
+        if (pinned) cudaFreeHost(pinned);
+        if (done) cudaEventDestroy(done);
+    }
+    // Writes the blob (after the frame that last read this slot has run) without copying it.
+    template <class Src>
+    int stage(const Plan<Src>& P) {
+        if (pending) {
+            AB_CUDA(cudaEventSynchronize(done));
+            pending = false;
+        }
+        const size_t bytes = P.blob_bytes();
+        if (bytes > cap) {
+            if (pinned) cudaFreeHost(pinned);
+            pinned = nullptr;
+            AB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&pinned), bytes));
+            AB_TRY(dev.reserve(bytes));
+            cap = bytes;
+        }
+        if (!done) AB_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        const size_t V = P.views.size(), S = P.scenes.size();
+        unsigned char* h = pinned;
+        std::memcpy(h, P.views.data(), V * sizeof(ViewInfo));
+        std::memcpy(h + V * sizeof(ViewInfo), P.scenes.data(), S * sizeof(BatchScene<Src>));
+        unsigned* t = reinterpret_cast<unsigned*>(h + V * sizeof(ViewInfo) + S * sizeof(BatchScene<Src>));
+        std::memcpy(t, P.entry_base.data(), V * sizeof(unsigned));
+        std::memcpy(t + V, P.tile_base.data(), V * sizeof(unsigned));
+        std::memcpy(t + 2 * V, P.tiles_x.data(), V * sizeof(unsigned));
+        return 0;
+    }
+    // Stages the blob and enqueues its upload on `st`; returns the device views, scenes, tables.
+    template <class Src>
+    int fill(const Plan<Src>& P, cudaStream_t st, const ViewInfo** views, const BatchScene<Src>** scenes,
+             BatchTables& tables) {
+        AB_TRY(stage(P));
+        AB_CUDA(cudaMemcpyAsync(dev.p, pinned, P.blob_bytes(), cudaMemcpyHostToDevice, st));
+        const size_t V = P.views.size(), S = P.scenes.size();
+        unsigned char* d = dev.p;
+        *views = reinterpret_cast<const ViewInfo*>(d);
+        *scenes = reinterpret_cast<const BatchScene<Src>*>(d + V * sizeof(ViewInfo));
+        const unsigned* dt = reinterpret_cast<const unsigned*>(d + V * sizeof(ViewInfo) + S * sizeof(BatchScene<Src>));
+        tables.entry_base = dt;
+        tables.tile_base = dt + V;
+        tables.tiles_x = dt + 2 * V;
+        tables.n_views = static_cast<unsigned>(V);
+        return 0;
+    }
+    int mark(cudaStream_t st) {
+        AB_CUDA(cudaEventRecord(done, st));
+        pending = true;
+        return 0;
+    }
+};
+
+void launch_preprocess_any(const BatchScene<SceneView>* sc, const Plan<SceneView>& P, const ViewInfo* views, Ctrl* ctrl,
+                           Arena& A, const DebugProjection* dbg, cudaStream_t st) {
+    launch_preprocess(sc, static_cast<unsigned>(P.scenes.size()), P.pre_blocks, views, P.rendered_degree(),
+                      P.shape.tile_w, P.shape.tile_h, ctrl, A.rec.p, A.rect16.p, A.depth_key.p, dbg, st);
+}
+void launch_preprocess_any(const BatchScene<RawParams>* sc, const Plan<RawParams>& P, const ViewInfo* views,
+                           Ctrl* ctrl, Arena& A, const DebugProjection*, cudaStream_t st) {
+    launch_preprocess_raw(sc, static_cast<unsigned>(P.scenes.size()), P.pre_blocks, views, P.rendered_degree(),
+                          P.shape.tile_w, P.shape.tile_h, ctrl, A.rec.p, A.rect16.p, A.depth_key.p, st);
+}
+
+// Enqueues one frame of a plan. ev (4 events, may be NULL) brackets the stages.
+template <class Src>
+int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cudaEvent_t* ev,
+                 const DebugProjection* dbg, bool stop_after_sort, bool train, int* final_buf, bool mark_slot = true) {
+    const ViewInfo* views = nullptr;
+    const BatchScene<Src>* scenes = nullptr;
+    BatchTables tables;
+    AB_TRY(slot.fill(P, st, &views, &scenes, tables));
+    if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
+    launch_frame_begin(A.ctrl.p, st);
+    launch_preprocess_any(scenes, P, views, A.ctrl.p, A, dbg, st);
+    if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
+    int fin = 0;
+    AB_TRY(enqueue_sort(A, static_cast<unsigned>(P.entries), static_cast<unsigned>(P.tiles), tables, st, &fin));
+    if (ev) AB_CUDA(cudaEventRecord(ev[2], st));
+    if (!stop_after_sort)
+        launch_blend(static_cast<unsigned>(P.tiles), A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, views, tables,
+                     P.shape.tile_w, P.shape.tile_h, P.shape.blend_batch, train, st);
+    if (ev) AB_CUDA(cudaEventRecord(ev[3], st));
+    AB_CUDA(cudaGetLastError());
+    if (mark_slot) AB_TRY(slot.mark(st));
+    if (final_buf) *final_buf = fin;
+    return 0;
+}
+
+// Reads the control block of the last frame on `st` (waits for it). The frame's flags are then
+// consumed: they are cleared on the device, so that the next frame_begin does not fold them into
+// the sticky flags as if no one had seen them.
+int read_ctrl(const Arena& A, Ctrl* host, cudaStream_t st) {
+    AB_CUDA(cudaMemcpyAsync(host, A.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    AB_CUDA(cudaMemsetAsync(&A.ctrl.p->flags, 0, sizeof(unsigned), st));
+    AB_CUDA(cudaStreamSynchronize(st));
+    return 0;
+}
+
+// After a synchronised frame: grows the pair buffers on overflow (*again = 1: render it again).
+// With all_frames, also looks at the frames before the last one (the sticky fields).
+int settle(Arena& A, const Ctrl& h, int* again, bool all_frames) {
+    *again = 0;
+    const unsigned flags = h.flags | (all_frames ? h.sticky_flags : 0u);
+    const uint64_t pairs = all_frames ? std::max(h.pair_total, h.max_pair_total) : h.pair_total;
+    if (flags & kFlagTimeout) return fail(ANISO_B200_ERR_DEVICE_WAIT, "a device-side look-back wait gave up");
+    if (flags & kFlagOverflow) {
+        const uint64_t need = pairs + pairs / 4 + 1024;
+        if (need > kMaxPairs) return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 splat-tile pairs");
+        AB_CUDA(cudaDeviceSynchronize());
+        AB_TRY(A.grow_pairs(static_cast<unsigned>(need)));
+        *again = 1;
+    }
+    return 0;
+}
+
+int clear_sticky(Arena& A, cudaStream_t st) {
+    AB_CUDA(cudaMemsetAsync(&A.ctrl.p->sticky_flags, 0, sizeof(unsigned), st));
+    AB_CUDA(cudaMemsetAsync(&A.ctrl.p->max_pair_total, 0, sizeof(unsigned long long), st));
+    AB_CUDA(cudaStreamSynchronize(st));
+    return 0;
+}
+
+constexpr int kSlots = 8;
+
 }  // namespace
+
+// ---- scenes ------------------------------------------------------------------------------------
 
 struct aniso_b200_scene {
     int64_t n = 0;
     int degree = 0;
     int planes = 0;
     DevBuf<float4> pos_op, scale, rot, sh;
-    Arena arena;
+    Arena arena;  // work buffers of the scene's own renders
+    Slot slots[kSlots];
+    int next_slot = 0;
+    DevBuf<uint8_t> image;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     Ctrl* host_ctrl = nullptr;  // pinned
@@ -204,8 +490,9 @@ struct aniso_b200_scene {
         v.sh_planes = planes;
         return v;
     }
+    Slot& slot() { return slots[next_slot++ % kSlots]; }
     ~aniso_b200_scene() {
-        if (stream) cudaStreamSynchronize(stream);
+        cudaDeviceSynchronize();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : prof_ev) cudaEventDestroy(e);
@@ -273,15 +560,20 @@ int validate_degree(int d) {
     return 0;
 }
 
-int new_scene(int64_t n, int degree, aniso_b200_scene** out, aniso_b200_scene** made) {
-    if (!out) return fail(ANISO_B200_ERR_ARGUMENT, "out is NULL");
-    if (n < 0 || n >= (int64_t(1) << 31)) return fail(ANISO_B200_ERR_ARGUMENT, "n must be in [0, 2^31)");
-    AB_TRY(validate_degree(degree));
+int device_present() {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         cudaGetLastError();
         return fail(ANISO_B200_ERR_NO_DEVICE, "no CUDA device");
     }
+    return 0;
+}
+
+int new_scene(int64_t n, int degree, aniso_b200_scene** out, aniso_b200_scene** made) {
+    if (!out) return fail(ANISO_B200_ERR_ARGUMENT, "out is NULL");
+    if (n < 0 || n >= (int64_t(1) << 31)) return fail(ANISO_B200_ERR_ARGUMENT, "n must be in [0, 2^31)");
+    AB_TRY(validate_degree(degree));
+    AB_TRY(device_present());
     aniso_b200_scene* s = new (std::nothrow) aniso_b200_scene();
     if (!s) return fail(ANISO_B200_ERR_OUT_OF_MEMORY, "host allocation failed");
     *made = s;
@@ -298,109 +590,25 @@ int new_scene(int64_t n, int degree, aniso_b200_scene** out, aniso_b200_scene** 
     for (auto& e : s->ev) AB_CUDA(cudaEventCreate(&e));
     AB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&s->host_ctrl), sizeof(Ctrl)));
     std::memset(s->host_ctrl, 0, sizeof(Ctrl));
-    const uint64_t cap = std::max<uint64_t>(1u << 20, 4ull * static_cast<uint64_t>(n));
-    AB_TRY(s->arena.init(n, static_cast<unsigned>(std::min<uint64_t>(cap, 0x3FFFFFFFull))));
-    return 0;
+    return s->arena.ensure(std::max<int64_t>(n, 1));
 }
 
-// The per-view constants, packed as gpu_render.cu:301-316 packs them (doubles cast to float; the
-// eye is Camera::centre(), camera.cpp:19-23, computed in double).
-int pack_camera_deg(int scene_degree, const aniso_b200_camera* c, const aniso_b200_options* o, CamParams& cp) {
-    if (!c) return fail(ANISO_B200_ERR_ARGUMENT, "camera is NULL");
-    if (c->width <= 0 || c->height <= 0 || c->width > 32767 || c->height > 32767)
-        return fail(ANISO_B200_ERR_ARGUMENT, "camera size must be in [1, 32767]");
-    const int opt_degree = o ? o->sh_degree : 3;
-    if (opt_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
-    std::memset(&cp, 0, sizeof cp);
-    for (int r = 0; r < 3; ++r) {
-        for (int k = 0; k < 3; ++k) cp.R[r * 3 + k] = static_cast<float>(c->R[r * 3 + k]);
-        cp.t[r] = static_cast<float>(c->t[r]);
-    }
-    const double* R = c->R;
-    const double* t = c->t;
-    cp.eye[0] = static_cast<float>(-(R[0] * t[0] + R[3] * t[1] + R[6] * t[2]));
-    cp.eye[1] = static_cast<float>(-(R[1] * t[0] + R[4] * t[1] + R[7] * t[2]));
-    cp.eye[2] = static_cast<float>(-(R[2] * t[0] + R[5] * t[1] + R[8] * t[2]));
-    cp.fx = static_cast<float>(c->fx);
-    cp.fy = static_cast<float>(c->fy);
-    cp.cx = static_cast<float>(c->cx);
-    cp.cy = static_cast<float>(c->cy);
-    cp.width = c->width;
-    cp.height = c->height;
-    cp.tilesX = (c->width + kTile - 1) / kTile;
-    cp.tilesY = (c->height + kTile - 1) / kTile;
-    cp.shDegree = std::min(std::min(opt_degree, scene_degree), 3);
-    cp.shCoeffs = (scene_degree + 1) * (scene_degree + 1);
-    cp.splatScale = o ? o->splat_scale : 1.0f;
-    return 0;
+PlanShape scene_shape(const aniso_b200_options* o) {
+    PlanShape shape;
+    shape.sh_degree = o ? o->sh_degree : 3;
+    shape.splat_scale = o ? o->splat_scale : 1.0f;
+    return shape;
 }
 
-int pack_camera(const aniso_b200_scene* s, const aniso_b200_camera* c, const aniso_b200_options* o, CamParams& cp) {
-    return pack_camera_deg(s->degree, c, o, cp);
-}
-
-// Enqueues one frame; ev (4 events, may be NULL) brackets the stages. With stop_after_sort, the
-// blend is skipped (introspection).
-int enqueue_frame(aniso_b200_scene* s, const CamParams& cam, const BlendOut& out, cudaStream_t st, cudaEvent_t* ev,
-                  const DebugProjection* dbg, bool stop_after_sort, int* final_buf) {
-    Arena& A = s->arena;
-    AB_TRY(A.tick(st));
-    if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
-    launch_frame_begin(A.ctrl.p, st);
-    launch_preprocess(s->view(), cam, A.ctrl.p, A.rec.p, A.rect16.p, A.depth_key.p, dbg, st);
-    if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
-    int fin = 0;
-    AB_TRY(enqueue_sort(A, cam.tilesX, cam.tilesY, st, &fin));
-    if (ev) AB_CUDA(cudaEventRecord(ev[2], st));
-    if (!stop_after_sort)
-        launch_blend(A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, cam.width, cam.height, cam.tilesX, cam.tilesY,
-                     out, st);
-    if (ev) AB_CUDA(cudaEventRecord(ev[3], st));
-    AB_CUDA(cudaGetLastError());
-    if (final_buf) *final_buf = fin;
-    return 0;
-}
-
-// After a synchronised frame: grows the pair buffers on overflow (returns 1 = render again).
-// With all_frames, also looks at the frames before the last one (the sticky fields).
-int settle(aniso_b200_scene* s, int* again, bool all_frames = false) {
-    *again = 0;
-    const Ctrl& h = *s->host_ctrl;
-    const unsigned flags = h.flags | (all_frames ? h.sticky_flags : 0u);
-    const uint64_t pairs = all_frames ? std::max(h.pair_total, h.max_pair_total) : h.pair_total;
-    if (flags & kFlagTimeout) return fail(ANISO_B200_ERR_DEVICE_WAIT, "a device-side look-back wait gave up");
-    if (flags & kFlagOverflow) {
-        const uint64_t need = pairs + pairs / 4 + 1024;
-        if (need > 0x3FFFFFFFull) return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 splat-tile pairs");
-        AB_CUDA(cudaStreamSynchronize(s->stream));
-        AB_TRY(s->arena.grow_pairs(static_cast<unsigned>(need)));
-        *again = 1;
-    }
-    return 0;
-}
-
-int read_ctrl(aniso_b200_scene* s, cudaStream_t st) {
-    AB_CUDA(cudaMemcpyAsync(s->host_ctrl, s->arena.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
-    AB_CUDA(cudaStreamSynchronize(st));
-    return 0;
+// A plan of one view of one scene.
+int single_plan(aniso_b200_scene* s, const aniso_b200_camera* camera, const aniso_b200_options* options,
+                Plan<SceneView>& P) {
+    if (options && options->sh_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
+    const int32_t vs = 0;
+    return P.build({s->view()}, {s->degree}, &vs, 1, camera, scene_shape(options));
 }
 
 }  // namespace
-
-struct aniso_b200_trainer {
-    Arena arena;
-    Ctrl* host_ctrl = nullptr;  // pinned
-    DevBuf<float> t_final, grad_pair;
-    DevBuf<unsigned> n_contrib;
-    // The state of the last forward, for its backward.
-    bool has_forward = false;
-    RawParams raw{};
-    CamParams cam{};
-    int fin = 0;
-    ~aniso_b200_trainer() {
-        if (host_ctrl) cudaFreeHost(host_ctrl);
-    }
-};
 
 extern "C" {
 
@@ -511,18 +719,19 @@ int aniso_b200_scene_destroy(aniso_b200_scene* scene) {
 int aniso_b200_render(aniso_b200_scene* s, const aniso_b200_camera* camera, const aniso_b200_options* options,
                       uint8_t* rgb_host, aniso_b200_stats* stats) {
     if (!s || !rgb_host) return fail(ANISO_B200_ERR_ARGUMENT, "scene/rgb_host is NULL");
-    CamParams cam;
-    AB_TRY(pack_camera(s, camera, options, cam));
-    const size_t bytes = static_cast<size_t>(cam.width) * cam.height * 3;
-    AB_TRY(s->arena.image.reserve(bytes));
-    BlendOut out;
-    out.rgb8 = s->arena.image.p;
+    Plan<SceneView> P;
+    AB_TRY(single_plan(s, camera, options, P));
+    const size_t bytes = static_cast<size_t>(camera->width) * camera->height * 3;
+    AB_TRY(s->image.reserve(bytes));
+    P.views[0].rgb8 = s->image.p;
     for (int attempt = 0; attempt < 3; ++attempt) {
-        AB_TRY(enqueue_frame(s, cam, out, s->stream, stats ? s->ev : nullptr, nullptr, false, nullptr));
-        AB_CUDA(cudaMemcpyAsync(rgb_host, out.rgb8, bytes, cudaMemcpyDeviceToHost, s->stream));
-        AB_TRY(read_ctrl(s, s->stream));
+        AB_TRY(s->arena.tick(s->stream));
+        AB_TRY(enqueue_plan(s->arena, s->slot(), P, s->stream, stats ? s->ev : nullptr, nullptr, false, false,
+                            nullptr));
+        AB_CUDA(cudaMemcpyAsync(rgb_host, s->image.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+        AB_TRY(read_ctrl(s->arena, s->host_ctrl, s->stream));
         int again = 0;
-        AB_TRY(settle(s, &again));
+        AB_TRY(settle(s->arena, *s->host_ctrl, &again, false));
         if (again) continue;
         if (stats) {
             float a = 0, b = 0, c = 0;
@@ -543,10 +752,9 @@ int aniso_b200_render(aniso_b200_scene* s, const aniso_b200_camera* camera, cons
 int aniso_b200_render_device(aniso_b200_scene* s, const aniso_b200_camera* camera, const aniso_b200_options* options,
                              uint8_t* rgb_device, void* stream) {
     if (!s || !rgb_device) return fail(ANISO_B200_ERR_ARGUMENT, "scene/rgb_device is NULL");
-    CamParams cam;
-    AB_TRY(pack_camera(s, camera, options, cam));
-    BlendOut out;
-    out.rgb8 = rgb_device;
+    Plan<SceneView> P;
+    AB_TRY(single_plan(s, camera, options, P));
+    P.views[0].rgb8 = rgb_device;
     cudaEvent_t* ev = nullptr;
     if (s->profiling) {
         while (s->prof_ev.size() < 4 * (s->prof_frames + 1)) {
@@ -556,7 +764,9 @@ int aniso_b200_render_device(aniso_b200_scene* s, const aniso_b200_camera* camer
         }
         ev = &s->prof_ev[4 * s->prof_frames++];
     }
-    return enqueue_frame(s, cam, out, static_cast<cudaStream_t>(stream), ev, nullptr, false, nullptr);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    AB_TRY(s->arena.tick(st));
+    return enqueue_plan(s->arena, s->slot(), P, st, ev, nullptr, false, false, nullptr);
 }
 
 int aniso_b200_profile(aniso_b200_scene* s, int32_t enable) {
@@ -589,18 +799,15 @@ int aniso_b200_profile_read(aniso_b200_scene* s, double* project_ms, double* sor
 int aniso_b200_sync(aniso_b200_scene* s, aniso_b200_stats* stats) {
     if (!s) return fail(ANISO_B200_ERR_ARGUMENT, "scene is NULL");
     AB_CUDA(cudaDeviceSynchronize());
-    AB_TRY(read_ctrl(s, s->stream));
+    AB_TRY(read_ctrl(s->arena, s->host_ctrl, s->stream));
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
         stats->visible = s->host_ctrl->vis_count;
         stats->tile_pairs = s->host_ctrl->pair_total;
     }
-    // Clear the sticky record of earlier frames once read.
-    AB_CUDA(cudaMemsetAsync(&s->arena.ctrl.p->sticky_flags, 0, sizeof(unsigned), s->stream));
-    AB_CUDA(cudaMemsetAsync(&s->arena.ctrl.p->max_pair_total, 0, sizeof(unsigned long long), s->stream));
-    AB_CUDA(cudaStreamSynchronize(s->stream));
+    AB_TRY(clear_sticky(s->arena, s->stream));
     int again = 0;
-    AB_TRY(settle(s, &again, true));
+    AB_TRY(settle(s->arena, *s->host_ctrl, &again, true));
     if (again) return fail(ANISO_B200_ERR_ARGUMENT, "pair capacity exceeded");
     return ANISO_B200_OK;
 }
@@ -609,8 +816,8 @@ int aniso_b200_debug_projection(aniso_b200_scene* s, const aniso_b200_camera* ca
                                 const aniso_b200_options* options, float* uv, float* conic_opacity, float* depth,
                                 float* rgb, uint32_t* rect, uint32_t* tiles_touched) {
     if (!s) return fail(ANISO_B200_ERR_ARGUMENT, "scene is NULL");
-    CamParams cam;
-    AB_TRY(pack_camera(s, camera, options, cam));
+    Plan<SceneView> P;
+    AB_TRY(single_plan(s, camera, options, P));
     const size_t nn = static_cast<size_t>(std::max<int64_t>(s->n, 1));
     DevBuf<float2> duv;
     DevBuf<float4> dco;
@@ -631,9 +838,14 @@ int aniso_b200_debug_projection(aniso_b200_scene* s, const aniso_b200_camera* ca
     dbg.rect = drect.p;
     dbg.tiles_touched = dtt.p;
     Arena& A = s->arena;
-    AB_TRY(A.tick(s->stream));
+    const ViewInfo* views = nullptr;
+    const BatchScene<SceneView>* scenes = nullptr;
+    BatchTables tables;
+    Slot& slot = s->slot();
+    AB_TRY(slot.fill(P, s->stream, &views, &scenes, tables));
     launch_frame_begin(A.ctrl.p, s->stream);
-    launch_preprocess(s->view(), cam, A.ctrl.p, A.rec.p, A.rect16.p, A.depth_key.p, &dbg, s->stream);
+    launch_preprocess_any(scenes, P, views, A.ctrl.p, A, &dbg, s->stream);
+    AB_TRY(slot.mark(s->stream));
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaStreamSynchronize(s->stream));
     const size_t n = static_cast<size_t>(s->n);
@@ -649,25 +861,25 @@ int aniso_b200_debug_projection(aniso_b200_scene* s, const aniso_b200_camera* ca
 int aniso_b200_debug_sorted(aniso_b200_scene* s, const aniso_b200_camera* camera, const aniso_b200_options* options,
                             uint32_t* tiles, uint32_t* values, uint64_t capacity, uint32_t* ranges, uint64_t* pairs) {
     if (!s || !pairs) return fail(ANISO_B200_ERR_ARGUMENT, "scene/pairs is NULL");
-    CamParams cam;
-    AB_TRY(pack_camera(s, camera, options, cam));
+    Plan<SceneView> P;
+    AB_TRY(single_plan(s, camera, options, P));
     int fin = 0;
     for (int attempt = 0; attempt < 3; ++attempt) {
-        AB_TRY(enqueue_frame(s, cam, BlendOut{}, s->stream, nullptr, nullptr, true, &fin));
-        AB_TRY(read_ctrl(s, s->stream));
+        AB_TRY(s->arena.tick(s->stream));
+        AB_TRY(enqueue_plan(s->arena, s->slot(), P, s->stream, nullptr, nullptr, true, false, &fin));
+        AB_TRY(read_ctrl(s->arena, s->host_ctrl, s->stream));
         int again = 0;
-        AB_TRY(settle(s, &again));
+        AB_TRY(settle(s->arena, *s->host_ctrl, &again, false));
         if (!again) break;
     }
-    const uint64_t P = s->host_ctrl->pair_total;
-    *pairs = P;
-    if (P > capacity) return fail(ANISO_B200_ERR_ARGUMENT, "capacity too small");
+    const uint64_t Pn = s->host_ctrl->pair_total;
+    *pairs = Pn;
+    if (Pn > capacity) return fail(ANISO_B200_ERR_ARGUMENT, "capacity too small");
     const Arena& A = s->arena;
-    if (tiles && P) AB_CUDA(cudaMemcpy(tiles, A.pair_key[fin].p, P * sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (values && P) AB_CUDA(cudaMemcpy(values, A.pair_val[fin].p, P * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (tiles && Pn) AB_CUDA(cudaMemcpy(tiles, A.pair_key[fin].p, Pn * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (values && Pn) AB_CUDA(cudaMemcpy(values, A.pair_val[fin].p, Pn * sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (ranges)
-        AB_CUDA(cudaMemcpy(ranges, A.ranges.p, static_cast<size_t>(cam.tilesX) * cam.tilesY * sizeof(uint2),
-                           cudaMemcpyDeviceToHost));
+        AB_CUDA(cudaMemcpy(ranges, A.ranges.p, static_cast<size_t>(P.tiles) * sizeof(uint2), cudaMemcpyDeviceToHost));
     return ANISO_B200_OK;
 }
 
@@ -677,20 +889,24 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     if (n < 0 || n >= (int64_t(1) << 31) || tiles_x <= 0 || tiles_y <= 0 || !pairs)
         return fail(ANISO_B200_ERR_ARGUMENT, "bad size or NULL pairs");
     if (n > 0 && (!tiles_touched || !rect || !depth)) return fail(ANISO_B200_ERR_ARGUMENT, "input is NULL");
-    uint64_t P = 0;
-    for (int64_t i = 0; i < n; ++i) P += tiles_touched[i];
-    *pairs = P;
-    if (P > capacity) return fail(ANISO_B200_ERR_ARGUMENT, "capacity too small");
-    if (P > 0x3FFFFFFFull) return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 pairs");
+    uint64_t Pn = 0;
+    for (int64_t i = 0; i < n; ++i) Pn += tiles_touched[i];
+    *pairs = Pn;
+    if (Pn > capacity) return fail(ANISO_B200_ERR_ARGUMENT, "capacity too small");
+    if (Pn > kMaxPairs) return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 pairs");
+    AB_TRY(device_present());
     Arena A;
-    AB_TRY(A.init(n, static_cast<unsigned>(std::max<uint64_t>(P, 1))));
+    AB_TRY(A.init(std::max<int64_t>(n, 1), static_cast<unsigned>(std::max<uint64_t>(Pn, 1))));
     const size_t nn = static_cast<size_t>(std::max<int64_t>(n, 1));
-    DevBuf<unsigned> dtt;
+    DevBuf<unsigned> dtt, dtab;
     DevBuf<uint4> drect;
     DevBuf<float> ddepth;
     AB_TRY(dtt.reserve(nn));
     AB_TRY(drect.reserve(nn));
     AB_TRY(ddepth.reserve(nn));
+    AB_TRY(dtab.reserve(3));
+    const unsigned tab[3] = {0u, 0u, static_cast<unsigned>(tiles_x)};  // one view: entry base, tile base, tiles_x
+    AB_CUDA(cudaMemcpy(dtab.p, tab, sizeof tab, cudaMemcpyHostToDevice));
     const size_t un = static_cast<size_t>(n);
     if (n > 0) {
         AB_CUDA(cudaMemcpy(dtt.p, tiles_touched, un * sizeof(unsigned), cudaMemcpyHostToDevice));
@@ -698,32 +914,297 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
         AB_CUDA(cudaMemcpy(ddepth.p, depth, un * sizeof(float), cudaMemcpyHostToDevice));
     }
     cudaStream_t st = nullptr;
+    const BatchTables tables{dtab.p, dtab.p + 1, dtab.p + 2, 1u};
     AB_TRY(A.tick(st));
     launch_frame_begin(A.ctrl.p, st);
     launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.ctrl.p, A.depth_key.p, A.rect16.p, st);
     int fin = 0;
-    AB_TRY(enqueue_sort(A, tiles_x, tiles_y, st, &fin));
+    const unsigned T = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
+    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, st, &fin));
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaDeviceSynchronize());
     Ctrl h;
     AB_CUDA(cudaMemcpy(&h, A.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost));
     if (h.flags & kFlagTimeout) return fail(ANISO_B200_ERR_DEVICE_WAIT, "a device-side look-back wait gave up");
-    if (h.pair_total != P) return fail(ANISO_B200_ERR_CUDA, "device pair count disagrees with the host");
-    if (tiles && P) AB_CUDA(cudaMemcpy(tiles, A.pair_key[fin].p, P * sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (values && P) AB_CUDA(cudaMemcpy(values, A.pair_val[fin].p, P * sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (ranges)
-        AB_CUDA(cudaMemcpy(ranges, A.ranges.p, static_cast<size_t>(tiles_x) * tiles_y * sizeof(uint2),
-                           cudaMemcpyDeviceToHost));
+    if (h.pair_total != Pn) return fail(ANISO_B200_ERR_CUDA, "device pair count disagrees with the host");
+    if (tiles && Pn) AB_CUDA(cudaMemcpy(tiles, A.pair_key[fin].p, Pn * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (values && Pn) AB_CUDA(cudaMemcpy(values, A.pair_val[fin].p, Pn * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (ranges) AB_CUDA(cudaMemcpy(ranges, A.ranges.p, static_cast<size_t>(T) * sizeof(uint2), cudaMemcpyDeviceToHost));
     return ANISO_B200_OK;
 }
 
+}  // extern "C"
+
+// ---- batches -------------------------------------------------------------------------------
+
+struct aniso_b200_batch {
+    std::vector<aniso_b200_scene*> scenes;
+    std::vector<int32_t> view_scene;
+    PlanShape shape;
+    bool use_graph = false;
+    Arena arena;
+    Slot slots[kSlots];
+    int next_slot = 0;
+    Slot graph_slot;
+    Plan<SceneView> graph_plan;
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t capture_stream = nullptr;
+    Ctrl* host_ctrl = nullptr;
+    ~aniso_b200_batch() {
+        cudaDeviceSynchronize();
+        if (graph) cudaGraphExecDestroy(graph);
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        if (host_ctrl) cudaFreeHost(host_ctrl);
+    }
+};
+
+extern "C" {
+
+int aniso_b200_batch_create(aniso_b200_scene* const* scenes, int32_t n_scenes, const int32_t* view_scene,
+                            int32_t n_views, const aniso_b200_batch_options* options, aniso_b200_batch** out) {
+    if (!out || !scenes || !view_scene || n_scenes <= 0 || n_views <= 0)
+        return fail(ANISO_B200_ERR_ARGUMENT, "a batch needs scenes, views and out");
+    for (int s = 0; s < n_scenes; ++s)
+        if (!scenes[s]) return fail(ANISO_B200_ERR_ARGUMENT, "a scene is NULL");
+    PlanShape shape;
+    AB_TRY(check_options(options, shape));
+    aniso_b200_batch* b = new (std::nothrow) aniso_b200_batch();
+    if (!b) return fail(ANISO_B200_ERR_OUT_OF_MEMORY, "host allocation failed");
+    b->scenes.assign(scenes, scenes + n_scenes);
+    b->view_scene.assign(view_scene, view_scene + n_views);
+    b->shape = shape;
+    b->use_graph = options && options->use_graph;
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&b->host_ctrl), sizeof(Ctrl));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "batch create");
+    }
+    std::memset(b->host_ctrl, 0, sizeof(Ctrl));
+    *out = b;
+    return ANISO_B200_OK;
+}
+
+int aniso_b200_batch_destroy(aniso_b200_batch* batch) {
+    delete batch;
+    return ANISO_B200_OK;
+}
+
+int aniso_b200_batch_render(aniso_b200_batch* b, const aniso_b200_camera* cameras, uint8_t* const* rgb_device,
+                            void* stream) {
+    if (!b || !cameras || !rgb_device) return fail(ANISO_B200_ERR_ARGUMENT, "batch/cameras/rgb_device is NULL");
+    std::vector<SceneView> srcs;
+    std::vector<int> degs;
+    for (auto* s : b->scenes) {
+        srcs.push_back(s->view());
+        degs.push_back(s->degree);
+    }
+    Plan<SceneView> P;
+    AB_TRY(P.build(srcs, degs, b->view_scene.data(), static_cast<int>(b->view_scene.size()), cameras, b->shape));
+    for (size_t k = 0; k < P.views.size(); ++k) {
+        if (!rgb_device[k]) return fail(ANISO_B200_ERR_ARGUMENT, "an output buffer is NULL");
+        P.views[k].rgb8 = rgb_device[k];
+    }
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (b->arena.n < static_cast<int64_t>(P.entries) && b->graph) {
+        AB_CUDA(cudaDeviceSynchronize());
+        cudaGraphExecDestroy(b->graph);  // buffers are about to move: record again
+        b->graph = nullptr;
+    }
+    AB_TRY(b->arena.ensure(static_cast<int64_t>(std::max<uint64_t>(P.entries, 1))));
+    AB_TRY(b->arena.tick(st));
+    if (!b->use_graph)
+        return enqueue_plan(b->arena, b->slots[b->next_slot++ % kSlots], P, st, nullptr, nullptr, false, false,
+                            nullptr);
+    if (b->graph && !P.same_geometry(b->graph_plan)) {
+        AB_CUDA(cudaDeviceSynchronize());
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    if (!b->graph) {
+        // Record the sequence on a private stream. The recorded upload reads the graph slot's
+        // pinned blob at every replay, and each replay refreshes that blob first.
+        // Every allocation the sequence needs happens first: none may happen while capturing.
+        AB_TRY(b->graph_slot.stage(P));
+        AB_TRY(b->arena.ranges.reserve(static_cast<size_t>(P.tiles)));
+        cudaGraph_t g = nullptr;
+        AB_CUDA(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue_plan(b->arena, b->graph_slot, P, b->capture_stream, nullptr, nullptr, false, false,
+                                    nullptr, false);
+        const cudaError_t ce = cudaStreamEndCapture(b->capture_stream, &g);
+        if (rc != 0) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+        const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate");
+        b->graph_plan = P;
+    } else {
+        AB_TRY(b->graph_slot.stage(P));  // waits for the previous replay to have read it
+    }
+    AB_CUDA(cudaGraphLaunch(b->graph, st));
+    return b->graph_slot.mark(st);
+}
+
+int aniso_b200_batch_sync(aniso_b200_batch* b, aniso_b200_stats* stats) {
+    if (!b) return fail(ANISO_B200_ERR_ARGUMENT, "batch is NULL");
+    AB_CUDA(cudaDeviceSynchronize());
+    AB_TRY(read_ctrl(b->arena, b->host_ctrl, b->capture_stream));
+    if (stats) {
+        std::memset(stats, 0, sizeof *stats);
+        stats->visible = b->host_ctrl->vis_count;
+        stats->tile_pairs = b->host_ctrl->pair_total;
+    }
+    AB_TRY(clear_sticky(b->arena, b->capture_stream));
+    int again = 0;
+    AB_TRY(settle(b->arena, *b->host_ctrl, &again, true));
+    if (again) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);  // buffers moved: record again
+            b->graph = nullptr;
+        }
+        return fail(ANISO_B200_ERR_ARGUMENT, "pair capacity exceeded");
+    }
+    return ANISO_B200_OK;
+}
+
+}  // extern "C"
+
+// ---- the differentiable path ---------------------------------------------------------------
+
+struct aniso_b200_trainer {
+    Arena arena;
+    Slot slots[kSlots];
+    int next_slot = 0;
+    Ctrl* host_ctrl = nullptr;  // pinned
+    std::vector<DevBuf<float>> t_final;
+    std::vector<DevBuf<unsigned>> n_contrib;
+    DevBuf<float> grad_pair;
+    // The state of the last forward, for its backward.
+    bool has_forward = false;
+    Plan<RawParams> plan;
+    int fin = 0;
+    Slot& slot() { return slots[next_slot++ % kSlots]; }
+    ~aniso_b200_trainer() {
+        cudaDeviceSynchronize();
+        if (host_ctrl) cudaFreeHost(host_ctrl);
+    }
+};
+
+namespace {
+
+int raw_of(const aniso_b200_raw_params& P, RawParams& raw) {
+    if (P.n < 0 || P.n >= (int64_t(1) << 31)) return fail(ANISO_B200_ERR_ARGUMENT, "n must be in [0, 2^31)");
+    if (P.sh_degree != 1 && P.sh_degree != 3)
+        return fail(ANISO_B200_ERR_ARGUMENT, "stored SH degree must be 1 or 3 (whole 16-byte words per Gaussian)");
+    if (P.n > 0 && (!P.means || !P.log_scales || !P.quats || !P.opacity_logits || !P.sh))
+        return fail(ANISO_B200_ERR_ARGUMENT, "a parameter pointer is NULL");
+    if ((reinterpret_cast<uintptr_t>(P.quats) | reinterpret_cast<uintptr_t>(P.sh)) & 15)
+        return fail(ANISO_B200_ERR_ARGUMENT, "quats and sh must be 16-byte aligned");
+    raw.means = P.means;
+    raw.log_scales = P.log_scales;
+    raw.quats = reinterpret_cast<const float4*>(P.quats);
+    raw.logits = P.opacity_logits;
+    raw.sh = reinterpret_cast<const float4*>(P.sh);
+    raw.n = P.n;
+    raw.sh_planes = (P.sh_degree + 1) * (P.sh_degree + 1) * 3 / 4;
+    return 0;
+}
+
+int train_forward(aniso_b200_trainer* t, const aniso_b200_raw_params* params, int32_t n_scenes,
+                  const int32_t* view_scene, const aniso_b200_camera* cameras, int32_t n_views, const PlanShape& shape,
+                  float* const* images, cudaStream_t st) {
+    if (!t || !params || !images) return fail(ANISO_B200_ERR_ARGUMENT, "trainer/params/images is NULL");
+    t->has_forward = false;
+    std::vector<RawParams> srcs(n_scenes);
+    std::vector<int> degs(n_scenes);
+    for (int s = 0; s < n_scenes; ++s) {
+        AB_TRY(raw_of(params[s], srcs[s]));
+        degs[s] = params[s].sh_degree;
+    }
+    Plan<RawParams>& P = t->plan;
+    AB_TRY(P.build(srcs, degs, view_scene, n_views, cameras, shape));
+    if (t->t_final.size() < static_cast<size_t>(n_views)) {
+        t->t_final.resize(n_views);
+        t->n_contrib.resize(n_views);
+    }
+    for (int k = 0; k < n_views; ++k) {
+        if (!images[k]) return fail(ANISO_B200_ERR_ARGUMENT, "an image buffer is NULL");
+        const size_t px = static_cast<size_t>(P.views[k].cam.width) * P.views[k].cam.height;
+        AB_TRY(t->t_final[k].reserve(px));
+        AB_TRY(t->n_contrib[k].reserve(px));
+        P.views[k].rgbf = images[k];
+        P.views[k].t_final = t->t_final[k].p;
+        P.views[k].n_contrib = t->n_contrib[k].p;
+    }
+    Arena& A = t->arena;
+    AB_TRY(A.ensure(static_cast<int64_t>(std::max<uint64_t>(P.entries, 1))));
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        AB_TRY(A.tick(st));
+        int fin = 0;
+        AB_TRY(enqueue_plan(A, t->slot(), P, st, nullptr, nullptr, false, true, &fin));
+        AB_TRY(read_ctrl(A, t->host_ctrl, st));
+        int again = 0;
+        AB_TRY(settle(A, *t->host_ctrl, &again, false));
+        if (again) continue;
+        t->fin = fin;
+        t->has_forward = true;
+        return ANISO_B200_OK;
+    }
+    return fail(ANISO_B200_ERR_ARGUMENT, "pair capacity kept overflowing");
+}
+
+int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const aniso_b200_raw_grads* grads,
+                   cudaStream_t st) {
+    if (!t || !grad_images || !grads) return fail(ANISO_B200_ERR_ARGUMENT, "trainer/grad_images/grads is NULL");
+    if (!t->has_forward) return fail(ANISO_B200_ERR_ARGUMENT, "no forward to differentiate");
+    Plan<RawParams>& P = t->plan;
+    for (size_t k = 0; k < P.views.size(); ++k) {
+        if (!grad_images[k]) return fail(ANISO_B200_ERR_ARGUMENT, "a gradient image is NULL");
+        P.views[k].grad_img = grad_images[k];
+    }
+    for (size_t s = 0; s < P.scenes.size(); ++s)
+        if (P.scenes[s].src.n > 0 && (!grads[s].means || !grads[s].log_scales || !grads[s].quats ||
+                                      !grads[s].opacity_logits || !grads[s].sh))
+            return fail(ANISO_B200_ERR_ARGUMENT, "a gradient pointer is NULL");
+    Arena& A = t->arena;
+    const Ctrl& h = *t->host_ctrl;
+    AB_TRY(t->grad_pair.reserve(std::max<uint64_t>(h.pair_total, 1) * 9));
+    const ViewInfo* views = nullptr;
+    const BatchScene<RawParams>* scenes = nullptr;
+    BackwardIn in;
+    Slot& slot = t->slot();
+    AB_TRY(slot.fill(P, st, &views, &scenes, in.tables));
+    in.ranges = A.ranges.p;
+    in.vals = A.pair_val[t->fin].p;
+    in.rec = A.rec.p;
+    in.ctrl = A.ctrl.p;
+    in.views = views;
+    in.rank = A.rank.p;
+    in.offs = A.offs.p;
+    in.rect_sorted = A.rect_sorted.p;
+    launch_blend_backward(in, static_cast<unsigned>(P.tiles), P.shape.tile_w, P.shape.tile_h, t->grad_pair.p, st);
+    for (size_t k = 0; k < P.views.size(); ++k) {
+        const unsigned s = P.views[k].scene;
+        const aniso_b200_raw_grads& g = grads[s];
+        const RawGrads out{g.means, g.log_scales, g.quats, g.opacity_logits, g.sh};
+        launch_gauss_backward(P.scenes[s].src, P.views[k].cam, P.views[k].entry_base, A.ctrl.p, A.depth_key.p,
+                              A.rank.p, A.offs.p, A.rect_sorted.p, t->grad_pair.p, out, st);
+    }
+    AB_TRY(slot.mark(st));
+    AB_CUDA(cudaGetLastError());
+    return ANISO_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int aniso_b200_trainer_create(aniso_b200_trainer** out) {
     if (!out) return fail(ANISO_B200_ERR_ARGUMENT, "out is NULL");
-    int count = 0;
-    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
-        cudaGetLastError();
-        return fail(ANISO_B200_ERR_NO_DEVICE, "no CUDA device");
-    }
+    AB_TRY(device_present());
     aniso_b200_trainer* t = new (std::nothrow) aniso_b200_trainer();
     if (!t) return fail(ANISO_B200_ERR_OUT_OF_MEMORY, "host allocation failed");
     cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&t->host_ctrl), sizeof(Ctrl));
@@ -737,125 +1218,40 @@ int aniso_b200_trainer_create(aniso_b200_trainer** out) {
 }
 
 int aniso_b200_trainer_destroy(aniso_b200_trainer* t) {
-    if (t) cudaDeviceSynchronize();
     delete t;
     return ANISO_B200_OK;
 }
 
 int aniso_b200_train_forward(aniso_b200_trainer* t, const aniso_b200_raw_params* params, const aniso_b200_camera* camera,
                              const aniso_b200_options* options, float* image_device, void* stream) {
-    if (!t || !params || !image_device) return fail(ANISO_B200_ERR_ARGUMENT, "trainer/params/image is NULL");
-    const aniso_b200_raw_params& P = *params;
-    if (P.n < 0 || P.n >= (int64_t(1) << 31)) return fail(ANISO_B200_ERR_ARGUMENT, "n must be in [0, 2^31)");
-    if (P.sh_degree != 1 && P.sh_degree != 3)
-        return fail(ANISO_B200_ERR_ARGUMENT, "stored SH degree must be 1 or 3 (whole 16-byte words per Gaussian)");
-    if (P.n > 0 && (!P.means || !P.log_scales || !P.quats || !P.opacity_logits || !P.sh))
-        return fail(ANISO_B200_ERR_ARGUMENT, "a parameter pointer is NULL");
-    if ((reinterpret_cast<uintptr_t>(P.quats) | reinterpret_cast<uintptr_t>(P.sh)) & 15)
-        return fail(ANISO_B200_ERR_ARGUMENT, "quats and sh must be 16-byte aligned");
-    CamParams cam;
-    AB_TRY(pack_camera_deg(P.sh_degree, camera, options, cam));
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    Arena& A = t->arena;
-    if (A.n < P.n) {
-        const uint64_t cap = std::max<uint64_t>(1u << 20, 4ull * static_cast<uint64_t>(P.n));
-        A.~Arena();
-        new (&A) Arena();
-        AB_TRY(A.init(P.n, static_cast<unsigned>(std::min<uint64_t>(cap, 0x3FFFFFFFull))));
-    }
-    const size_t pixels = static_cast<size_t>(cam.width) * cam.height;
-    AB_TRY(t->t_final.reserve(pixels));
-    AB_TRY(t->n_contrib.reserve(pixels));
-    RawParams raw;
-    raw.means = P.means;
-    raw.log_scales = P.log_scales;
-    raw.quats = reinterpret_cast<const float4*>(P.quats);
-    raw.logits = P.opacity_logits;
-    raw.sh = reinterpret_cast<const float4*>(P.sh);
-    raw.n = P.n;
-    raw.sh_planes = (P.sh_degree + 1) * (P.sh_degree + 1) * 3 / 4;
-    BlendOut out;
-    out.rgbf = image_device;
-    out.t_final = t->t_final.p;
-    out.n_contrib = t->n_contrib.p;
-    const int64_t saved_n = A.n;
-    A.n = P.n;  // grids follow this frame's Gaussian count
-    int rc = ANISO_B200_OK;
-    for (int attempt = 0; attempt < 3; ++attempt) {
-        rc = A.tick(st);
-        if (rc) break;
-        launch_frame_begin(A.ctrl.p, st);
-        launch_preprocess_raw(raw, cam, A.ctrl.p, A.rec.p, A.rect16.p, A.depth_key.p, st);
-        int fin = 0;
-        rc = enqueue_sort(A, cam.tilesX, cam.tilesY, st, &fin);
-        if (rc) break;
-        launch_blend(A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, cam.width, cam.height, cam.tilesX, cam.tilesY,
-                     out, st);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(t->host_ctrl, A.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) {
-            rc = cuda_fail(e, "train forward");
-            break;
-        }
-        const Ctrl& h = *t->host_ctrl;
-        if (h.flags & kFlagTimeout) {
-            rc = fail(ANISO_B200_ERR_DEVICE_WAIT, "a device-side look-back wait gave up");
-            break;
-        }
-        if (h.flags & kFlagOverflow) {
-            const uint64_t need = h.pair_total + h.pair_total / 4 + 1024;
-            if (need > 0x3FFFFFFFull) {
-                rc = fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 splat-tile pairs");
-                break;
-            }
-            rc = A.grow_pairs(static_cast<unsigned>(need));
-            if (rc) break;
-            rc = fail(ANISO_B200_ERR_ARGUMENT, "pair capacity kept overflowing");
-            continue;
-        }
-        t->has_forward = true;
-        t->raw = raw;
-        t->cam = cam;
-        t->fin = fin;
-        rc = ANISO_B200_OK;
-        break;
-    }
-    A.n = std::max(A.n, saved_n);
-    if (rc != ANISO_B200_OK) t->has_forward = false;
-    return rc;
+    if (!image_device) return fail(ANISO_B200_ERR_ARGUMENT, "image is NULL");
+    if (options && options->sh_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
+    const int32_t vs = 0;
+    float* images[1] = {image_device};
+    return train_forward(t, params, 1, &vs, camera, 1, scene_shape(options), images, static_cast<cudaStream_t>(stream));
 }
 
 int aniso_b200_train_backward(aniso_b200_trainer* t, const float* grad_image_device, const aniso_b200_raw_grads* grads,
                               void* stream) {
-    if (!t || !grad_image_device || !grads) return fail(ANISO_B200_ERR_ARGUMENT, "trainer/grad_image/grads is NULL");
-    if (!t->has_forward) return fail(ANISO_B200_ERR_ARGUMENT, "no forward to differentiate");
-    if (t->raw.n > 0 && (!grads->means || !grads->log_scales || !grads->quats || !grads->opacity_logits || !grads->sh))
-        return fail(ANISO_B200_ERR_ARGUMENT, "a gradient pointer is NULL");
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    Arena& A = t->arena;
-    const Ctrl& h = *t->host_ctrl;
-    AB_TRY(t->grad_pair.reserve(std::max<uint64_t>(h.pair_total, 1) * 9));
-    BackwardIn in;
-    in.ranges = A.ranges.p;
-    in.vals = A.pair_val[t->fin].p;
-    in.rec = A.rec.p;
-    in.ctrl = A.ctrl.p;
-    in.t_final = t->t_final.p;
-    in.n_contrib = t->n_contrib.p;
-    in.grad_img = grad_image_device;
-    in.rank = A.rank.p;
-    in.offs = A.offs.p;
-    in.rect_sorted = A.rect_sorted.p;
-    in.width = t->cam.width;
-    in.height = t->cam.height;
-    in.tiles_x = t->cam.tilesX;
-    launch_blend_backward(in, t->cam.tilesY, t->grad_pair.p, st);
-    RawGrads g{grads->means, grads->log_scales, grads->quats, grads->opacity_logits, grads->sh};
-    launch_gauss_backward(t->raw, t->cam, A.ctrl.p, A.vis_idx[A.sorted_buf()].p, A.offs.p, A.rect_sorted.p,
-                          t->grad_pair.p, h.vis_count, g, st);
-    AB_CUDA(cudaGetLastError());
-    return ANISO_B200_OK;
+    if (!grad_image_device) return fail(ANISO_B200_ERR_ARGUMENT, "grad_image is NULL");
+    const float* g[1] = {grad_image_device};
+    return train_backward(t, g, grads, static_cast<cudaStream_t>(stream));
+}
+
+int aniso_b200_train_batch_forward(aniso_b200_trainer* t, const aniso_b200_raw_params* params, int32_t n_scenes,
+                                   const int32_t* view_scene, const aniso_b200_camera* cameras, int32_t n_views,
+                                   const aniso_b200_batch_options* options, float* const* images_device,
+                                   void* stream) {
+    PlanShape shape;
+    AB_TRY(check_options(options, shape));
+    if (n_scenes <= 0) return fail(ANISO_B200_ERR_ARGUMENT, "n_scenes must be > 0");
+    return train_forward(t, params, n_scenes, view_scene, cameras, n_views, shape, images_device,
+                         static_cast<cudaStream_t>(stream));
+}
+
+int aniso_b200_train_batch_backward(aniso_b200_trainer* t, const float* const* grad_images_device,
+                                    const aniso_b200_raw_grads* grads, void* stream) {
+    return train_backward(t, grad_images_device, grads, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

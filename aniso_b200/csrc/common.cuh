@@ -79,6 +79,50 @@ struct RawParams {
     }
 };
 
+// ---- batches: V views of S scenes rendered by one launch sequence ----------------------------
+// Each (view, Gaussian of its scene) is an entry with a global index entry_base + i; each
+// (view, tile) a global tile tile_base + local tile. Entries of one view, and tiles of one view,
+// are contiguous; views of one scene are contiguous.
+struct ViewInfo {
+    CamParams cam;          // tilesX / tilesY in units of the batch's tile shape
+    unsigned scene;
+    unsigned entry_base;
+    unsigned tile_base;
+    unsigned n;             // Gaussians of its scene
+    uint8_t* rgb8;          // outputs, any may be null: RGB8 image, float colour, and for the
+    float* rgbf;            // backward the final transmittance and last contributor per pixel
+    float* t_final;
+    unsigned* n_contrib;
+    const float* grad_img;  // dL/d(colour) of the view, for the backward
+};
+
+template <class Src>
+struct BatchScene {
+    Src src;
+    unsigned view_begin, view_end;  // its views
+    unsigned block_base;            // its first preprocess block
+};
+
+// Compact per-view tables of a batch (device arrays of n_views entries) for the kernels that map
+// an entry or a global tile back to its view.
+struct BatchTables {
+    const unsigned* entry_base;
+    const unsigned* tile_base;
+    const unsigned* tiles_x;
+    unsigned n_views;
+};
+
+// Largest k in [0, count) with bases[k] <= x (bases ascending, bases[0] <= x).
+__device__ __forceinline__ unsigned find_segment(const unsigned* bases, unsigned count, unsigned x) {
+    unsigned lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const unsigned mid = (lo + hi + 1) >> 1;
+        if (bases[mid] <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 // Control block of one frame. Zeroed (except epoch, which advances) by frame_begin.
 struct Ctrl {
     unsigned long long pair_total;  // sum of tiles touched over visible Gaussians

@@ -23,11 +23,14 @@ struct DebugProjection {
 // Clears the frame's control block (counters, histograms, flags) and advances its epoch.
 void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
 
-void launch_preprocess(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
-                       unsigned long long* rect16, unsigned* depth_key, const DebugProjection* dbg,
-                       cudaStream_t stream);
+// Projection of every (view, Gaussian) entry of a batch; `blocks` = sum over scenes of
+// ceil(n / 256) (scene s starts at block scenes[s].block_base).
+void launch_preprocess(const BatchScene<SceneView>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
+                       int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec, unsigned long long* rect16,
+                       unsigned* depth_key, const DebugProjection* dbg, cudaStream_t stream);
 // The same projection of the optimizer's raw tensors (activated in the kernel).
-void launch_preprocess_raw(const RawParams& params, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
+void launch_preprocess_raw(const BatchScene<RawParams>* scenes, unsigned n_scenes, unsigned blocks,
+                           const ViewInfo* views, int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec,
                            unsigned long long* rect16, unsigned* depth_key, cudaStream_t stream);
 
 // One stable onesweep LSD radix pass over (key, value) u32 pairs, 8-bit digit at `shift`; `hist` is
@@ -53,8 +56,8 @@ struct DupBuffers {
 unsigned pair_scan_chunk_items();
 unsigned expand_chunk_pairs();
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
-                      unsigned max_visible, int tiles_x, int tile_passes, const DupBuffers& buf, unsigned* pair_key,
-                      unsigned* pair_val, unsigned long long* status, cudaStream_t stream);
+                      unsigned max_visible, const BatchTables& tables, int tile_passes, const DupBuffers& buf,
+                      unsigned* pair_key, unsigned* pair_val, unsigned long long* status, cudaStream_t stream);
 
 // ranges[tile] = [start, end) over the sorted tile keys (gpu_render.cu:164-177); ranges must be
 // zeroed before.
@@ -66,33 +69,26 @@ void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capac
 void launch_projection_keys(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
                             Ctrl* ctrl, unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream);
 
-// Blend outputs.
-struct BlendOut {
-    uint8_t* rgb8 = nullptr;        // H x W x 3 (gpu_render.cu:227-232 rounding)
-    float* rgbf = nullptr;          // H x W x 3 unclamped colour (differentiable path)
-    float* t_final = nullptr;       // H x W transmittance after the last applied splat
-    unsigned* n_contrib = nullptr;  // H x W: position in the tile list one past the last applied splat
-};
-
-void launch_blend(const uint2* ranges, const unsigned* sorted_vals, const SplatRecord* rec, const Ctrl* ctrl,
-                  int width, int height, int tiles_x, int tiles_y, const BlendOut& out, cudaStream_t stream);
+// Blends every tile of a batch (blockIdx = global tile); outputs go to each view's ViewInfo.
+// train: also the float colour, final transmittance and last contributor per pixel.
+bool blend_shape_supported(int tile_w, int tile_h);
+void launch_blend(unsigned tiles, const uint2* ranges, const unsigned* sorted_vals, const SplatRecord* rec,
+                  const Ctrl* ctrl, const ViewInfo* views, const BatchTables& tables, int tile_w, int tile_h,
+                  int batch, bool train, cudaStream_t stream);
 
 // ---- the adjoint ----------------------------------------------------------------------------
 struct BackwardIn {
     const uint2* ranges;
-    const unsigned* vals;                // sorted pair values (Gaussian indices)
+    const unsigned* vals;                // sorted pair values (entries)
     const SplatRecord* rec;
     const Ctrl* ctrl;
-    const float* t_final;                // H x W, from the training forward
-    const unsigned* n_contrib;           // H x W
-    const float* grad_img;               // H x W x 3, dL/d(colour)
-    const unsigned* rank;                // depth-sorted position of each Gaussian
-    const unsigned* offs;                // pair offset of each depth-sorted Gaussian
+    const ViewInfo* views;               // t_final, n_contrib, grad_img per view
+    BatchTables tables;
+    const unsigned* rank;                // depth-sorted position of each visible entry
+    const unsigned* offs;                // pair offset of each depth-sorted entry
     const unsigned long long* rect_sorted;
-    int width, height, tiles_x;
 };
-// Gradients of the raw parameters (device, the layout of RawParams; overwritten for visible
-// Gaussians, left untouched for culled ones -- callers zero them).
+// Gradients of the raw parameters of one scene (device, the layout of RawParams). Added to.
 struct RawGrads {
     float* means;
     float* log_scales;
@@ -101,9 +97,12 @@ struct RawGrads {
     float* sh;
 };
 // grad_pair: 9 floats per pair, at the pair's depth-ordered slot.
-void launch_blend_backward(const BackwardIn& in, int tiles_y, float* grad_pair, cudaStream_t stream);
-void launch_gauss_backward(const RawParams& raw, const CamParams& cam, const Ctrl* ctrl, const unsigned* sorted_idx,
-                           const unsigned* offs, const unsigned long long* rect_sorted, const float* grad_pair,
-                           unsigned max_visible, const RawGrads& out, cudaStream_t stream);
+void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int tile_h, float* grad_pair,
+                           cudaStream_t stream);
+// One view: its scene's Gaussians visible in it add their gradients to `out`.
+void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
+                           const unsigned* depth_key, const unsigned* rank, const unsigned* offs,
+                           const unsigned long long* rect_sorted, const float* grad_pair, const RawGrads& out,
+                           cudaStream_t stream);
 
 }  // namespace ab2

@@ -1,4 +1,5 @@
-// Step 1 of the rasterizer: one thread per Gaussian.
+// Step 1 of the rasterizer: one thread per Gaussian of a scene, for all the views of the scene in
+// the batch.
 //
 // Projects each Gaussian the way gpu_render.cu:86-145 does (the same fp32 expressions in the same
 // order, compiled without fast-math, so depth, rectangle and conic come out bit-identical to the
@@ -58,9 +59,10 @@ struct Projected {
     int x0, y0, x1, y1;       // 16x16-tile rectangle
 };
 
-// The culling and projection of gpu_render.cu:93-135. Returns false when the Gaussian is culled.
+// The culling and projection of gpu_render.cu:93-135 (the rectangle in units of tile_w x tile_h
+// pixels; 16 x 16 is the reference's). Returns false when the Gaussian is culled.
 __device__ __forceinline__ bool project(const float4 pg, const float4 sg, const float4 q, const CamParams& cam,
-                                        Projected& o) {
+                                        int tile_w, int tile_h, Projected& o) {
     const float gx = pg.x, gy = pg.y, gz = pg.z;
     const float px = cam.R[0] * gx + cam.R[1] * gy + cam.R[2] * gz + cam.t[0];
     const float py = cam.R[3] * gx + cam.R[4] * gy + cam.R[5] * gz + cam.t[1];
@@ -108,8 +110,8 @@ __device__ __forceinline__ bool project(const float4 pg, const float4 sg, const 
     const float u = cam.fx * px / pz + cam.cx, v = cam.fy * py / pz + cam.cy;
     if (u + radius < 0 || v + radius < 0 || u - radius >= cam.width || v - radius >= cam.height) return false;
 
-    const int x0 = max(0, (int)(u - radius) / kTile), y0 = max(0, (int)(v - radius) / kTile);
-    const int x1 = min(cam.tilesX - 1, (int)(u + radius) / kTile), y1 = min(cam.tilesY - 1, (int)(v + radius) / kTile);
+    const int x0 = max(0, (int)(u - radius) / tile_w), y0 = max(0, (int)(v - radius) / tile_h);
+    const int x1 = min(cam.tilesX - 1, (int)(u + radius) / tile_w), y1 = min(cam.tilesY - 1, (int)(v + radius) / tile_h);
     if (x1 < x0 || y1 < y0) return false;
 
     o.u = u; o.v = v; o.depth = pz;
@@ -144,37 +146,66 @@ __device__ __forceinline__ unsigned axis_bounds(float centre, float cov, float t
     return pack_i16x2(lo, hi);
 }
 
+constexpr int kMaxStagedViews = 64;  // cameras of a scene's views kept in shared memory
+
+// One thread per Gaussian of one scene: its geometry is read once and projected for every view of
+// the scene (its SH words once, when it is first visible). Outputs are indexed by entry
+// (view entry_base + Gaussian index).
 template <int D, bool kDebug, class Src>
-__global__ void __launch_bounds__(256, 3) preprocess_kernel(Src sc, CamParams cam, Ctrl* __restrict__ ctrl,
-                                                         SplatRecord* __restrict__ rec,
-                                                         unsigned long long* __restrict__ rect16,
-                                                         unsigned* __restrict__ depth_key, DebugProjection dbg) {
+__global__ void __launch_bounds__(256, 3) preprocess_kernel(const BatchScene<Src>* __restrict__ scenes,
+                                                            unsigned n_scenes, const ViewInfo* __restrict__ views,
+                                                            int tile_w, int tile_h, Ctrl* __restrict__ ctrl,
+                                                            SplatRecord* __restrict__ rec,
+                                                            unsigned long long* __restrict__ rect16,
+                                                            unsigned* __restrict__ depth_key, DebugProjection dbg) {
     __shared__ unsigned s_hist[kMaxPasses * kRadix];
+    __shared__ CamParams s_cam[kMaxStagedViews];
+    __shared__ unsigned s_scene;
     const int tid = threadIdx.x;
     for (int k = tid; k < kMaxPasses * kRadix; k += 256) s_hist[k] = 0;
+    if (tid == 0) {
+        unsigned sidx = 0;
+        for (unsigned k = 1; k < n_scenes; ++k)
+            if (scenes[k].block_base <= blockIdx.x) sidx = k;
+        s_scene = sidx;
+    }
     __syncthreads();
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * 256 + tid;
+    const BatchScene<Src> sc = scenes[s_scene];
+    const unsigned nv = sc.view_end - sc.view_begin;
+    for (unsigned k = tid; k < min(nv, static_cast<unsigned>(kMaxStagedViews)) * (sizeof(CamParams) / 4); k += 256)
+        reinterpret_cast<unsigned*>(s_cam)[k] =
+            reinterpret_cast<const unsigned*>(&views[sc.view_begin + k / (sizeof(CamParams) / 4)].cam)[k % (sizeof(CamParams) / 4)];
+    __syncthreads();
+    const int64_t i = static_cast<int64_t>(blockIdx.x - sc.block_base) * 256 + tid;
 
-    bool vis = false;
-    unsigned depth_bits = 0;
-    if (i < sc.n) {
+    if (i < sc.src.n) {
         float4 pg, sg, q;
-        sc.load(i, pg, sg, q);
-        Projected p;
-        vis = project(pg, sg, q, cam, p);
-        if (kDebug) dbg.tiles_touched[i] = 0;
-        if (vis) {
-            // Colour along the unit direction from the camera centre (gpu_render.cu:137-139).
-            constexpr int planes = ((D + 1) * (D + 1) * 3 + 3) / 4;
-            float sh[planes * 4];
-#pragma unroll
-            for (int k = 0; k < planes; ++k) {
-                const float4 f = sc.sh[i * sc.sh_planes + k];
-                sh[4 * k + 0] = f.x;
-                sh[4 * k + 1] = f.y;
-                sh[4 * k + 2] = f.z;
-                sh[4 * k + 3] = f.w;
+        sc.src.load(i, pg, sg, q);
+        constexpr int planes = ((D + 1) * (D + 1) * 3 + 3) / 4;
+        float sh[planes * 4];
+        bool have_sh = false;
+        for (unsigned vk = 0; vk < nv; ++vk) {
+            const CamParams& cam = vk < kMaxStagedViews ? s_cam[vk] : views[sc.view_begin + vk].cam;
+            const unsigned e = views[sc.view_begin + vk].entry_base + static_cast<unsigned>(i);
+            Projected p;
+            const bool vis = project(pg, sg, q, cam, tile_w, tile_h, p);
+            if (kDebug) dbg.tiles_touched[e] = 0;
+            if (!vis) {
+                depth_key[e] = kCulledKey;
+                continue;
             }
+            if (!have_sh) {
+#pragma unroll
+                for (int k = 0; k < planes; ++k) {
+                    const float4 f = sc.src.sh[i * sc.src.sh_planes + k];
+                    sh[4 * k + 0] = f.x;
+                    sh[4 * k + 1] = f.y;
+                    sh[4 * k + 2] = f.z;
+                    sh[4 * k + 3] = f.w;
+                }
+                have_sh = true;
+            }
+            // Colour along the unit direction from the camera centre (gpu_render.cu:137-139).
             float3 d = make_float3(pg.x - cam.eye[0], pg.y - cam.eye[1], pg.z - cam.eye[2]);
             const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
             const float3 rgb = sh_color<D>(sh, d.x / len, d.y / len, d.z / len);
@@ -193,61 +224,65 @@ __global__ void __launch_bounds__(256, 3) preprocess_kernel(Src sc, CamParams ca
             r.r0 = make_float4(p.u, p.v, kHalfLog2e * p.conicA, kLog2e * p.conicB);
             r.r1 = make_float4(kHalfLog2e * p.conicC, log2f(opacity), rgb.x, rgb.y);
             r.r2 = make_float4(rgb.z, __uint_as_float(bx), __uint_as_float(by), 0.f);
-            rec[i] = r;
-            rect16[i] = static_cast<unsigned long long>(p.x0) | (static_cast<unsigned long long>(p.y0) << 16) |
+            rec[e] = r;
+            rect16[e] = static_cast<unsigned long long>(p.x0) | (static_cast<unsigned long long>(p.y0) << 16) |
                         (static_cast<unsigned long long>(p.x1) << 32) | (static_cast<unsigned long long>(p.y1) << 48);
-            depth_bits = __float_as_uint(p.depth);
+            // The depth key: visible depths are >= 0.2 (or the canonical NaN), so the sign bit of
+            // kCulledKey never collides. The first depth pass compacts the visible entries.
+            const unsigned depth_bits = __float_as_uint(p.depth);
+            depth_key[e] = depth_bits;
             if (kDebug) {
-                dbg.uv[i] = make_float2(p.u, p.v);
-                dbg.conic_opacity[i] = make_float4(p.conicA, p.conicB, p.conicC, opacity);
-                dbg.depth[i] = p.depth;
-                dbg.rgb[3 * i + 0] = rgb.x;
-                dbg.rgb[3 * i + 1] = rgb.y;
-                dbg.rgb[3 * i + 2] = rgb.z;
-                dbg.rect[i] = make_uint4(p.x0, p.y0, p.x1, p.y1);
-                dbg.tiles_touched[i] = static_cast<unsigned>((p.x1 - p.x0 + 1) * (p.y1 - p.y0 + 1));
+                dbg.uv[e] = make_float2(p.u, p.v);
+                dbg.conic_opacity[e] = make_float4(p.conicA, p.conicB, p.conicC, opacity);
+                dbg.depth[e] = p.depth;
+                dbg.rgb[3 * e + 0] = rgb.x;
+                dbg.rgb[3 * e + 1] = rgb.y;
+                dbg.rgb[3 * e + 2] = rgb.z;
+                dbg.rect[e] = make_uint4(p.x0, p.y0, p.x1, p.y1);
+                dbg.tiles_touched[e] = static_cast<unsigned>((p.x1 - p.x0 + 1) * (p.y1 - p.y0 + 1));
             }
 #pragma unroll
             for (int pass = 0; pass < kMaxPasses; ++pass)
                 atomicAdd(&s_hist[pass * kRadix + ((depth_bits >> (pass * kRadixBits)) & (kRadix - 1))], 1u);
         }
     }
-
-    // The depth key of every Gaussian, kCulledKey for culled ones: visible depths are >= 0.2 (or
-    // the canonical NaN), so the sign bit never collides. The first depth pass compacts the list.
-    if (i < sc.n) depth_key[i] = vis ? depth_bits : kCulledKey;
     __syncthreads();
     for (int k = tid; k < kMaxPasses * kRadix; k += 256)
         if (s_hist[k]) atomicAdd(&ctrl->depth_hist[k], s_hist[k]);
 }
 
 template <bool kDebug, class Src>
-void launch_preprocess_t(const Src& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec, unsigned long long* rect16,
-                         unsigned* depth_key, const DebugProjection& dbg, cudaStream_t stream) {
-    const unsigned blocks = static_cast<unsigned>((sc.n + 255) / 256);
+void launch_preprocess_t(const BatchScene<Src>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
+                         int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec,
+                         unsigned long long* rect16, unsigned* depth_key, const DebugProjection& dbg,
+                         cudaStream_t stream) {
     if (blocks == 0) return;
-    switch (cam.shDegree) {
-        case 0: preprocess_kernel<0, kDebug, Src><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
-        case 1: preprocess_kernel<1, kDebug, Src><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
-        case 2: preprocess_kernel<2, kDebug, Src><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
-        default: preprocess_kernel<3, kDebug, Src><<<blocks, 256, 0, stream>>>(sc, cam, ctrl, rec, rect16, depth_key, dbg); break;
+    switch (sh_degree) {
+        case 0: preprocess_kernel<0, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, ctrl, rec, rect16, depth_key, dbg); break;
+        case 1: preprocess_kernel<1, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, ctrl, rec, rect16, depth_key, dbg); break;
+        case 2: preprocess_kernel<2, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, ctrl, rec, rect16, depth_key, dbg); break;
+        default: preprocess_kernel<3, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, ctrl, rec, rect16, depth_key, dbg); break;
     }
 }
 
 }  // namespace
 
-void launch_preprocess(const SceneView& sc, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
-                       unsigned long long* rect16, unsigned* depth_key, const DebugProjection* dbg,
-                       cudaStream_t stream) {
+void launch_preprocess(const BatchScene<SceneView>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
+                       int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec, unsigned long long* rect16,
+                       unsigned* depth_key, const DebugProjection* dbg, cudaStream_t stream) {
     if (dbg)
-        launch_preprocess_t<true>(sc, cam, ctrl, rec, rect16, depth_key, *dbg, stream);
+        launch_preprocess_t<true>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, ctrl, rec, rect16,
+                                  depth_key, *dbg, stream);
     else
-        launch_preprocess_t<false>(sc, cam, ctrl, rec, rect16, depth_key, DebugProjection{}, stream);
+        launch_preprocess_t<false>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, ctrl, rec, rect16,
+                                   depth_key, DebugProjection{}, stream);
 }
 
-void launch_preprocess_raw(const RawParams& params, const CamParams& cam, Ctrl* ctrl, SplatRecord* rec,
+void launch_preprocess_raw(const BatchScene<RawParams>* scenes, unsigned n_scenes, unsigned blocks,
+                           const ViewInfo* views, int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec,
                            unsigned long long* rect16, unsigned* depth_key, cudaStream_t stream) {
-    launch_preprocess_t<false>(params, cam, ctrl, rec, rect16, depth_key, DebugProjection{}, stream);
+    launch_preprocess_t<false>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, ctrl, rec, rect16,
+                               depth_key, DebugProjection{}, stream);
 }
 
 }  // namespace ab2

@@ -30,7 +30,7 @@ constexpr int kOsItems = 8;
 constexpr int kOsChunk = kOsThreads * kOsItems;
 constexpr int kScanItems = 4;
 constexpr int kScanChunk = 256 * kScanItems;
-constexpr int kExpandChunk = 2048;
+constexpr int kExpandChunk = 1024;
 
 __global__ void frame_begin_kernel(Ctrl* ctrl) {
     const int tid = threadIdx.x;
@@ -265,12 +265,14 @@ __global__ void __launch_bounds__(256) expand_kernel(const unsigned* __restrict_
                                                      const unsigned long long* __restrict__ rect_sorted,
                                                      const unsigned* __restrict__ offs,
                                                      const unsigned* __restrict__ chunk_start, Ctrl* ctrl,
-                                                     unsigned capacity, int tiles_x, int tile_passes,
+                                                     unsigned capacity, BatchTables tables, int tile_passes,
                                                      unsigned* __restrict__ pair_key,
                                                      unsigned* __restrict__ pair_val) {
     __shared__ unsigned s_off[kExpandChunk + 1];
     __shared__ unsigned s_idx[kExpandChunk + 1];
     __shared__ unsigned long long s_rect[kExpandChunk + 1];
+    __shared__ unsigned s_tbase[kExpandChunk + 1];  // global tile of (0, 0) of the entry's view
+    __shared__ unsigned short s_tx[kExpandChunk + 1];  // tiles per row of the entry's view
     __shared__ unsigned s_hist[kMaxPasses * kRadix];
     const int tid = threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
@@ -285,29 +287,44 @@ __global__ void __launch_bounds__(256) expand_kernel(const unsigned* __restrict_
     const unsigned G = j1 - j0 + 1;  // <= kExpandChunk + 1: every Gaussian owns at least one pair
     for (unsigned k = tid; k < G; k += 256) {
         s_off[k] = offs[j0 + k];
-        s_idx[k] = sorted_idx[j0 + k];
+        const unsigned e = sorted_idx[j0 + k];
+        s_idx[k] = e;
         s_rect[k] = rect_sorted[j0 + k];
+        const unsigned v = find_segment(tables.entry_base, tables.n_views, e);
+        s_tbase[k] = tables.tile_base[v];
+        s_tx[k] = static_cast<unsigned short>(tables.tiles_x[v]);
     }
     __syncthreads();
     const unsigned n_here = static_cast<unsigned>(min(static_cast<unsigned long long>(kExpandChunk), P - base));
-    for (unsigned q = tid; q < n_here; q += 256) {
-        const unsigned p = base + q;
-        unsigned lo = 0, hi = G - 1;  // last k with s_off[k] <= p
-        while (lo < hi) {
-            const unsigned mid = (lo + hi + 1) >> 1;
-            if (s_off[mid] <= p) lo = mid;
-            else hi = mid - 1;
+    const int lane = tid & 31;
+    for (unsigned q0 = 0; q0 < n_here; q0 += 256) {  // uniform trip count: whole warps vote below
+        const unsigned q = q0 + tid;
+        unsigned tile = 0;
+        const bool valid = q < n_here;
+        if (valid) {
+            const unsigned p = base + q;
+            unsigned lo = 0, hi = G - 1;  // last k with s_off[k] <= p
+            while (lo < hi) {
+                const unsigned mid = (lo + hi + 1) >> 1;
+                if (s_off[mid] <= p) lo = mid;
+                else hi = mid - 1;
+            }
+            const unsigned k = p - s_off[lo];
+            const unsigned long long r = s_rect[lo];
+            const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu;
+            const unsigned w = x1 - x0 + 1;
+            const unsigned row = k / w;
+            tile = s_tbase[lo] + (y0 + row) * static_cast<unsigned>(s_tx[lo]) + x0 + (k - row * w);
+            pair_key[p] = tile;
+            pair_val[p] = s_idx[lo];
+            atomicAdd(&s_hist[tile & (kRadix - 1)], 1u);  // low digit: neighbours differ, few conflicts
         }
-        const unsigned k = p - s_off[lo];
-        const unsigned long long r = s_rect[lo];
-        const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu;
-        const unsigned w = x1 - x0 + 1;
-        const unsigned row = k / w;
-        const unsigned tile = (y0 + row) * static_cast<unsigned>(tiles_x) + x0 + (k - row * w);
-        pair_key[p] = tile;
-        pair_val[p] = s_idx[lo];
-        for (int ps = 0; ps < tile_passes; ++ps)
-            atomicAdd(&s_hist[ps * kRadix + ((tile >> (ps * kRadixBits)) & (kRadix - 1))], 1u);
+        // Higher digits repeat along a warp (neighbouring tiles share them): one add per distinct digit.
+        for (int ps = 1; ps < tile_passes; ++ps) {
+            const unsigned dg = valid ? (tile >> (ps * kRadixBits)) & (kRadix - 1) : kRadix;
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_hist[ps * kRadix + dg], __popc(peers));
+        }
     }
     __syncthreads();
     for (int k = tid; k < tile_passes * kRadix; k += 256)
@@ -384,7 +401,8 @@ unsigned pair_scan_chunk_items() { return kScanChunk; }
 unsigned expand_chunk_pairs() { return kExpandChunk; }
 
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
-                      unsigned max_visible, int tiles_x, int tile_passes, const DupBuffers& buf, unsigned* pair_key,
+                      unsigned max_visible, const BatchTables& tables, int tile_passes, const DupBuffers& buf,
+                      unsigned* pair_key,
                       unsigned* pair_val, unsigned long long* status, cudaStream_t stream) {
     const unsigned scan_blocks = (max_visible + kScanChunk - 1) / kScanChunk;
     if (scan_blocks == 0) return;
@@ -392,7 +410,7 @@ void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect
                                                       buf.rect_sorted, buf.chunk_start, status);
     const unsigned expand_blocks = (capacity + kExpandChunk - 1) / kExpandChunk;
     expand_kernel<<<expand_blocks, 256, 0, stream>>>(sorted_idx, buf.rect_sorted, buf.offs, buf.chunk_start, ctrl,
-                                                     capacity, tiles_x, tile_passes, pair_key, pair_val);
+                                                     capacity, tables, tile_passes, pair_key, pair_val);
 }
 
 void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capacity, uint2* ranges,

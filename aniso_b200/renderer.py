@@ -186,3 +186,67 @@ def keys_of(tiles: np.ndarray, values: np.ndarray, depth: np.ndarray) -> np.ndar
     """The reference's 64-bit sort keys (tile << 32 | depth bits, gpu_render.cu:157) of a pair list."""
     bits = np.ascontiguousarray(depth, np.float32).view(np.uint32)
     return (tiles.astype(np.uint64) << np.uint64(32)) | bits[values].astype(np.uint64)
+
+
+@dataclasses.dataclass
+class BatchOptions:
+    """aniso_b200_batch_options: colour options plus the launch shape (tile, blend batch, graph)."""
+
+    sh_degree: int = 3
+    splat_scale: float = 1.0
+    tile: tuple[int, int] = (16, 16)
+    blend_batch: int = 256
+    use_graph: bool = False
+
+    def c(self) -> _lib.BatchOptions:
+        return _lib.BatchOptions(int(self.sh_degree), float(self.splat_scale), int(self.tile[0]), int(self.tile[1]),
+                                 int(self.blend_batch), 1 if self.use_graph else 0)
+
+
+def c_cameras(cameras) -> ctypes.Array:
+    arr = (_lib.Camera * len(cameras))()
+    for k, cam in enumerate(cameras):
+        arr[k] = c_camera(cam)
+    return arr
+
+
+class BatchRenderer:
+    """Many views of several uploaded scenes in one launch sequence (aniso_b200_batch_*).
+
+    view_scene[k] names the scene (an index into `scenes`) of view k; the views of one scene are
+    consecutive. The scenes must stay alive as long as the batch.
+    """
+
+    def __init__(self, scenes: list[GpuRenderer], view_scene, options: BatchOptions | None = None):
+        self.scenes = list(scenes)
+        self.view_scene = np.ascontiguousarray(view_scene, np.int32)
+        self.options = options or BatchOptions()
+        handles = (ctypes.c_void_p * len(self.scenes))(*[s._h.value for s in self.scenes])
+        o = self.options.c()
+        self._h = ctypes.c_void_p()
+        check(lib.aniso_b200_batch_create(handles, len(self.scenes), _ptr(self.view_scene), len(self.view_scene),
+                                          ctypes.byref(o), ctypes.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.aniso_b200_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render_device(self, cameras, rgb_device_ptrs, stream_ptr: int = 0):
+        """Enqueues every view (camera k into device buffer rgb_device_ptrs[k]); no wait."""
+        if len(cameras) != len(self.view_scene) or len(rgb_device_ptrs) != len(self.view_scene):
+            raise ValueError("one camera and one output buffer per view")
+        cams = c_cameras(cameras)
+        ptrs = (ctypes.c_void_p * len(rgb_device_ptrs))(*[int(p) for p in rgb_device_ptrs])
+        check(lib.aniso_b200_batch_render(self._h, cams, ptrs, ctypes.c_void_p(stream_ptr)))
+
+    def sync(self) -> dict:
+        st = _lib.Stats()
+        check(lib.aniso_b200_batch_sync(self._h, ctypes.byref(st)))
+        return _stats_dict(st)

@@ -111,6 +111,39 @@ int aniso_b200_profile_read(aniso_b200_scene* scene, double* project_ms, double*
 /* Copies the last error message (NUL-terminated, truncated to len) and returns its full length. */
 size_t aniso_b200_last_error(char* buf, size_t len);
 
+/* ---- batches (no counterpart in the reference, whose multi-view caller renders views one by one
+ * with two host syncs each, main.cpp:233-244): many views of several scenes rendered by one fixed
+ * launch sequence. Every Gaussian is read once and projected for all views of its scene; one
+ * sort orders every view's pairs; one blend launch covers every tile of every view. ---------- */
+
+typedef struct aniso_b200_batch aniso_b200_batch;
+
+typedef struct aniso_b200_batch_options {
+    int32_t sh_degree;   /* colour up to this SH degree, clamped to every scene's and to 3 */
+    float splat_scale;   /* as aniso_b200_options */
+    int32_t tile_w;      /* tile shape: 8x8, 16x16 (the reference's, and the default for 0) or 16x32; */
+    int32_t tile_h;      /*   the image is the same for every shape */
+    int32_t blend_batch; /* splats staged per blend round: < 256 the smaller, >= 256 the larger set */
+    int32_t use_graph;   /* 1: record the launch sequence once as a CUDA graph and replay it */
+} aniso_b200_batch_options;
+
+/* A batch of n_views views; view k shows scene scenes[view_scene[k]]. The views of one scene must
+ * be consecutive. The scenes are not copied and must outlive the batch. */
+int aniso_b200_batch_create(aniso_b200_scene* const* scenes, int32_t n_scenes, const int32_t* view_scene,
+                            int32_t n_views, const aniso_b200_batch_options* options, aniso_b200_batch** out);
+
+/* Renders every view, camera k into the DEVICE RGB8 buffer rgb_device[k] (its width*height*3
+ * bytes), stream-ordered, without waiting. With use_graph, the first call (and any call whose
+ * image sizes differ from the recorded ones) records the graph; later calls replay it. */
+int aniso_b200_batch_render(aniso_b200_batch* batch, const aniso_b200_camera* cameras, uint8_t* const* rgb_device,
+                            void* stream);
+
+/* Waits for the batch's work and reports totals over its views; as aniso_b200_sync, returns
+ * ANISO_B200_ERR_ARGUMENT "pair capacity exceeded" if a render overflowed (capacity then grown). */
+int aniso_b200_batch_sync(aniso_b200_batch* batch, aniso_b200_stats* stats);
+
+int aniso_b200_batch_destroy(aniso_b200_batch* batch);
+
 /* ---- the differentiable path (no counterpart in the reference: it has no backward pass; the
  * training pipeline it drives calls the third-party gsplat rasterizer instead,
  * pipeline/train_gsplat.py:96-102) ----------------------------------------------------------- */
@@ -158,6 +191,17 @@ int aniso_b200_train_forward(aniso_b200_trainer* trainer, const aniso_b200_raw_p
  * Deterministic: no atomics; every sum runs in a fixed order. Enqueued on `stream`. */
 int aniso_b200_train_backward(aniso_b200_trainer* trainer, const float* grad_image_device,
                               const aniso_b200_raw_grads* grads, void* stream);
+
+/* The training-step shape: n_views views of n_scenes scenes (params[s], view k of scene
+ * view_scene[k], views of a scene consecutive) in one forward; images_device[k] receives view k.
+ * The backward adds each view's gradient to its scene's grads[s], views in order, so the sum over
+ * views is deterministic too. */
+int aniso_b200_train_batch_forward(aniso_b200_trainer* trainer, const aniso_b200_raw_params* params,
+                                   int32_t n_scenes, const int32_t* view_scene, const aniso_b200_camera* cameras,
+                                   int32_t n_views, const aniso_b200_batch_options* options,
+                                   float* const* images_device, void* stream);
+int aniso_b200_train_batch_backward(aniso_b200_trainer* trainer, const float* const* grad_images_device,
+                                    const aniso_b200_raw_grads* grads, void* stream);
 
 /* ---- introspection used by the parity tests (no counterpart in gpu_render.h) ---------------- */
 
