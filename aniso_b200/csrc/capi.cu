@@ -92,7 +92,6 @@ constexpr uint64_t kMaxPairs = 0x3FFFFFFFull;    // look-back status values are 
 struct Arena {
     int64_t n = -1;
     unsigned pair_cap = 0;
-    uint64_t frames = 0;
     DevBuf<SplatRecord> rec;
     DevBuf<unsigned long long> rect16;
     DevBuf<unsigned> depth_key;
@@ -102,10 +101,9 @@ struct Arena {
     DevBuf<unsigned long long> rect_sorted;
     DevBuf<uint2> ranges;
     DevBuf<Ctrl> ctrl;
-    DevBuf<unsigned long long> st_depth, st_dup, st_tile;
+    DevBuf<unsigned> sort_scratch;          // per-span digit counts of the pass in flight
+    DevBuf<unsigned long long> span_sum;    // pairs per span of the pair-offset scan
 
-    unsigned depth_chunks() const { return chunks_of(static_cast<uint64_t>(std::max<int64_t>(n, 1)), onesweep_chunk_items()); }
-    unsigned tile_chunks() const { return chunks_of(std::max(pair_cap, 1u), onesweep_chunk_items()); }
     // The vis_idx buffer that holds the depth-sorted visible list after the depth passes.
     static int sorted_buf() { return (kMaxPasses - 1) & 1; }
 
@@ -120,8 +118,8 @@ struct Arena {
             AB_TRY(vis_idx[k].reserve(nn));
         }
         AB_TRY(ctrl.reserve(1, true));
-        AB_TRY(st_depth.reserve(static_cast<size_t>(kMaxPasses) * depth_chunks() * kRadix, true));
-        AB_TRY(st_dup.reserve(chunks_of(nn, pair_scan_chunk_items()), true));
+        AB_TRY(sort_scratch.reserve(sort_scratch_words()));
+        AB_TRY(span_sum.reserve(sort_span_sums()));
         AB_TRY(offs.reserve(nn));
         AB_TRY(rank.reserve(nn));
         AB_TRY(rect_sorted.reserve(nn));
@@ -145,48 +143,34 @@ struct Arena {
             AB_TRY(pair_val[k].reserve(cap));
         }
         pair_cap = cap;
-        AB_TRY(chunk_start.reserve(chunks_of(cap, expand_chunk_pairs()) + 2));
-        st_tile.release();
-        return st_tile.reserve(static_cast<size_t>(kMaxPasses) * tile_chunks() * kRadix, true);
-    }
-
-    // Status words carry a 30-bit frame epoch; clear them long before it could wrap.
-    int tick(cudaStream_t st) {
-        if (++frames % (1ull << 29) == 0) {
-            AB_CUDA(cudaMemsetAsync(st_depth.p, 0, st_depth.cap * sizeof(unsigned long long), st));
-            AB_CUDA(cudaMemsetAsync(st_dup.p, 0, st_dup.cap * sizeof(unsigned long long), st));
-            AB_CUDA(cudaMemsetAsync(st_tile.p, 0, st_tile.cap * sizeof(unsigned long long), st));
-        }
-        return 0;
+        return chunk_start.reserve(chunks_of(cap, expand_chunk_pairs()) + 2);
     }
 };
 
 // Depth passes over `entries` depth keys (the first compacts the visible ones), pair scan and
 // expansion, tile passes over `tiles` global tiles, and ranges. *final_buf = the pair buffer that
-// holds the sorted pairs.
-int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, cudaStream_t st,
-                 int* final_buf) {
+// holds the sorted pairs. keep_rank: also record each visible entry's depth-sorted position (the
+// adjoint reads it).
+int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank,
+                 cudaStream_t st, int* final_buf) {
     Ctrl* ctrl = A.ctrl.p;
     const unsigned cap = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
     for (int p = 0; p < kMaxPasses; ++p) {
         const int src = (p + 1) & 1, dst = p & 1;  // pass 0 reads depth_key and writes buffer 0
-        launch_onesweep(p == 0 ? A.depth_key.p : A.vis_key[src].p, p == 0 ? nullptr : A.vis_idx[src].p,
-                        p == kMaxPasses - 1 ? nullptr : A.vis_key[dst].p, A.vis_idx[dst].p, p == 0 ? entries : 0u,
-                        p == 0 ? entries : cap, p * kRadixBits, &ctrl->depth_hist[p * kRadix],
-                        A.st_depth.p + static_cast<size_t>(p) * A.depth_chunks() * kRadix,
-                        &ctrl->chunk_ctr[kCtrDepth0 + p], ctrl, st);
+        launch_radix_pass(p == 0 ? A.depth_key.p : A.vis_key[src].p, p == 0 ? nullptr : A.vis_idx[src].p,
+                          p == kMaxPasses - 1 ? nullptr : A.vis_key[dst].p, A.vis_idx[dst].p, p == 0,
+                          p == 0 ? SortCount::kFixed : SortCount::kVisible, entries, p == 0 ? entries : cap,
+                          p * kRadixBits, A.sort_scratch.p, ctrl, st);
     }
     const int sorted = Arena::sorted_buf();
     const int tile_passes = std::max(1, (bits_for(tiles - 1) + kRadixBits - 1) / kRadixBits);
-    const DupBuffers dup{A.offs.p, A.rank.p, A.rect_sorted.p, A.chunk_start.p};
-    launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, tile_passes, dup,
-                     A.pair_key[0].p, A.pair_val[0].p, A.st_dup.p, st);
+    const DupBuffers dup{A.offs.p, keep_rank ? A.rank.p : nullptr, A.rect_sorted.p, A.chunk_start.p, A.span_sum.p};
+    launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, dup, A.pair_key[0].p,
+                     A.pair_val[0].p, st);
     for (int p = 0; p < tile_passes; ++p) {
         const int src = p & 1, dst = src ^ 1;
-        launch_onesweep(A.pair_key[src].p, A.pair_val[src].p, A.pair_key[dst].p, A.pair_val[dst].p, 0u, A.pair_cap,
-                        p * kRadixBits, &ctrl->tile_hist[p * kRadix],
-                        A.st_tile.p + static_cast<size_t>(p) * A.tile_chunks() * kRadix,
-                        &ctrl->chunk_ctr[kCtrTile0 + p], ctrl, st);
+        launch_radix_pass(A.pair_key[src].p, A.pair_val[src].p, A.pair_key[dst].p, A.pair_val[dst].p, false,
+                          SortCount::kPairs, 0u, A.pair_cap, p * kRadixBits, A.sort_scratch.p, ctrl, st);
     }
     const int fin = tile_passes & 1;
     AB_TRY(A.ranges.reserve(tiles));
@@ -387,15 +371,15 @@ struct Slot {
     }
 };
 
-void launch_preprocess_any(const BatchScene<SceneView>* sc, const Plan<SceneView>& P, const ViewInfo* views, Ctrl* ctrl,
-                           Arena& A, const DebugProjection* dbg, cudaStream_t st) {
+void launch_preprocess_any(const BatchScene<SceneView>* sc, const Plan<SceneView>& P, const ViewInfo* views, Arena& A,
+                           const DebugProjection* dbg, cudaStream_t st) {
     launch_preprocess(sc, static_cast<unsigned>(P.scenes.size()), P.pre_blocks, views, P.rendered_degree(),
-                      P.shape.tile_w, P.shape.tile_h, ctrl, A.rec.p, A.rect16.p, A.depth_key.p, dbg, st);
+                      P.shape.tile_w, P.shape.tile_h, A.rec.p, A.rect16.p, A.depth_key.p, dbg, st);
 }
 void launch_preprocess_any(const BatchScene<RawParams>* sc, const Plan<RawParams>& P, const ViewInfo* views,
-                           Ctrl* ctrl, Arena& A, const DebugProjection*, cudaStream_t st) {
+                           Arena& A, const DebugProjection*, cudaStream_t st) {
     launch_preprocess_raw(sc, static_cast<unsigned>(P.scenes.size()), P.pre_blocks, views, P.rendered_degree(),
-                          P.shape.tile_w, P.shape.tile_h, ctrl, A.rec.p, A.rect16.p, A.depth_key.p, st);
+                          P.shape.tile_w, P.shape.tile_h, A.rec.p, A.rect16.p, A.depth_key.p, st);
 }
 
 // Enqueues one frame of a plan. ev (4 events, may be NULL) brackets the stages.
@@ -408,10 +392,10 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     AB_TRY(slot.fill(P, st, &views, &scenes, tables));
     if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
     launch_frame_begin(A.ctrl.p, st);
-    launch_preprocess_any(scenes, P, views, A.ctrl.p, A, dbg, st);
+    launch_preprocess_any(scenes, P, views, A, dbg, st);
     if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
     int fin = 0;
-    AB_TRY(enqueue_sort(A, static_cast<unsigned>(P.entries), static_cast<unsigned>(P.tiles), tables, st, &fin));
+    AB_TRY(enqueue_sort(A, static_cast<unsigned>(P.entries), static_cast<unsigned>(P.tiles), tables, train, st, &fin));
     if (ev) AB_CUDA(cudaEventRecord(ev[2], st));
     if (!stop_after_sort)
         launch_blend(static_cast<unsigned>(P.tiles), A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, views, tables,
@@ -439,7 +423,6 @@ int settle(Arena& A, const Ctrl& h, int* again, bool all_frames) {
     *again = 0;
     const unsigned flags = h.flags | (all_frames ? h.sticky_flags : 0u);
     const uint64_t pairs = all_frames ? std::max(h.pair_total, h.max_pair_total) : h.pair_total;
-    if (flags & kFlagTimeout) return fail(ANISO_B200_ERR_DEVICE_WAIT, "a device-side look-back wait gave up");
     if (flags & kFlagOverflow) {
         const uint64_t need = pairs + pairs / 4 + 1024;
         if (need > kMaxPairs) return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 splat-tile pairs");
@@ -725,7 +708,6 @@ int aniso_b200_render(aniso_b200_scene* s, const aniso_b200_camera* camera, cons
     AB_TRY(s->image.reserve(bytes));
     P.views[0].rgb8 = s->image.p;
     for (int attempt = 0; attempt < 3; ++attempt) {
-        AB_TRY(s->arena.tick(s->stream));
         AB_TRY(enqueue_plan(s->arena, s->slot(), P, s->stream, stats ? s->ev : nullptr, nullptr, false, false,
                             nullptr));
         AB_CUDA(cudaMemcpyAsync(rgb_host, s->image.p, bytes, cudaMemcpyDeviceToHost, s->stream));
@@ -765,7 +747,6 @@ int aniso_b200_render_device(aniso_b200_scene* s, const aniso_b200_camera* camer
         ev = &s->prof_ev[4 * s->prof_frames++];
     }
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    AB_TRY(s->arena.tick(st));
     return enqueue_plan(s->arena, s->slot(), P, st, ev, nullptr, false, false, nullptr);
 }
 
@@ -844,7 +825,7 @@ int aniso_b200_debug_projection(aniso_b200_scene* s, const aniso_b200_camera* ca
     Slot& slot = s->slot();
     AB_TRY(slot.fill(P, s->stream, &views, &scenes, tables));
     launch_frame_begin(A.ctrl.p, s->stream);
-    launch_preprocess_any(scenes, P, views, A.ctrl.p, A, &dbg, s->stream);
+    launch_preprocess_any(scenes, P, views, A, &dbg, s->stream);
     AB_TRY(slot.mark(s->stream));
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaStreamSynchronize(s->stream));
@@ -865,7 +846,6 @@ int aniso_b200_debug_sorted(aniso_b200_scene* s, const aniso_b200_camera* camera
     AB_TRY(single_plan(s, camera, options, P));
     int fin = 0;
     for (int attempt = 0; attempt < 3; ++attempt) {
-        AB_TRY(s->arena.tick(s->stream));
         AB_TRY(enqueue_plan(s->arena, s->slot(), P, s->stream, nullptr, nullptr, true, false, &fin));
         AB_TRY(read_ctrl(s->arena, s->host_ctrl, s->stream));
         int again = 0;
@@ -915,17 +895,15 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     }
     cudaStream_t st = nullptr;
     const BatchTables tables{dtab.p, dtab.p + 1, dtab.p + 2, 1u};
-    AB_TRY(A.tick(st));
     launch_frame_begin(A.ctrl.p, st);
-    launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.ctrl.p, A.depth_key.p, A.rect16.p, st);
+    launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.depth_key.p, A.rect16.p, st);
     int fin = 0;
     const unsigned T = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
-    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, st, &fin));
+    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, st, &fin));
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaDeviceSynchronize());
     Ctrl h;
     AB_CUDA(cudaMemcpy(&h, A.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-    if (h.flags & kFlagTimeout) return fail(ANISO_B200_ERR_DEVICE_WAIT, "a device-side look-back wait gave up");
     if (h.pair_total != Pn) return fail(ANISO_B200_ERR_CUDA, "device pair count disagrees with the host");
     if (tiles && Pn) AB_CUDA(cudaMemcpy(tiles, A.pair_key[fin].p, Pn * sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (values && Pn) AB_CUDA(cudaMemcpy(values, A.pair_val[fin].p, Pn * sizeof(unsigned), cudaMemcpyDeviceToHost));
@@ -1012,7 +990,6 @@ int aniso_b200_batch_render(aniso_b200_batch* b, const aniso_b200_camera* camera
         b->graph = nullptr;
     }
     AB_TRY(b->arena.ensure(static_cast<int64_t>(std::max<uint64_t>(P.entries, 1))));
-    AB_TRY(b->arena.tick(st));
     if (!b->use_graph)
         return enqueue_plan(b->arena, b->slots[b->next_slot++ % kSlots], P, st, nullptr, nullptr, false, false,
                             nullptr);
@@ -1142,7 +1119,6 @@ int train_forward(aniso_b200_trainer* t, const aniso_b200_raw_params* params, in
     Arena& A = t->arena;
     AB_TRY(A.ensure(static_cast<int64_t>(std::max<uint64_t>(P.entries, 1))));
     for (int attempt = 0; attempt < 3; ++attempt) {
-        AB_TRY(A.tick(st));
         int fin = 0;
         AB_TRY(enqueue_plan(A, t->slot(), P, st, nullptr, nullptr, false, true, &fin));
         AB_TRY(read_ctrl(A, t->host_ctrl, st));

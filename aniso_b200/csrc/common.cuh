@@ -27,7 +27,6 @@ constexpr int kCpuTile = 8;   // the CPU renderer's binning tile (render.cpp:16)
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kMaxPasses = 4;
-constexpr unsigned kSpinLimit = 1u << 20;  // bound on every look-back wait
 
 // Per-view constants, packed on the host exactly as gpu_render.cu:301-316 packs CameraParams.
 struct CamParams {
@@ -123,17 +122,14 @@ __device__ __forceinline__ unsigned find_segment(const unsigned* bases, unsigned
     return lo;
 }
 
-// Control block of one frame. Zeroed (except epoch, which advances) by frame_begin.
+// Control block of one frame. Cleared (the flags folded into the sticky ones) by frame_begin.
 struct Ctrl {
-    unsigned long long pair_total;  // sum of tiles touched over visible Gaussians
-    unsigned int vis_count;         // visible Gaussians
-    unsigned int flags;             // kFlag* bits, read back by the host after the frame
-    unsigned int epoch;             // tags look-back status words of this frame
-    unsigned int sticky_flags;      // OR of the flags of earlier frames since the host last read it
+    unsigned long long pair_total;      // sum of tiles touched over visible entries
+    unsigned int vis_count;             // visible entries
+    unsigned int flags;                 // kFlag* bits, read back by the host after the frame
+    unsigned int sticky_flags;          // OR of the flags of earlier frames since the host last read it
+    unsigned int pad;
     unsigned long long max_pair_total;  // largest pair_total of earlier frames since then
-    unsigned int chunk_ctr[16];     // dynamic chunk counters, one per kernel launch of the frame
-    unsigned int depth_hist[kMaxPasses * kRadix];
-    unsigned int tile_hist[kMaxPasses * kRadix];
 };
 
 // Depth key of a culled Gaussian. Visible depths are >= 0.2 (or a canonical NaN), so their float
@@ -142,28 +138,7 @@ constexpr unsigned kCulledKey = 0xFFFFFFFFu;
 
 enum : unsigned {
     kFlagOverflow = 1u,  // pairs exceeded the pair capacity: nothing after duplication ran
-    kFlagTimeout = 2u,   // a look-back wait hit kSpinLimit (never expected)
 };
-
-// Chunk counter slots.
-enum : int { kCtrDepth0 = 1, kCtrDup = 5, kCtrTile0 = 6 };
-
-// ---- look-back status words: [epoch:30][flag:2][value:32] ------------------------------------
-enum : unsigned { kStAgg = 1u, kStInc = 2u };
-
-__device__ __forceinline__ unsigned long long st_make(unsigned epoch, unsigned flag, unsigned value) {
-    return (static_cast<unsigned long long>(epoch & 0x3FFFFFFFu) << 34) |
-           (static_cast<unsigned long long>(flag) << 32) | value;
-}
-__device__ __forceinline__ unsigned st_flag(unsigned long long s, unsigned epoch) {
-    return (static_cast<unsigned>(s >> 34) == (epoch & 0x3FFFFFFFu)) ? static_cast<unsigned>(s >> 32) & 3u : 0u;
-}
-__device__ __forceinline__ void st_store(unsigned long long* p, unsigned long long v) {
-    *reinterpret_cast<volatile unsigned long long*>(p) = v;
-}
-__device__ __forceinline__ unsigned long long st_load(const unsigned long long* p) {
-    return *reinterpret_cast<const volatile unsigned long long*>(p);
-}
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
@@ -201,58 +176,6 @@ __device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* s_tmp,
     const unsigned before = warp > 0 ? s_tmp[warp - 1] : 0u;
     __syncthreads();
     return before + incl - v;
-}
-
-// Decoupled look-back for one running total, done by one whole warp. Publishes `aggregate` for
-// `chunk`, waits (bounded) for the predecessors, publishes the inclusive total and returns the
-// exclusive prefix to every lane.
-__device__ __forceinline__ unsigned lookback_warp(unsigned long long* status, unsigned chunk, unsigned aggregate,
-                                                  unsigned epoch, unsigned* flags) {
-    const int lane = threadIdx.x & 31;
-    if (lane == 0) st_store(status + chunk, st_make(epoch, chunk == 0 ? kStInc : kStAgg, aggregate));
-    unsigned exclusive = 0;
-    if (chunk > 0) {
-        long long pos = static_cast<long long>(chunk) - 1;
-        unsigned spins = 0;
-        while (true) {
-            const long long idx = pos - lane;
-            unsigned flag, value;
-            if (idx >= 0) {
-                const unsigned long long s = st_load(status + idx);
-                flag = st_flag(s, epoch);
-                value = static_cast<unsigned>(s);
-            } else {
-                flag = kStInc;
-                value = 0;
-            }
-            const unsigned inc = __ballot_sync(0xFFFFFFFFu, flag == kStInc);
-            const unsigned ready = __ballot_sync(0xFFFFFFFFu, flag != 0);
-            if (inc) {
-                const int k = __ffs(inc) - 1;
-                const unsigned need = k == 31 ? 0xFFFFFFFFu : ((2u << k) - 1u);
-                if ((ready & need) == need) {
-                    unsigned v = lane <= k ? value : 0u;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-                    exclusive += v;
-                    break;
-                }
-            } else if (ready == 0xFFFFFFFFu) {
-                unsigned v = value;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-                exclusive += v;
-                pos -= 32;
-                continue;
-            }
-            if (++spins > kSpinLimit) {
-                if (lane == 0) atomicOr(flags, kFlagTimeout);
-                break;
-            }
-        }
-        if (lane == 0) st_store(status + chunk, st_make(epoch, kStInc, exclusive + aggregate));
-    }
-    return exclusive;
 }
 
 __device__ __forceinline__ float ex2_approx(float x) {

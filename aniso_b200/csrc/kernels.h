@@ -20,54 +20,58 @@ struct DebugProjection {
     unsigned* tiles_touched = nullptr;
 };
 
-// Clears the frame's control block (counters, histograms, flags) and advances its epoch.
+// Clears the frame's control block (counts and flags; the flags are folded into the sticky ones).
 void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
 
 // Projection of every (view, Gaussian) entry of a batch; `blocks` = sum over scenes of
 // ceil(n / 256) (scene s starts at block scenes[s].block_base).
 void launch_preprocess(const BatchScene<SceneView>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
-                       int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec, unsigned long long* rect16,
+                       int sh_degree, int tile_w, int tile_h, SplatRecord* rec, unsigned long long* rect16,
                        unsigned* depth_key, const DebugProjection* dbg, cudaStream_t stream);
 // The same projection of the optimizer's raw tensors (activated in the kernel).
 void launch_preprocess_raw(const BatchScene<RawParams>* scenes, unsigned n_scenes, unsigned blocks,
-                           const ViewInfo* views, int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec,
+                           const ViewInfo* views, int sh_degree, int tile_w, int tile_h, SplatRecord* rec,
                            unsigned long long* rect16, unsigned* depth_key, cudaStream_t stream);
 
-// One stable onesweep LSD radix pass over (key, value) u32 pairs, 8-bit digit at `shift`; `hist` is
-// this digit's global histogram. masked_count > 0: the input is the N depth keys with culled ones
-// dropped and the index as value (the first depth pass); else the histogram total is the item
-// count. Grids are sized for `capacity` items; surplus blocks exit at once.
-int onesweep_items_per_thread();
-unsigned onesweep_chunk_items();
-void launch_onesweep(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
-                     unsigned masked_count, unsigned capacity, int shift, const unsigned* hist,
-                     unsigned long long* status, unsigned* chunk_ctr, Ctrl* ctrl, cudaStream_t stream);
+// Where a sort pass finds its item count: a host value, the visible count the first depth pass
+// publishes, or the frame's pair total.
+enum class SortCount : int { kFixed = 0, kVisible = 1, kPairs = 2 };
 
-// Expands the depth-sorted visible list into (tile, Gaussian) pairs in depth order, building the
-// tile-digit histograms; sets kFlagOverflow (and writes no pairs) if they exceed capacity.
-// Two kernels: a pair-offset scan over the V Gaussians, then an expansion with a fixed number of
-// pairs per block.
+// One stable LSD radix pass over (key, value) u32 pairs, 8-bit digit at `shift` (three launches:
+// upsweep, per-digit span scan, downsweep). masked: the input is the N depth keys in entry order,
+// culled ones dropped, the entry index as value (the first depth pass; it publishes the visible
+// count); keys_out may be NULL on the last pass. Grids are sized for `capacity` (`fixed` for
+// kFixed) items. scratch holds sort_scratch_words() words.
+size_t sort_scratch_words();
+void launch_radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
+                       bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned* scratch,
+                       Ctrl* ctrl, cudaStream_t stream);
+
+// Expands the depth-sorted visible list into (tile, entry) pairs in depth order; sets kFlagOverflow
+// (and writes no pairs) if they exceed capacity. Three kernels: per-span pair counts, pair offsets,
+// and an expansion with a fixed number of pairs per CTA.
 struct DupBuffers {
-    unsigned* offs;                   // [N] exclusive pair offset of each depth-sorted Gaussian
-    unsigned* rank;                   // [N] depth-sorted position of each visible Gaussian index
-    unsigned long long* rect_sorted;  // [N] its 16x16-tile rectangle, in sorted order
-    unsigned* chunk_start;            // [capacity / expand_chunk_pairs() + 2] first Gaussian per chunk
+    unsigned* offs;                   // [N] exclusive pair offset of each depth-sorted entry
+    unsigned* rank;                   // [N] depth-sorted position of each visible entry (or NULL)
+    unsigned long long* rect_sorted;  // [N] its tile rectangle, in sorted order
+    unsigned* chunk_start;            // [capacity / expand_chunk_pairs() + 2] first entry per chunk
+    unsigned long long* span_sum;     // [sort_span_sums()] pairs per span
 };
-unsigned pair_scan_chunk_items();
+size_t sort_span_sums();
 unsigned expand_chunk_pairs();
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
-                      unsigned max_visible, const BatchTables& tables, int tile_passes, const DupBuffers& buf,
-                      unsigned* pair_key, unsigned* pair_val, unsigned long long* status, cudaStream_t stream);
+                      unsigned max_visible, const BatchTables& tables, const DupBuffers& buf, unsigned* pair_key,
+                      unsigned* pair_val, cudaStream_t stream);
 
 // ranges[tile] = [start, end) over the sorted tile keys (gpu_render.cu:164-177); ranges must be
 // zeroed before.
 void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capacity, uint2* ranges,
                    cudaStream_t stream);
 
-// Depth keys, rectangles and depth histograms of a projection computed elsewhere (tiles_touched,
-// rect, depth in the reference kernel's layout), as the preprocess kernel writes them.
+// Depth keys and rectangles of a projection computed elsewhere (tiles_touched, rect, depth in the
+// reference kernel's layout), as the preprocess kernel writes them.
 void launch_projection_keys(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
-                            Ctrl* ctrl, unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream);
+                            unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream);
 
 // Blends every tile of a batch (blockIdx = global tile); outputs go to each view's ViewInfo.
 // train: also the float colour, final transmittance and last contributor per pixel.

@@ -4,10 +4,9 @@
 // Projects each Gaussian the way gpu_render.cu:86-145 does (the same fp32 expressions in the same
 // order, compiled without fast-math, so depth, rectangle and conic come out bit-identical to the
 // reference kernel built without --use_fast_math), then, fused into the same kernel:
-//   * writes the blend record (SplatRecord) and the 16x16-tile rectangle of visible Gaussians;
-//   * writes every Gaussian's depth key (the float bits of its depth; a sentinel if culled) -- the
-//     first onesweep pass of the depth sort compacts the visible ones as it ranks them;
-//   * builds the four 8-bit digit histograms of the depth bits for the onesweep passes.
+//   * writes the blend record (SplatRecord) and the tile rectangle of visible Gaussians;
+//   * writes every entry's depth key (the float bits of its depth; a sentinel if culled) -- the
+//     first LSD pass of the depth sort compacts the visible ones as it ranks them.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -154,15 +153,12 @@ constexpr int kMaxStagedViews = 64;  // cameras of a scene's views kept in share
 template <int D, bool kDebug, class Src>
 __global__ void __launch_bounds__(256, 3) preprocess_kernel(const BatchScene<Src>* __restrict__ scenes,
                                                             unsigned n_scenes, const ViewInfo* __restrict__ views,
-                                                            int tile_w, int tile_h, Ctrl* __restrict__ ctrl,
-                                                            SplatRecord* __restrict__ rec,
+                                                            int tile_w, int tile_h, SplatRecord* __restrict__ rec,
                                                             unsigned long long* __restrict__ rect16,
                                                             unsigned* __restrict__ depth_key, DebugProjection dbg) {
-    __shared__ unsigned s_hist[kMaxPasses * kRadix];
     __shared__ CamParams s_cam[kMaxStagedViews];
     __shared__ unsigned s_scene;
     const int tid = threadIdx.x;
-    for (int k = tid; k < kMaxPasses * kRadix; k += 256) s_hist[k] = 0;
     if (tid == 0) {
         unsigned sidx = 0;
         for (unsigned k = 1; k < n_scenes; ++k)
@@ -241,47 +237,41 @@ __global__ void __launch_bounds__(256, 3) preprocess_kernel(const BatchScene<Src
                 dbg.rect[e] = make_uint4(p.x0, p.y0, p.x1, p.y1);
                 dbg.tiles_touched[e] = static_cast<unsigned>((p.x1 - p.x0 + 1) * (p.y1 - p.y0 + 1));
             }
-#pragma unroll
-            for (int pass = 0; pass < kMaxPasses; ++pass)
-                atomicAdd(&s_hist[pass * kRadix + ((depth_bits >> (pass * kRadixBits)) & (kRadix - 1))], 1u);
         }
     }
-    __syncthreads();
-    for (int k = tid; k < kMaxPasses * kRadix; k += 256)
-        if (s_hist[k]) atomicAdd(&ctrl->depth_hist[k], s_hist[k]);
 }
 
 template <bool kDebug, class Src>
 void launch_preprocess_t(const BatchScene<Src>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
-                         int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec,
+                         int sh_degree, int tile_w, int tile_h, SplatRecord* rec,
                          unsigned long long* rect16, unsigned* depth_key, const DebugProjection& dbg,
                          cudaStream_t stream) {
     if (blocks == 0) return;
     switch (sh_degree) {
-        case 0: preprocess_kernel<0, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, ctrl, rec, rect16, depth_key, dbg); break;
-        case 1: preprocess_kernel<1, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, ctrl, rec, rect16, depth_key, dbg); break;
-        case 2: preprocess_kernel<2, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, ctrl, rec, rect16, depth_key, dbg); break;
-        default: preprocess_kernel<3, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, ctrl, rec, rect16, depth_key, dbg); break;
+        case 0: preprocess_kernel<0, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, rec, rect16, depth_key, dbg); break;
+        case 1: preprocess_kernel<1, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, rec, rect16, depth_key, dbg); break;
+        case 2: preprocess_kernel<2, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, rec, rect16, depth_key, dbg); break;
+        default: preprocess_kernel<3, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, rec, rect16, depth_key, dbg); break;
     }
 }
 
 }  // namespace
 
 void launch_preprocess(const BatchScene<SceneView>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
-                       int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec, unsigned long long* rect16,
+                       int sh_degree, int tile_w, int tile_h, SplatRecord* rec, unsigned long long* rect16,
                        unsigned* depth_key, const DebugProjection* dbg, cudaStream_t stream) {
     if (dbg)
-        launch_preprocess_t<true>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, ctrl, rec, rect16,
+        launch_preprocess_t<true>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, rec, rect16,
                                   depth_key, *dbg, stream);
     else
-        launch_preprocess_t<false>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, ctrl, rec, rect16,
+        launch_preprocess_t<false>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, rec, rect16,
                                    depth_key, DebugProjection{}, stream);
 }
 
 void launch_preprocess_raw(const BatchScene<RawParams>* scenes, unsigned n_scenes, unsigned blocks,
-                           const ViewInfo* views, int sh_degree, int tile_w, int tile_h, Ctrl* ctrl, SplatRecord* rec,
+                           const ViewInfo* views, int sh_degree, int tile_w, int tile_h, SplatRecord* rec,
                            unsigned long long* rect16, unsigned* depth_key, cudaStream_t stream) {
-    launch_preprocess_t<false>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, ctrl, rec, rect16,
+    launch_preprocess_t<false>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, rec, rect16,
                                depth_key, DebugProjection{}, stream);
 }
 

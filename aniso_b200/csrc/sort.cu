@@ -5,424 +5,547 @@
 // A stable LSD sort handles the low (depth) digits first, and duplication commutes with a stable
 // sort on a key every copy of a Gaussian shares, so the same order is produced here with less
 // traffic:
-//   1. the preprocess kernel writes every Gaussian's depth key (a sentinel when culled);
-//   2. four 8-bit onesweep passes sort the V visible (depth bits, index) pairs -- V, not P, items;
-//      the first pass reads all N keys in index order and drops the culled ones as it ranks;
-//   3. a pair-offset scan over those V, then an expansion, in depth order, into P (tile, index)
+//   1. the preprocess kernel writes every entry's depth key (a sentinel when culled);
+//   2. four 8-bit LSD passes sort the V visible (depth bits, entry) pairs -- V, not P, items;
+//      the first pass reads all N keys in entry order and drops the culled ones as it ranks;
+//   3. a pair-offset scan over those V, then an expansion, in depth order, into P (tile, entry)
 //      pairs with the same number of pairs per block (the nearest splats own thousands of tiles);
-//   4. ceil(bits(tiles) / 8) onesweep passes stably sort the pairs by tile;
+//   4. ceil(bits(tiles) / 8) LSD passes stably sort the pairs by tile;
 //   5. tile ranges as gpu_render.cu:164-177.
-// Each tile's run ends up ordered by (depth bits, Gaussian index), exactly the reference's order,
-// so keys, values and ranges are bit-identical to the reference's for the same projection.
+// Each tile's run ends up ordered by (depth bits, entry index), exactly the reference's order, so
+// keys, values and ranges are bit-identical to the reference's for the same projection.
 //
-// The onesweep pass follows the single-pass LSD scheme of Adinets & Merrill (2022): a block ranks
-// a chunk of keys with warp-level match_any, publishes its per-digit counts, looks back over the
-// preceding chunks (decoupled look-back, bounded waits) for each digit's running offset, and
-// scatters through shared memory so global writes are contiguous per digit.
+// Every LSD pass is reduce-then-scan over a fixed number of spans (contiguous runs of 2048-item
+// blocks, one span per CTA, four CTAs per SM): an upsweep counts each span's digits, one CTA per
+// digit scans that digit's counts over the spans, and a downsweep re-reads each block, ranks it
+// with warp match_any, and scatters it through shared memory so global writes are contiguous per
+// digit.
+// No CTA ever waits on another, so there is no spin loop anywhere in the sort; item counts that
+// are known only on the device (visible entries, pairs) are read from the control block, and the
+// grids are sized for the capacity.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
 namespace ab2 {
 namespace {
 
-constexpr int kOsThreads = 256;
-constexpr int kOsItems = 8;
-constexpr int kOsChunk = kOsThreads * kOsItems;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = 8;
+constexpr int kBlockItems = kThreads * kItems;  // items one CTA ranks at a time
+constexpr int kMaxSpans = 4 * 148;
 constexpr int kScanItems = 4;
-constexpr int kScanChunk = 256 * kScanItems;
-constexpr int kExpandChunk = 1024;
+constexpr int kScanBlock = kThreads * kScanItems;
+constexpr int kExpandItems = 8;
+constexpr int kExpandChunk = kThreads * kExpandItems;  // pairs per expansion CTA
 
 __global__ void frame_begin_kernel(Ctrl* ctrl) {
-    const int tid = threadIdx.x;
-    if (tid == 0) {
-        ctrl->sticky_flags |= ctrl->flags;
-        if (ctrl->pair_total > ctrl->max_pair_total) ctrl->max_pair_total = ctrl->pair_total;
-        ctrl->pair_total = 0;
-        ctrl->vis_count = 0;
-        ctrl->flags = 0;
-        unsigned e = (ctrl->epoch + 1u) & 0x3FFFFFFFu;
-        ctrl->epoch = e == 0 ? 1u : e;
-    }
-    if (tid < 16) ctrl->chunk_ctr[tid] = 0;
-    for (int k = tid; k < kMaxPasses * kRadix; k += blockDim.x) {
-        ctrl->depth_hist[k] = 0;
-        ctrl->tile_hist[k] = 0;
-    }
+    ctrl->sticky_flags |= ctrl->flags;
+    if (ctrl->pair_total > ctrl->max_pair_total) ctrl->max_pair_total = ctrl->pair_total;
+    ctrl->pair_total = 0;
+    ctrl->vis_count = 0;
+    ctrl->flags = 0;
 }
 
-// One stable LSD pass over a chunk of kOsThreads * ITEMS (key, value) pairs.
-//   masked_count > 0: the input is every Gaussian's depth key (kCulledKey = culled), values are the
-//                     indices themselves (vals_in unused); culled keys are dropped, so this pass
-//                     also compacts the visible list. The pass publishes the visible count.
-//   masked_count = 0: the input holds exactly as many items as this digit's histogram counts.
-template <int ITEMS>
-__global__ void __launch_bounds__(kOsThreads) onesweep_kernel(const unsigned* __restrict__ keys_in,
-                                                               const unsigned* __restrict__ vals_in,
-                                                               unsigned* __restrict__ keys_out,
-                                                               unsigned* __restrict__ vals_out, unsigned masked_count,
-                                                               int shift, const unsigned* __restrict__ hist,
-                                                               unsigned long long* status, unsigned* chunk_ctr,
-                                                               Ctrl* ctrl) {
-    constexpr int CH = kOsThreads * ITEMS;
-    constexpr int NW = kOsThreads / 32;
-    __shared__ unsigned s_keys[CH];
-    __shared__ unsigned s_vals[CH];
-    __shared__ unsigned s_wh[NW][kRadix];
-    __shared__ unsigned s_dstart[kRadix];
-    __shared__ unsigned s_gbase[kRadix];
-    __shared__ unsigned s_tmp[NW];
-    __shared__ unsigned s_chunk;
+// Items of this frame's pass; false when the frame overflowed (nothing after duplication runs).
+__device__ __forceinline__ bool pass_items(const Ctrl* ctrl, SortCount src, unsigned fixed, unsigned capacity,
+                                           unsigned& n) {
+    if (ctrl->flags & kFlagOverflow) return false;
+    if (src == SortCount::kFixed) {
+        n = fixed;
+    } else if (src == SortCount::kVisible) {
+        n = ctrl->vis_count;
+    } else {
+        const unsigned long long p = ctrl->pair_total;
+        if (p > capacity) return false;
+        n = static_cast<unsigned>(p);
+    }
+    return true;
+}
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (ctrl->flags & kFlagOverflow) return;
-    if (tid == 0) s_chunk = atomicAdd(chunk_ctr, 1u);
-    for (int k = tid; k < NW * kRadix; k += kOsThreads) (&s_wh[0][0])[k] = 0;
-    const unsigned d = tid;  // this thread's digit in the per-digit phases
-    unsigned hist_total;
-    const unsigned gstart = block_excl_scan<kOsThreads>(hist[d], s_tmp, hist_total);
-    const unsigned chunk = s_chunk;
-    const bool masked = masked_count > 0;
-    const unsigned count = masked ? masked_count : hist_total;
-    if (masked && chunk == 0 && tid == 0) ctrl->vis_count = hist_total;
-    const unsigned base = chunk * CH;
-    if (base >= count) return;
+// Blocks [t0, t1) of the n items that span b of `spans` covers.
+__device__ __forceinline__ void span_blocks(unsigned n, unsigned spans, unsigned b, unsigned& t0, unsigned& t1) {
+    const unsigned long long T = (static_cast<unsigned long long>(n) + kBlockItems - 1) / kBlockItems;
+    t0 = static_cast<unsigned>(T * b / spans);
+    t1 = static_cast<unsigned>(T * (b + 1) / spans);
+}
 
-    unsigned key[ITEMS], val[ITEMS], rank[ITEMS];
-    const unsigned wbase = base + warp * (ITEMS * 32) + lane;
+// Loads block t: lane `lane` of warp `warp` holds items base + warp*kItems*32 + k*32 + lane, so
+// (k, lane) order within a warp is ascending position. dg = the digit, or kRadix for no item.
+template <bool kMasked, bool kVals>
+__device__ __forceinline__ void load_block(const unsigned* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
+                                           unsigned t, unsigned n, int shift, int warp, int lane, unsigned (&key)[kItems],
+                                           unsigned (&val)[kItems], unsigned (&dg)[kItems]) {
+    const unsigned long long wbase = static_cast<unsigned long long>(t) * kBlockItems + warp * (kItems * 32) + lane;
 #pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-        const unsigned idx = wbase + k * 32;
-        bool valid = idx < count;
+    for (int k = 0; k < kItems; ++k) {
+        const unsigned long long idx = wbase + k * 32;
+        bool valid = idx < n;
         key[k] = valid ? keys_in[idx] : 0u;
-        if (masked) {
+        if (kMasked) {
             valid = valid && key[k] != kCulledKey;
-            val[k] = idx;
-        } else {
+            val[k] = static_cast<unsigned>(idx);
+        } else if (kVals) {
             val[k] = valid ? vals_in[idx] : 0u;
         }
-        rank[k] = valid ? ((key[k] >> shift) & (kRadix - 1)) : kRadix;  // digit; kRadix = not an item
+        dg[k] = valid ? ((key[k] >> shift) & (kRadix - 1)) : kRadix;
     }
-    // Warp-level stable ranking: items in (k, lane) order, i.e. ascending position.
+}
+
+// Digit counts of each span: counts[d * spans + b]. Counting needs no ranks, so each warp adds
+// into its own shared histogram with plain atomics (lanes of one warp that share a digit are
+// serialised by the hardware, which costs less than resolving peers first).
+template <bool kMasked>
+__global__ void __launch_bounds__(kThreads) upsweep_kernel(const unsigned* __restrict__ keys_in, SortCount src,
+                                                           unsigned fixed, unsigned capacity, int shift,
+                                                           unsigned spans, unsigned* __restrict__ counts,
+                                                           const Ctrl* __restrict__ ctrl) {
+    __shared__ unsigned s_h[kWarps][kRadix];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned n;
+    if (!pass_items(ctrl, src, fixed, capacity, n)) return;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) s_h[w][tid] = 0;
+    __syncthreads();
+    unsigned t0, t1;
+    span_blocks(n, spans, blockIdx.x, t0, t1);
+    for (unsigned t = t0; t < t1; ++t) {
+        unsigned key[kItems], val[kItems], dg[kItems];
+        load_block<kMasked, false>(keys_in, nullptr, t, n, shift, warp, lane, key, val, dg);
+#pragma unroll
+        for (int k = 0; k < kItems; ++k)
+            if (dg[k] < kRadix) atomicAdd(&s_h[warp][dg[k]], 1u);
+    }
+    __syncthreads();
+    unsigned c = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) c += s_h[w][tid];
+    counts[static_cast<size_t>(tid) * spans + blockIdx.x] = c;
+}
+
+// One CTA per digit: exclusive scan of the digit's counts over the spans, in place, and its total.
+__global__ void __launch_bounds__(kThreads) span_scan_kernel(unsigned* __restrict__ counts, unsigned* __restrict__ totals,
+                                                             unsigned spans, SortCount src, unsigned fixed,
+                                                             unsigned capacity, const Ctrl* __restrict__ ctrl) {
+    __shared__ unsigned s_tmp[kWarps];
+    unsigned n;
+    if (!pass_items(ctrl, src, fixed, capacity, n)) return;
+    unsigned* row = counts + static_cast<size_t>(blockIdx.x) * spans;
+    unsigned carry = 0;
+    for (unsigned b0 = 0; b0 < spans; b0 += kThreads) {  // spans <= kMaxSpans: at most 3 rounds
+        const unsigned b = b0 + threadIdx.x;
+        const unsigned c = b < spans ? row[b] : 0u;
+        unsigned tot;
+        const unsigned ex = block_excl_scan<kThreads>(c, s_tmp, tot);
+        if (b < spans) row[b] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
+// Ranks, scatters and writes each block of the span. The masked pass publishes the visible count.
+template <bool kMasked, bool kKeysOut>
+__global__ void __launch_bounds__(kThreads) downsweep_kernel(const unsigned* __restrict__ keys_in,
+                                                             const unsigned* __restrict__ vals_in,
+                                                             unsigned* __restrict__ keys_out,
+                                                             unsigned* __restrict__ vals_out, SortCount src,
+                                                             unsigned fixed, unsigned capacity, int shift,
+                                                             unsigned spans, const unsigned* __restrict__ counts,
+                                                             const unsigned* __restrict__ totals, Ctrl* ctrl) {
+    __shared__ unsigned s_keys[kBlockItems];
+    __shared__ unsigned s_vals[kBlockItems];
+    __shared__ unsigned s_wh[kWarps][kRadix];
+    __shared__ unsigned s_dstart[kRadix];
+    __shared__ unsigned s_gbase[kRadix];
+    __shared__ unsigned s_tmp[kWarps];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned n;
+    if (!pass_items(ctrl, src, fixed, capacity, n)) return;
+    const unsigned d = tid;  // this thread's digit in the per-digit phases
+    unsigned all;
+    const unsigned gstart = block_excl_scan<kThreads>(totals[d], s_tmp, all);
+    if (kMasked && blockIdx.x == 0 && tid == 0) ctrl->vis_count = all;
+    unsigned run = gstart + counts[static_cast<size_t>(d) * spans + blockIdx.x];  // next output of digit d
+    unsigned t0, t1;
+    span_blocks(n, spans, blockIdx.x, t0, t1);
     const unsigned lt = lanemask_lt();
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-        const unsigned dg = rank[k];
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg);
-        const unsigned cnt = dg < kRadix ? s_wh[warp][dg] : 0u;
-        const unsigned r = cnt + __popc(peers & lt);
-        __syncwarp();
-        if (dg < kRadix && lane == 31 - __clz(peers)) s_wh[warp][dg] = cnt + __popc(peers);
-        __syncwarp();
-        rank[k] = dg < kRadix ? r : 0xFFFFFFFFu;
-    }
-    __syncthreads();
 
-    // Per digit: offsets of each warp's run, the block's digit total and the block-local start.
-    unsigned run = 0;
+    for (unsigned t = t0; t < t1; ++t) {
 #pragma unroll
-    for (int w = 0; w < NW; ++w) {
-        const unsigned c = s_wh[w][d];
-        s_wh[w][d] = run;
-        run += c;
-    }
-    unsigned block_total;
-    const unsigned dstart = block_excl_scan<kOsThreads>(run, s_tmp, block_total);
-    s_dstart[d] = dstart;
-
-    // Decoupled look-back for digit d over the preceding chunks. Each round trip loads the status
-    // of kLookback predecessors at once, so a block whose predecessors have only published their
-    // own counts (all blocks finish ranking together when the chunks fit on the GPU at once) sums
-    // kLookback of them per L2 latency instead of one.
-    const unsigned epoch = ctrl->epoch;
-    unsigned long long* my = status + static_cast<size_t>(chunk) * kRadix + d;
-    st_store(my, st_make(epoch, chunk == 0 ? kStInc : kStAgg, run));
-    unsigned excl = 0;
-    if (chunk > 0) {
-        constexpr unsigned kLookback = 8;
-        unsigned c = chunk, spins = 0;  // predecessors still to add: c-1, c-2, ...
-        bool found = false;
-        while (!found && c > 0) {
-            const unsigned k_count = min(kLookback, c);
-            unsigned long long sv[kLookback];
+        for (int w = 0; w < kWarps; ++w) s_wh[w][d] = 0;
+        unsigned key[kItems], val[kItems], dg[kItems];
+        load_block<kMasked, true>(keys_in, vals_in, t, n, shift, warp, lane, key, val, dg);
+        __syncthreads();
+        // Warp-level stable ranking: items in (k, lane) order, i.e. ascending position.
+        unsigned rank[kItems];
 #pragma unroll
-            for (unsigned k = 0; k < kLookback; ++k)
-                sv[k] = k < k_count ? st_load(status + static_cast<size_t>(c - 1 - k) * kRadix + d) : 0ull;
-            unsigned used = 0;
+        for (int k = 0; k < kItems; ++k) {
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg[k]);
+            const unsigned cnt = dg[k] < kRadix ? s_wh[warp][dg[k]] : 0u;
+            rank[k] = cnt + __popc(peers & lt);
+            __syncwarp();
+            if (dg[k] < kRadix && lane == 31 - __clz(peers)) s_wh[warp][dg[k]] = cnt + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        // Per digit: the offset of each warp's run, the block's digit count and the block-local start.
+        unsigned cnt = 0;
 #pragma unroll
-            for (unsigned k = 0; k < kLookback; ++k) {
-                if (k >= k_count || found) break;
-                const unsigned f = st_flag(sv[k], epoch);
-                if (f == 0) break;  // not published yet: reload from here
-                excl += static_cast<unsigned>(sv[k]);
-                used = k + 1;
-                if (f == kStInc) found = true;
-            }
-            c -= used;
-            if (!found && used < k_count && ++spins > kSpinLimit) {
-                atomicOr(&ctrl->flags, kFlagTimeout);
-                break;
+        for (int w = 0; w < kWarps; ++w) {
+            const unsigned c = s_wh[w][d];
+            s_wh[w][d] = cnt;
+            cnt += c;
+        }
+        unsigned block_total;
+        const unsigned dstart = block_excl_scan<kThreads>(cnt, s_tmp, block_total);
+        s_dstart[d] = dstart;
+        s_gbase[d] = run - dstart;
+        run += cnt;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            if (dg[k] < kRadix) {
+                const unsigned pos = s_dstart[dg[k]] + s_wh[warp][dg[k]] + rank[k];
+                s_keys[pos] = key[k];
+                s_vals[pos] = val[k];
             }
         }
-        st_store(my, st_make(epoch, kStInc, excl + run));
-    }
-    s_gbase[d] = gstart + excl - dstart;
-    __syncthreads();
-
-    // Scatter into shared memory in block-sorted order, then write out contiguously per digit.
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-        if (rank[k] != 0xFFFFFFFFu) {
-            const unsigned dd = (key[k] >> shift) & (kRadix - 1);
-            const unsigned pos = s_dstart[dd] + s_wh[warp][dd] + rank[k];
-            s_keys[pos] = key[k];
-            s_vals[pos] = val[k];
+        __syncthreads();
+        for (unsigned p = tid; p < block_total; p += kThreads) {
+            const unsigned k = s_keys[p];
+            const unsigned g = s_gbase[(k >> shift) & (kRadix - 1)] + p;
+            if (kKeysOut) keys_out[g] = k;
+            vals_out[g] = s_vals[p];
         }
-    }
-    __syncthreads();
-    for (unsigned p = tid; p < block_total; p += kOsThreads) {
-        const unsigned k = s_keys[p];
-        const unsigned g = s_gbase[(k >> shift) & (kRadix - 1)] + p;
-        if (keys_out) keys_out[g] = k;
-        vals_out[g] = s_vals[p];
+        __syncthreads();
     }
 }
 
-// Pair offsets of the depth-sorted visible list: an exclusive scan of each Gaussian's tile count
-// (single pass, decoupled look-back), written with its rectangle in sorted order. For every chunk
-// of kExpandChunk pairs it also records the Gaussian that holds the chunk's first pair, so the
-// expansion can give every block the same number of pairs. The last block stores the frame's
-// pair total and flags an overflow of the pair capacity.
-__global__ void __launch_bounds__(256) pair_scan_kernel(const unsigned* __restrict__ sorted_idx,
-                                                        const unsigned long long* __restrict__ rect16, Ctrl* ctrl,
-                                                        unsigned capacity, unsigned* __restrict__ offs,
-                                                        unsigned* __restrict__ rank,
-                                                        unsigned long long* __restrict__ rect_sorted,
-                                                        unsigned* __restrict__ chunk_start,
-                                                        unsigned long long* status) {
-    __shared__ unsigned s_tmp[8];
-    __shared__ unsigned s_chunk, s_base;
-    const int tid = threadIdx.x;
-    if (tid == 0) s_chunk = atomicAdd(&ctrl->chunk_ctr[kCtrDup], 1u);
-    __syncthreads();
-    const unsigned chunk = s_chunk;
-    const unsigned V = ctrl->vis_count;
-    const unsigned first = chunk * kScanChunk;
-    if (first >= V) return;
+__device__ __forceinline__ unsigned rect_area(unsigned long long r) {
+    const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu, y1 = r >> 48;
+    return (x1 - x0 + 1) * (y1 - y0 + 1);
+}
 
-    unsigned cnt[kScanItems];
-    unsigned long long rect[kScanItems];
-    unsigned thread_total = 0;
+__device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v, unsigned long long* s_tmp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const unsigned j = first + tid * kScanItems + k;
-        unsigned c = 0;
-        unsigned long long r = 0;
-        if (j < V) {
-            const unsigned g = sorted_idx[j];
-            rank[g] = j;
-            r = rect16[g];
-            const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu, y1 = r >> 48;
-            c = (x1 - x0 + 1) * (y1 - y0 + 1);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if (lane == 0) s_tmp[warp] = v;
+    __syncthreads();
+    unsigned long long s = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) s += s_tmp[w];
+    __syncthreads();
+    return s;
+}
+
+// Entries [V b / spans, V (b+1) / spans) of the depth-sorted list: gathers each one's rectangle
+// into sorted order, records its sorted position (for the adjoint; rank may be NULL), and sums
+// its tile counts. The gathers are random, so each thread keeps kGather of them in flight.
+constexpr int kGather = 8;
+__global__ void __launch_bounds__(kThreads) pair_count_kernel(const unsigned* __restrict__ sorted_idx,
+                                                              const unsigned long long* __restrict__ rect16,
+                                                              const Ctrl* __restrict__ ctrl, unsigned spans,
+                                                              unsigned* __restrict__ rank,
+                                                              unsigned long long* __restrict__ rect_sorted,
+                                                              unsigned long long* __restrict__ span_sum) {
+    __shared__ unsigned long long s_tmp[kWarps];
+    const unsigned long long V = ctrl->vis_count;
+    const unsigned lo = static_cast<unsigned>(V * blockIdx.x / spans);
+    const unsigned hi = static_cast<unsigned>(V * (blockIdx.x + 1) / spans);
+    unsigned long long sum = 0;
+    for (unsigned j0 = lo + threadIdx.x; j0 < hi; j0 += kThreads * kGather) {
+        unsigned g[kGather];
+        unsigned long long r[kGather];
+#pragma unroll
+        for (int k = 0; k < kGather; ++k) {
+            const unsigned j = j0 + k * kThreads;
+            g[k] = j < hi ? sorted_idx[j] : 0u;
         }
-        cnt[k] = c;
-        rect[k] = r;
-        thread_total += c;
-    }
-    unsigned block_total;
-    const unsigned thread_base = block_excl_scan<256>(thread_total, s_tmp, block_total);
-    if (tid < 32) {
-        const unsigned b = lookback_warp(status, chunk, block_total, ctrl->epoch, &ctrl->flags);
-        if (tid == 0) {
-            s_base = b;
-            if (first + kScanChunk >= V) {  // the last chunk: the frame's pair total
-                const unsigned long long P = static_cast<unsigned long long>(b) + block_total;
-                ctrl->pair_total = P;
-                if (P > capacity) atomicOr(&ctrl->flags, kFlagOverflow);
+#pragma unroll
+        for (int k = 0; k < kGather; ++k) {
+            const unsigned j = j0 + k * kThreads;
+            r[k] = j < hi ? rect16[g[k]] : 0ull;
+        }
+#pragma unroll
+        for (int k = 0; k < kGather; ++k) {
+            const unsigned j = j0 + k * kThreads;
+            if (j < hi) {
+                if (rank) rank[g[k]] = j;
+                rect_sorted[j] = r[k];
+                sum += rect_area(r[k]);
             }
         }
     }
-    __syncthreads();
-    const unsigned last_chunk = (capacity + kExpandChunk - 1) / kExpandChunk;
-    unsigned long long o = static_cast<unsigned long long>(s_base) + thread_base;
+    sum = block_sum_u64(sum, s_tmp);
+    if (threadIdx.x == 0) span_sum[blockIdx.x] = sum;
+}
+
+// Exclusive pair offset of every depth-sorted entry, and, for every chunk of kExpandChunk pairs,
+// the entry that holds the chunk's first pair. The last span stores the frame's pair total and
+// flags an overflow of the pair capacity.
+__global__ void __launch_bounds__(kThreads) pair_offsets_kernel(const unsigned long long* __restrict__ rect_sorted,
+                                                                Ctrl* ctrl, unsigned spans, unsigned capacity,
+                                                                const unsigned long long* __restrict__ span_sum,
+                                                                unsigned* __restrict__ offs,
+                                                                unsigned* __restrict__ chunk_start) {
+    __shared__ unsigned long long s_tmp64[kWarps];
+    __shared__ unsigned s_tmp[kWarps];
+    const unsigned b = blockIdx.x;
+    unsigned long long before = 0;
+    for (unsigned k = threadIdx.x; k < b; k += kThreads) before += span_sum[k];
+    unsigned long long base = block_sum_u64(before, s_tmp64);
+    if (b == spans - 1 && threadIdx.x == 0) {
+        const unsigned long long P = base + span_sum[b];
+        ctrl->pair_total = P;
+        if (P > capacity) atomicOr(&ctrl->flags, kFlagOverflow);
+    }
+    if (base > capacity) return;  // the frame overflows: nothing reads these offsets
+    const unsigned long long V = ctrl->vis_count;
+    const unsigned lo = static_cast<unsigned>(V * b / spans);
+    const unsigned hi = static_cast<unsigned>(V * (b + 1) / spans);
+    const unsigned long long last_chunk = (static_cast<unsigned long long>(capacity) + kExpandChunk - 1) / kExpandChunk;
+    for (unsigned j0 = lo; j0 < hi; j0 += kScanBlock) {
+        unsigned cnt[kScanItems];
+        unsigned thread_total = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const unsigned j = first + tid * kScanItems + k;
-        if (j < V) {
-            offs[j] = static_cast<unsigned>(o);
-            rect_sorted[j] = rect[k];
-            for (unsigned long long c = (o + kExpandChunk - 1) / kExpandChunk;
-                 c * kExpandChunk < o + cnt[k] && c <= last_chunk; ++c)
-                chunk_start[c] = j;
+        for (int k = 0; k < kScanItems; ++k) {
+            const unsigned j = j0 + threadIdx.x * kScanItems + k;
+            cnt[k] = j < hi ? rect_area(rect_sorted[j]) : 0u;
+            thread_total += cnt[k];
         }
-        o += cnt[k];
+        unsigned tile_total;
+        const unsigned ex = block_excl_scan<kThreads>(thread_total, s_tmp, tile_total);
+        unsigned long long o = base + ex;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            const unsigned j = j0 + threadIdx.x * kScanItems + k;
+            if (j < hi && o <= capacity) {
+                offs[j] = static_cast<unsigned>(o);
+                for (unsigned long long c = (o + kExpandChunk - 1) / kExpandChunk;
+                     c * kExpandChunk < o + cnt[k] && c <= last_chunk; ++c)
+                    chunk_start[c] = j;
+            }
+            o += cnt[k];
+        }
+        base += tile_total;
     }
 }
 
-// Expands the depth-sorted list into (tile, Gaussian) pairs: block b writes pairs
-// [b * kExpandChunk, (b + 1) * kExpandChunk), row-major over each rectangle as
-// gpu_render.cu:155-160 does, and builds the tile-digit histograms of the onesweep passes.
-__global__ void __launch_bounds__(256) expand_kernel(const unsigned* __restrict__ sorted_idx,
-                                                     const unsigned long long* __restrict__ rect_sorted,
-                                                     const unsigned* __restrict__ offs,
-                                                     const unsigned* __restrict__ chunk_start, Ctrl* ctrl,
-                                                     unsigned capacity, BatchTables tables, int tile_passes,
-                                                     unsigned* __restrict__ pair_key,
-                                                     unsigned* __restrict__ pair_val) {
-    __shared__ unsigned s_off[kExpandChunk + 1];
+// Expands the depth-sorted list into (tile, entry) pairs: CTA b writes pairs
+// [b * kExpandChunk, (b + 1) * kExpandChunk), each thread kExpandItems consecutive ones (one
+// search for its first pair, then a walk), row-major over each rectangle as gpu_render.cu:155-160
+// does. Tile ids are global over the batch.
+__global__ void __launch_bounds__(kThreads) expand_kernel(const unsigned* __restrict__ sorted_idx,
+                                                          const unsigned long long* __restrict__ rect_sorted,
+                                                          const unsigned* __restrict__ offs,
+                                                          const unsigned* __restrict__ chunk_start,
+                                                          const Ctrl* __restrict__ ctrl, unsigned capacity,
+                                                          BatchTables tables, unsigned* __restrict__ pair_key,
+                                                          unsigned* __restrict__ pair_val) {
+    __shared__ unsigned s_off[kExpandChunk + 2];
     __shared__ unsigned s_idx[kExpandChunk + 1];
-    __shared__ unsigned long long s_rect[kExpandChunk + 1];
-    __shared__ unsigned s_tbase[kExpandChunk + 1];  // global tile of (0, 0) of the entry's view
+    __shared__ unsigned s_org[kExpandChunk + 1];       // global tile of the rectangle's corner
+    __shared__ unsigned short s_w[kExpandChunk + 1];   // rectangle width in tiles
     __shared__ unsigned short s_tx[kExpandChunk + 1];  // tiles per row of the entry's view
-    __shared__ unsigned s_hist[kMaxPasses * kRadix];
     const int tid = threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
-    const unsigned long long P = ctrl->pair_total;
-    if (P > capacity) return;
+    const unsigned long long P64 = ctrl->pair_total;
+    if (P64 > capacity) return;
+    const unsigned P = static_cast<unsigned>(P64);
     const unsigned base = blockIdx.x * kExpandChunk;
     if (base >= P) return;
-    for (int k = tid; k < kMaxPasses * kRadix; k += 256) s_hist[k] = 0;
     const unsigned V = ctrl->vis_count;
     const unsigned j0 = chunk_start[blockIdx.x];
     const unsigned j1 = base + kExpandChunk < P ? chunk_start[blockIdx.x + 1] : V - 1;
-    const unsigned G = j1 - j0 + 1;  // <= kExpandChunk + 1: every Gaussian owns at least one pair
-    for (unsigned k = tid; k < G; k += 256) {
-        s_off[k] = offs[j0 + k];
+    const unsigned G = j1 - j0 + 1;  // <= kExpandChunk + 1: every entry owns at least one pair
+    for (unsigned k = tid; k < G; k += kThreads) {
+        const unsigned long long r = rect_sorted[j0 + k];
         const unsigned e = sorted_idx[j0 + k];
-        s_idx[k] = e;
-        s_rect[k] = rect_sorted[j0 + k];
         const unsigned v = find_segment(tables.entry_base, tables.n_views, e);
-        s_tbase[k] = tables.tile_base[v];
-        s_tx[k] = static_cast<unsigned short>(tables.tiles_x[v]);
+        const unsigned tx = tables.tiles_x[v];
+        const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu;
+        s_off[k] = offs[j0 + k];
+        s_idx[k] = e;
+        s_org[k] = tables.tile_base[v] + y0 * tx + x0;
+        s_w[k] = static_cast<unsigned short>(x1 - x0 + 1);
+        s_tx[k] = static_cast<unsigned short>(tx);
     }
+    if (tid == 0) s_off[G] = j1 + 1 < V ? offs[j1 + 1] : P;
     __syncthreads();
-    const unsigned n_here = static_cast<unsigned>(min(static_cast<unsigned long long>(kExpandChunk), P - base));
-    const int lane = tid & 31;
-    for (unsigned q0 = 0; q0 < n_here; q0 += 256) {  // uniform trip count: whole warps vote below
-        const unsigned q = q0 + tid;
-        unsigned tile = 0;
-        const bool valid = q < n_here;
-        if (valid) {
-            const unsigned p = base + q;
-            unsigned lo = 0, hi = G - 1;  // last k with s_off[k] <= p
-            while (lo < hi) {
-                const unsigned mid = (lo + hi + 1) >> 1;
-                if (s_off[mid] <= p) lo = mid;
-                else hi = mid - 1;
+
+    const unsigned p0 = base + tid * kExpandItems;
+    if (p0 >= P) return;
+    unsigned lo = 0, hi = G - 1;  // last k with s_off[k] <= p0
+    while (lo < hi) {
+        const unsigned mid = (lo + hi + 1) >> 1;
+        if (s_off[mid] <= p0) lo = mid;
+        else hi = mid - 1;
+    }
+    unsigned w = s_w[lo], tx = s_tx[lo], org = s_org[lo], idx = s_idx[lo], next = s_off[lo + 1];
+    const unsigned kk = p0 - s_off[lo];
+    unsigned row = kk / w, col = kk - row * w;
+    unsigned key[kExpandItems], val[kExpandItems];
+#pragma unroll
+    for (int i = 0; i < kExpandItems; ++i) {
+        const unsigned p = p0 + i;
+        key[i] = org + row * tx + col;
+        val[i] = idx;
+        if (p + 1 == next && p + 1 < P) {  // the next pair starts the next entry
+            ++lo;
+            w = s_w[lo];
+            tx = s_tx[lo];
+            org = s_org[lo];
+            idx = s_idx[lo];
+            next = s_off[lo + 1];
+            row = 0;
+            col = 0;
+        } else if (++col == w) {
+            col = 0;
+            ++row;
+        }
+    }
+    if (p0 + kExpandItems <= P) {
+        uint4* k4 = reinterpret_cast<uint4*>(pair_key + p0);
+        uint4* v4 = reinterpret_cast<uint4*>(pair_val + p0);
+        k4[0] = make_uint4(key[0], key[1], key[2], key[3]);
+        k4[1] = make_uint4(key[4], key[5], key[6], key[7]);
+        v4[0] = make_uint4(val[0], val[1], val[2], val[3]);
+        v4[1] = make_uint4(val[4], val[5], val[6], val[7]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kExpandItems; ++i)
+            if (p0 + i < P) {
+                pair_key[p0 + i] = key[i];
+                pair_val[p0 + i] = val[i];
             }
-            const unsigned k = p - s_off[lo];
-            const unsigned long long r = s_rect[lo];
-            const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu;
-            const unsigned w = x1 - x0 + 1;
-            const unsigned row = k / w;
-            tile = s_tbase[lo] + (y0 + row) * static_cast<unsigned>(s_tx[lo]) + x0 + (k - row * w);
-            pair_key[p] = tile;
-            pair_val[p] = s_idx[lo];
-            atomicAdd(&s_hist[tile & (kRadix - 1)], 1u);  // low digit: neighbours differ, few conflicts
-        }
-        // Higher digits repeat along a warp (neighbouring tiles share them): one add per distinct digit.
-        for (int ps = 1; ps < tile_passes; ++ps) {
-            const unsigned dg = valid ? (tile >> (ps * kRadixBits)) & (kRadix - 1) : kRadix;
-            const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg);
-            if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_hist[ps * kRadix + dg], __popc(peers));
-        }
     }
-    __syncthreads();
-    for (int k = tid; k < tile_passes * kRadix; k += 256)
-        if (s_hist[k]) atomicAdd(&ctrl->tile_hist[k], s_hist[k]);
 }
 
-__global__ void ranges_kernel(const unsigned* __restrict__ keys, const Ctrl* ctrl, unsigned capacity,
-                              uint2* __restrict__ ranges) {
+// ranges[tile] = [first, last + 1) over the sorted tile keys; four keys per thread and step.
+__global__ void __launch_bounds__(kThreads) ranges_kernel(const unsigned* __restrict__ keys,
+                                                          const Ctrl* __restrict__ ctrl, unsigned capacity,
+                                                          uint2* __restrict__ ranges) {
     if (ctrl->flags & kFlagOverflow) return;
     const unsigned long long pt = ctrl->pair_total;
     if (pt > capacity) return;
     const unsigned P = static_cast<unsigned>(pt);
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
-        const unsigned tile = keys[i];
-        if (i == 0) ranges[tile].x = 0;
-        else {
-            const unsigned prev = keys[i - 1];
-            if (prev != tile) {
-                ranges[prev].y = i;
-                ranges[tile].x = i;
-            }
+    for (unsigned long long g = static_cast<unsigned long long>(blockIdx.x) * kThreads + threadIdx.x; g * 4 < P;
+         g += static_cast<unsigned long long>(gridDim.x) * kThreads) {
+        const unsigned i0 = static_cast<unsigned>(g * 4);
+        unsigned k[4];
+        if (i0 + 4 <= P) {
+            const uint4 q = *reinterpret_cast<const uint4*>(keys + i0);
+            k[0] = q.x;
+            k[1] = q.y;
+            k[2] = q.z;
+            k[3] = q.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) k[i] = i0 + i < P ? keys[i0 + i] : 0u;
         }
-        if (i == P - 1) ranges[tile].y = P;
+        unsigned prev = i0 > 0 ? keys[i0 - 1] : 0u;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const unsigned idx = i0 + i;
+            if (idx >= P) break;
+            const unsigned tile = k[i];
+            if (idx == 0) {
+                ranges[tile].x = 0;
+            } else if (prev != tile) {
+                ranges[prev].y = idx;
+                ranges[tile].x = idx;
+            }
+            if (idx == P - 1) ranges[tile].y = P;
+            prev = tile;
+        }
     }
 }
 
-// Depth keys (kCulledKey when tiles_touched is 0), rectangles and depth histograms of a projection
-// given in the reference kernel's layout -- what the preprocess kernel writes for its own.
-__global__ void __launch_bounds__(256) projection_keys_kernel(int64_t n, const unsigned* __restrict__ tiles_touched,
-                                                              const float* __restrict__ depth,
-                                                              const uint4* __restrict__ rect, Ctrl* ctrl,
-                                                              unsigned* __restrict__ depth_key,
-                                                              unsigned long long* __restrict__ rect16) {
-    __shared__ unsigned s_hist[kMaxPasses * kRadix];
-    const int tid = threadIdx.x;
-    for (int k = tid; k < kMaxPasses * kRadix; k += 256) s_hist[k] = 0;
-    __syncthreads();
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * 256 + tid;
-    if (i < n) {
-        unsigned key = kCulledKey;
-        if (tiles_touched[i]) {
-            key = __float_as_uint(depth[i]);
-            const uint4 r = rect[i];
-            rect16[i] = static_cast<unsigned long long>(r.x) | (static_cast<unsigned long long>(r.y) << 16) |
-                        (static_cast<unsigned long long>(r.z) << 32) | (static_cast<unsigned long long>(r.w) << 48);
-#pragma unroll
-            for (int p = 0; p < kMaxPasses; ++p)
-                atomicAdd(&s_hist[p * kRadix + ((key >> (p * kRadixBits)) & (kRadix - 1))], 1u);
-        }
-        depth_key[i] = key;
+// Depth keys (kCulledKey when tiles_touched is 0) and rectangles of a projection given in the
+// reference kernel's layout -- what the preprocess kernel writes for its own.
+__global__ void __launch_bounds__(kThreads) projection_keys_kernel(int64_t n, const unsigned* __restrict__ tiles_touched,
+                                                                   const float* __restrict__ depth,
+                                                                   const uint4* __restrict__ rect,
+                                                                   unsigned* __restrict__ depth_key,
+                                                                   unsigned long long* __restrict__ rect16) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
+    if (i >= n) return;
+    unsigned key = kCulledKey;
+    if (tiles_touched[i]) {
+        key = __float_as_uint(depth[i]);
+        const uint4 r = rect[i];
+        rect16[i] = static_cast<unsigned long long>(r.x) | (static_cast<unsigned long long>(r.y) << 16) |
+                    (static_cast<unsigned long long>(r.z) << 32) | (static_cast<unsigned long long>(r.w) << 48);
     }
-    __syncthreads();
-    for (int k = tid; k < kMaxPasses * kRadix; k += 256)
-        if (s_hist[k]) atomicAdd(&ctrl->depth_hist[k], s_hist[k]);
+    depth_key[i] = key;
+}
+
+unsigned spans_for(uint64_t max_items) {
+    const uint64_t blocks = (max_items + kBlockItems - 1) / kBlockItems;
+    return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(blocks, kMaxSpans)));
 }
 
 }  // namespace
 
-void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream) { frame_begin_kernel<<<1, 256, 0, stream>>>(ctrl); }
+void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream) { frame_begin_kernel<<<1, 1, 0, stream>>>(ctrl); }
 
-int onesweep_items_per_thread() { return kOsItems; }
-unsigned onesweep_chunk_items() { return kOsChunk; }
-
-void launch_onesweep(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
-                     unsigned masked_count, unsigned capacity, int shift, const unsigned* hist,
-                     unsigned long long* status, unsigned* chunk_ctr, Ctrl* ctrl, cudaStream_t stream) {
-    const unsigned blocks = (capacity + kOsChunk - 1) / kOsChunk;
-    if (blocks == 0) return;
-    onesweep_kernel<kOsItems><<<blocks, kOsThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, masked_count,
-                                                                 shift, hist, status, chunk_ctr, ctrl);
-}
-
-unsigned pair_scan_chunk_items() { return kScanChunk; }
+size_t sort_scratch_words() { return static_cast<size_t>(kRadix) * kMaxSpans + kRadix; }
+size_t sort_span_sums() { return kMaxSpans; }
 unsigned expand_chunk_pairs() { return kExpandChunk; }
 
+void launch_radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
+                       bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned* scratch,
+                       Ctrl* ctrl, cudaStream_t stream) {
+    const unsigned spans = spans_for(src == SortCount::kFixed ? fixed : capacity);
+    unsigned* counts = scratch;
+    unsigned* totals = scratch + static_cast<size_t>(kRadix) * kMaxSpans;
+    if (masked)
+        upsweep_kernel<true><<<spans, kThreads, 0, stream>>>(keys_in, src, fixed, capacity, shift, spans, counts, ctrl);
+    else
+        upsweep_kernel<false><<<spans, kThreads, 0, stream>>>(keys_in, src, fixed, capacity, shift, spans, counts, ctrl);
+    span_scan_kernel<<<kRadix, kThreads, 0, stream>>>(counts, totals, spans, src, fixed, capacity, ctrl);
+    if (masked)
+        downsweep_kernel<true, true><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src, fixed,
+                                                                    capacity, shift, spans, counts, totals, ctrl);
+    else if (keys_out)
+        downsweep_kernel<false, true><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src, fixed,
+                                                                     capacity, shift, spans, counts, totals, ctrl);
+    else
+        downsweep_kernel<false, false><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src,
+                                                                      fixed, capacity, shift, spans, counts, totals,
+                                                                      ctrl);
+}
+
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
-                      unsigned max_visible, const BatchTables& tables, int tile_passes, const DupBuffers& buf,
-                      unsigned* pair_key,
-                      unsigned* pair_val, unsigned long long* status, cudaStream_t stream) {
-    const unsigned scan_blocks = (max_visible + kScanChunk - 1) / kScanChunk;
-    if (scan_blocks == 0) return;
-    pair_scan_kernel<<<scan_blocks, 256, 0, stream>>>(sorted_idx, rect16, ctrl, capacity, buf.offs, buf.rank,
-                                                      buf.rect_sorted, buf.chunk_start, status);
+                      unsigned max_visible, const BatchTables& tables, const DupBuffers& buf, unsigned* pair_key,
+                      unsigned* pair_val, cudaStream_t stream) {
+    if (max_visible == 0) return;
+    const unsigned spans = spans_for(max_visible);
+    pair_count_kernel<<<spans, kThreads, 0, stream>>>(sorted_idx, rect16, ctrl, spans, buf.rank, buf.rect_sorted,
+                                                      buf.span_sum);
+    pair_offsets_kernel<<<spans, kThreads, 0, stream>>>(buf.rect_sorted, ctrl, spans, capacity, buf.span_sum,
+                                                        buf.offs, buf.chunk_start);
     const unsigned expand_blocks = (capacity + kExpandChunk - 1) / kExpandChunk;
-    expand_kernel<<<expand_blocks, 256, 0, stream>>>(sorted_idx, buf.rect_sorted, buf.offs, buf.chunk_start, ctrl,
-                                                     capacity, tables, tile_passes, pair_key, pair_val);
+    expand_kernel<<<expand_blocks, kThreads, 0, stream>>>(sorted_idx, buf.rect_sorted, buf.offs, buf.chunk_start, ctrl,
+                                                          capacity, tables, pair_key, pair_val);
 }
 
 void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capacity, uint2* ranges,
                    cudaStream_t stream) {
-    ranges_kernel<<<148 * 4, 256, 0, stream>>>(sorted_keys, ctrl, capacity, ranges);
+    const unsigned groups = (capacity + 4u * kThreads - 1) / (4u * kThreads);
+    const unsigned blocks = std::max(1u, std::min(groups, 148u * 8u));
+    ranges_kernel<<<blocks, kThreads, 0, stream>>>(sorted_keys, ctrl, capacity, ranges);
 }
 
 void launch_projection_keys(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
-                            Ctrl* ctrl, unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream) {
-    const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+                            unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream) {
+    const unsigned blocks = static_cast<unsigned>((n + kThreads - 1) / kThreads);
     if (blocks == 0) return;
-    projection_keys_kernel<<<blocks, 256, 0, stream>>>(n, tiles_touched, depth, rect, ctrl, depth_key, rect16);
+    projection_keys_kernel<<<blocks, kThreads, 0, stream>>>(n, tiles_touched, depth, rect, depth_key, rect16);
 }
 
 }  // namespace ab2
