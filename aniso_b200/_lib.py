@@ -17,6 +17,8 @@ ERR_CUDA = 2
 ERR_NO_DEVICE = 3
 ERR_OUT_OF_MEMORY = 4
 ERR_DEVICE_WAIT = 5
+NOALLOC_MAX_GAUSSIANS = 65536   # ANISO_B200_NOALLOC_MAX_GAUSSIANS
+NOALLOC_MAX_PAIRS = 1048576     # ANISO_B200_NOALLOC_MAX_PAIRS
 
 # Every symbol include/aniso_b200.h declares.
 EXPORTS = [
@@ -43,6 +45,7 @@ EXPORTS = [
     "aniso_b200_batch_destroy",
     "aniso_b200_train_batch_forward",
     "aniso_b200_train_batch_backward",
+    "aniso_b200_sort_projection_noalloc",
 ]
 
 
@@ -113,6 +116,7 @@ def _load():
         "aniso_b200_batch_destroy": [P],
         "aniso_b200_train_batch_forward": [P, P, I32, P, P, I32, ctypes.POINTER(BatchOptions), P, P],
         "aniso_b200_train_batch_backward": [P, P, P, P],
+        "aniso_b200_sort_projection_noalloc": [I64, P, P, P, I32, I32, P, P, U64, P, P, P],
         "aniso_b200_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(I64)],
     }

@@ -444,6 +444,11 @@ constexpr int kSlots = 8;
 
 }  // namespace
 
+namespace ab2 {
+// For entry points defined in other files: sets the aniso_b200_last_error message, returns code.
+int report_error(int code, const char* msg) { return fail(code, msg); }
+}  // namespace ab2
+
 // ---- scenes ------------------------------------------------------------------------------------
 
 struct aniso_b200_scene {

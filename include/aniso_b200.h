@@ -227,6 +227,29 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
                                int32_t tiles_x, int32_t tiles_y, uint32_t* tiles, uint32_t* values,
                                uint64_t capacity, uint32_t* ranges, uint64_t* pairs);
 
+/* ---- a sort that allocates nothing (no counterpart in the reference, whose GpuRenderer grows
+ * its buffers with cudaFree + cudaMalloc inside render(), gpu_render.cu:24-37, 326-354) ---------
+ * For callers that must not touch the CUDA allocator while they run: a render loop or a serving
+ * worker that keeps all device memory in its own pool, where cudaFree would synchronise the whole
+ * device and cudaMalloc could stall or fail in the middle of a frame. Same sort and outputs as
+ * aniso_b200_sort_projection, but every array is a DEVICE pointer, the work is enqueued on
+ * `stream` without waiting, and the work buffers are one static device array of about 20 MB per
+ * device (held once the call has been used on that device), which bounds the problem size:
+ *   n <= ANISO_B200_NOALLOC_MAX_GAUSSIANS (else ANISO_B200_ERR_ARGUMENT, nothing enqueued);
+ *   pairs beyond min(capacity, ANISO_B200_NOALLOC_MAX_PAIRS) are not written: tiles/values are
+ *   left untouched, ranges are all zero, and *pairs (device) still receives the total.
+ * A rectangle outside the tile grid refuses the call on the device: *pairs = UINT64_MAX.
+ * Alignment: rect and tiles 16 bytes, ranges and pairs 8 bytes (cudaMalloc'd memory is).
+ * The static buffers are shared: calls on one device must not overlap in time (issue them on one
+ * stream, or wait for the previous one). The first call on a device looks the buffers up
+ * (cudaGetSymbolAddress), so make it before any stream capture starts. */
+#define ANISO_B200_NOALLOC_MAX_GAUSSIANS 65536
+#define ANISO_B200_NOALLOC_MAX_PAIRS 1048576
+int aniso_b200_sort_projection_noalloc(int64_t n, const uint32_t* tiles_touched, const uint32_t* rect,
+                                       const float* depth, int32_t tiles_x, int32_t tiles_y, uint32_t* tiles,
+                                       uint32_t* values, uint64_t capacity, uint32_t* ranges, uint64_t* pairs,
+                                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif
