@@ -53,6 +53,22 @@ def _release(t: Trainer):
     _pool.append(t)
 
 
+class _Lease:
+    """Holds a trainer for one forward until its backward, and gives it back to the pool (not
+    destroys it) if the graph is dropped without a backward -- e.g. a forward under no_grad."""
+
+    def __init__(self, trainer: Trainer):
+        self.trainer = trainer
+
+    def release(self):
+        if self.trainer is not None:
+            _release(self.trainer)
+            self.trainer = None
+
+    def __del__(self):
+        self.release()
+
+
 def _raw_params(means, log_scales, quats, opacity_logits, sh) -> _lib.RawParams:
     n = means.shape[0]
     k = sh.shape[1]
@@ -83,11 +99,10 @@ class RasterizeFunction(torch.autograd.Function):
         except Exception:
             _release(trainer)
             raise
-        if any(ctx.needs_input_grad[:5]):
-            ctx.trainer = trainer
-        else:
-            ctx.trainer = None
-            _release(trainer)  # no backward will come; the next forward on this stream is ordered after
+        # The next forward on this trainer is ordered after this one's kernels (same stream).
+        ctx.lease = _Lease(trainer)
+        if not any(ctx.needs_input_grad[:5]):
+            ctx.lease.release()
         ctx.save_for_backward(means, log_scales, quats, opacity_logits, sh)
         return img
 
@@ -98,14 +113,14 @@ class RasterizeFunction(torch.autograd.Function):
         g = _lib.RawGrads(*[t.data_ptr() for t in grads])
         gi = grad_img.contiguous().float()
         stream = torch.cuda.current_stream(means.device).cuda_stream
-        trainer = ctx.trainer
+        if ctx.lease.trainer is None:
+            raise RuntimeError("this render's backward already ran (its work buffers are reused): render again")
         try:
-            check(lib.aniso_b200_train_backward(trainer._h, ctypes.c_void_p(gi.data_ptr()), ctypes.byref(g),
-                                                ctypes.c_void_p(stream)))
+            check(lib.aniso_b200_train_backward(ctx.lease.trainer._h, ctypes.c_void_p(gi.data_ptr()),
+                                                ctypes.byref(g), ctypes.c_void_p(stream)))
         finally:
-            ctx.trainer = None
             # The next forward on this trainer is ordered after the backward's kernels (same stream).
-            _release(trainer)
+            ctx.lease.release()
         return (*grads, None, None)
 
 
@@ -137,11 +152,9 @@ class RasterizeBatchFunction(torch.autograd.Function):
         except Exception:
             _release(trainer)
             raise
-        if any(ctx.needs_input_grad[1:]):
-            ctx.trainer = trainer
-        else:
-            ctx.trainer = None
-            _release(trainer)
+        ctx.lease = _Lease(trainer)
+        if not any(ctx.needs_input_grad[1:]):
+            ctx.lease.release()
         ctx.n_scenes = S
         ctx.save_for_backward(*tensors)
         return tuple(imgs)
@@ -156,12 +169,12 @@ class RasterizeBatchFunction(torch.autograd.Function):
         gi = [gimg.contiguous().float() for gimg in grad_imgs]
         ptrs = (ctypes.c_void_p * len(gi))(*[t.data_ptr() for t in gi])
         stream = torch.cuda.current_stream(tensors[0].device).cuda_stream
-        trainer = ctx.trainer
+        if ctx.lease.trainer is None:
+            raise RuntimeError("this render's backward already ran (its work buffers are reused): render again")
         try:
-            check(lib.aniso_b200_train_batch_backward(trainer._h, ptrs, g, ctypes.c_void_p(stream)))
+            check(lib.aniso_b200_train_batch_backward(ctx.lease.trainer._h, ptrs, g, ctypes.c_void_p(stream)))
         finally:
-            ctx.trainer = None
-            _release(trainer)
+            ctx.lease.release()
         return (None, *grads)
 
 

@@ -1,0 +1,116 @@
+"""Launch-shape autotuner for batched rendering.
+
+For a batch (its scenes and its cameras), times every candidate launch shape -- tile shape
+(8x8, 16x16, 16x32), blend batch (128, 256 splats staged per round) -- with the batch's own CUDA
+graph, keeps the fastest, and caches the choice in a JSON file keyed by the GPU name and a
+signature of the workload (Gaussian counts, view count, resolutions). Every candidate renders the
+same image (the tile shape only changes how pixels are grouped), so the choice is a pure speed
+decision; the tuner checks that the candidates agree on one view before it trusts them.
+
+    best = tune(scenes, view_scene, cameras)            # -> BatchOptions
+    batch = BatchRenderer(scenes, view_scene, best)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+
+import numpy as np
+
+from .renderer import BatchOptions, BatchRenderer
+
+TILES = [(8, 8), (16, 16), (16, 32)]
+BLEND_BATCHES = [128, 256]
+CACHE_PATH = os.path.join(os.path.expanduser("~"), ".cache", "aniso_b200", "autotune.json")
+
+
+def signature(scenes, view_scene, cameras, sh_degree: int, splat_scale: float) -> str:
+    """Workload key: Gaussians per scene, the view -> scene map, resolutions, colour options."""
+    parts = [",".join(str(s.n) for s in scenes), ",".join(str(int(v)) for v in view_scene),
+             ",".join("%dx%d" % (c.width, c.height) for c in cameras), "sh%d" % sh_degree, "s%g" % splat_scale]
+    return hashlib.sha1("|".join(parts).encode()).hexdigest()[:16]
+
+
+def _load_cache(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _store_cache(path, cache):
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass  # a read-only home only costs a re-tune next time
+
+
+def time_batch(batch: BatchRenderer, cameras, ptrs, stream, warmup: int = 2, iters: int = 5) -> float:
+    """Device milliseconds per batched render (CUDA events on `stream`)."""
+    import torch
+
+    from ._lib import AnisoError
+
+    for _ in range(warmup):
+        for _attempt in range(3):  # a first frame may overflow the pair capacity and grow it
+            batch.render_device(cameras, ptrs, stream.cuda_stream)
+            try:
+                batch.sync()
+                break
+            except AnisoError as e:
+                if "pair capacity" not in str(e):
+                    raise
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(iters):
+        batch.render_device(cameras, ptrs, stream.cuda_stream)
+    e1.record(stream)
+    batch.sync()
+    return e0.elapsed_time(e1) / iters
+
+
+def tune(scenes, view_scene, cameras, sh_degree: int = 3, splat_scale: float = 1.0, use_graph: bool = True,
+         cache_path: str | None = CACHE_PATH, force: bool = False, report: list | None = None) -> BatchOptions:
+    """The fastest launch shape for this batch (from the cache when it holds this GPU/workload)."""
+    import torch
+
+    gpu = torch.cuda.get_device_name()
+    key = "%s|%s" % (gpu, signature(scenes, view_scene, cameras, sh_degree, splat_scale))
+    cache = _load_cache(cache_path) if cache_path else {}
+    if not force and key in cache:
+        c = cache[key]
+        return BatchOptions(sh_degree, splat_scale, tuple(c["tile"]), int(c["blend_batch"]), use_graph)
+
+    outs = [torch.empty((c.height, c.width, 3), dtype=torch.uint8, device="cuda") for c in cameras]
+    ptrs = [o.data_ptr() for o in outs]
+    stream = torch.cuda.Stream()
+    results = []
+    probe = None
+    for tile in TILES:
+        for bb in BLEND_BATCHES:
+            opt = BatchOptions(sh_degree, splat_scale, tile, bb, use_graph)
+            b = BatchRenderer(scenes, view_scene, opt)
+            ms = time_batch(b, cameras, ptrs, stream)
+            img = outs[0].cpu().numpy()
+            if probe is None:
+                probe = img
+            elif not np.array_equal(img, probe):
+                raise RuntimeError("launch shapes disagree on the image (tile %s, batch %d)" % (tile, bb))
+            results.append({"tile": list(tile), "blend_batch": bb, "ms": ms})
+            b.close()
+    best = min(results, key=lambda r: r["ms"])
+    if report is not None:
+        report.extend(results)
+    if cache_path:
+        cache[key] = dict(best, candidates=results)
+        _store_cache(cache_path, cache)
+    return BatchOptions(sh_degree, splat_scale, tuple(best["tile"]), int(best["blend_batch"]), use_graph)
+
+
+__all__ = ["tune", "time_batch", "signature", "TILES", "BLEND_BATCHES", "CACHE_PATH"]

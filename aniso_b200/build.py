@@ -6,7 +6,9 @@
 Each csrc/*.cu file is compiled separately (in parallel) with -O3, IEEE division and square root
 (no --use_fast_math: the projection must round like the reference kernel built without it),
 -lineinfo for ncu source correlation, and -Xptxas -v, whose register / spill / shared-memory
-report is written to _build/ptxas.txt. The GpuRenderer shim (shim/gpu_render_shim.cpp) is built
+report is written to _build/ptxas.txt. csrc/peaks/peaks.cu becomes libaniso_b200_peaks.so, the
+ex2 / FMA throughput probe whose rates are the blend's compute-roofline denominators (the
+renderer does not link it). The GpuRenderer shim (shim/gpu_render_shim.cpp) is built
 by oracle/Makefile's `dropin` target, against the reference's headers.
 """
 from __future__ import annotations
@@ -22,6 +24,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libaniso_b200.so")
+PEAKS_SRC = os.path.join(CSRC, "peaks", "peaks.cu")
+PEAKS_LIB = os.path.join(PKG, "libaniso_b200_peaks.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v", "-I", os.path.join(ROOT, "include")]
@@ -64,6 +68,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stdout + r.stderr))
+    if force or _newer(PEAKS_LIB, [PEAKS_SRC]):
+        cmd = [NVCC] + GENCODE + ["-O3", "-Xcompiler", "-fPIC", "-shared", PEAKS_SRC, "-o", PEAKS_LIB, "-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed for %s:\n%s" % (PEAKS_SRC, r.stdout + r.stderr))
     return LIB
 
 

@@ -4,14 +4,15 @@
 // blend_backward: one block per tile of a batch, the forward's pixel layout (8x8 per warp, two
 //   pixels per lane). Each pixel walks its tile list back to front from its last applied
 //   splat, replaying the forward's alpha tests bit for bit (same record, same exponent code) and
-//   recovering the transmittance in front of each splat by division (T_j = T_{j+1} / (1 - a_j));
+//   recovering the transmittance in front of each splat (T_j = T_{j+1} / (1 - a_j));
 //   nothing per pixel is stored but the final T and the last contributor. Per splat, the gradient
 //   with respect to its nine record parameters (u, v, A2, B2, C2, L, r, g, b) is reduced over the
-//   warp (12 shuffles for the 9 values), summed over the four warps in a fixed order, and written
+//   warp (12 shuffles for the 9 values; skipped when no pixel of the warp took the splat), summed
+//   over the warps in a fixed order, and written
 //   to the pair's slot in the depth-ordered pair list -- no atomics, so the result does not depend
 //   on scheduling.
-// gauss_backward: one launch per view, one thread per Gaussian of its scene; a Gaussian visible in
-//   the view sums its pairs' slots, which are contiguous and summed in list order, applies the
+// gauss_backward: one launch per view over the Gaussians visible in it (compacted first, so no lane
+//   idles on a culled one); each sums its pairs' slots (contiguous, in a fixed order), applies the
 //   chain rule through the record
 //   (conic, log2 opacity, SH colour), the EWA projection (2D covariance, clamped Jacobian, camera
 //   transform), the 3D covariance M M^T with M = R(q) diag(s), and the activations (exp, sigmoid,
@@ -70,20 +71,28 @@ struct PixelState {
     unsigned last;           // list position one past the last applied splat
 };
 
-// One pixel's adjoint step for splat j (list position pos); adds to g[0..8].
-__device__ __forceinline__ void pixel_step(PixelState& s, unsigned pos, float p, float dx, float dy, const float4& r0,
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// One pixel's adjoint step for splat j (list position pos); adds to g[0..8] and returns whether
+// the splat was applied to this pixel in the forward (else it contributes nothing).
+// 1/(1 - alpha) is the approximate reciprocal (relative error below 2^-22): the recovered
+// transmittance drifts by that much per splat, far inside the gradients' tolerance.
+__device__ __forceinline__ bool pixel_step(PixelState& s, unsigned pos, float p, float dx, float dy, const float4& r0,
                                            const float4& r1, float rb, float g[kG]) {
-    if (pos >= s.last) return;
+    if (pos >= s.last) return false;
     const float e = ex2_approx(p);
     const float alpha = fminf(0.99f, e);  // the same bits as the forward's splat_alpha
-    if (!(!(p > r1.y) && alpha >= 1.0f / 255.0f)) return;
-    const float om = 1.0f - alpha;
-    const float Tb = s.T / om;  // transmittance in front of the splat
+    if (!(!(p > r1.y) && alpha >= 1.0f / 255.0f)) return false;
+    const float inv_om = rcp_approx(1.0f - alpha);
+    const float Tb = s.T * inv_om;  // transmittance in front of the splat
     const float w = alpha * Tb;
     g[6] = fmaf(s.gr, w, g[6]);
     g[7] = fmaf(s.gg, w, g[7]);
     g[8] = fmaf(s.gb, w, g[8]);
-    const float inv_om = 1.0f / om;
     const float dalpha = s.gr * (r1.z * Tb - s.ar * inv_om) + s.gg * (r1.w * Tb - s.ag * inv_om) +
                          s.gb * (rb * Tb - s.ab * inv_om);
     s.ar = fmaf(r1.z, w, s.ar);
@@ -97,6 +106,7 @@ __device__ __forceinline__ void pixel_step(PixelState& s, unsigned pos, float p,
     g[3] = fmaf(dp, dx * dy, g[3]);
     g[4] = fmaf(dp, dy * dy, g[4]);
     g[5] += dp;
+    return true;
 }
 
 template <int TW, int TH>
@@ -209,8 +219,10 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_backward_kernel(BackwardIn 
                     float p0, p1;
                     splat_exponents(r0, r1, dx0, dy, p0, p1);
                     float g[kG] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                    pixel_step(s0, pos, p0, dx0, dy, r0, r1, rb, g);
-                    pixel_step(s1, pos, p1, __fadd_rn(dx0, 1.0f), dy, r0, r1, rb, g);
+                    const bool a0 = pixel_step(s0, pos, p0, dx0, dy, r0, r1, rb, g);
+                    const bool a1 = pixel_step(s1, pos, p1, __fadd_rn(dx0, 1.0f), dy, r0, r1, rb, g);
+                    // No pixel of the warp took the splat: its share is zero, leave it out of the sum.
+                    if (!__any_sync(0xFFFFFFFFu, a0 || a1)) continue;
                     int k;
                     const float sum = warp_reduce9(g, lane, k);
                     if (k >= 0) s_grad[warp][jj][k] = sum;
@@ -283,26 +295,75 @@ __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16],
     }
 }
 
+// The Gaussians of one view that are visible in it, appended in any order: the adjoint of each is
+// independent of where it sits in the list, so the order does not change any result.
+__global__ void __launch_bounds__(256) visible_list_kernel(int64_t n, unsigned entry_base,
+                                                           const unsigned* __restrict__ depth_key,
+                                                           unsigned* __restrict__ list, unsigned* counter) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool vis = i < n && depth_key[entry_base + static_cast<unsigned>(i)] != kCulledKey;
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, vis);
+    if (!m) return;
+    unsigned base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, __ffs(m) - 1);
+    if (vis) list[base + __popc(m & lanemask_lt())] = static_cast<unsigned>(i);
+}
+
 template <int D>
 __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamParams cam, unsigned entry_base,
-                                                             const Ctrl* ctrl, const unsigned* __restrict__ depth_key,
+                                                             const Ctrl* ctrl, const unsigned* __restrict__ list,
+                                                             const unsigned* __restrict__ list_count,
                                                              const unsigned* __restrict__ rank,
                                                              const unsigned* __restrict__ offs,
                                                              const unsigned long long* __restrict__ rect_sorted,
                                                              const float* __restrict__ grad_pair, RawGrads out) {
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
-    if (i >= raw.n) return;
+    const unsigned count = *list_count;
+    if (blockIdx.x * blockDim.x >= count) return;
+    const int lane = threadIdx.x & 31;
+    // Past the end of the list: no Gaussian, but the lane still helps its warp.
+    const bool active = t < count;
+    const int64_t i = active ? list[t] : 0;
     const unsigned e = entry_base + static_cast<unsigned>(i);
-    if (depth_key[e] == kCulledKey) return;  // culled in this view: no gradient from it
-    const unsigned j = rank[e];
-    const unsigned long long rc = rect_sorted[j];
-    const unsigned cnt = ((rc >> 32 & 0xFFFFu) - (rc & 0xFFFFu) + 1) * ((rc >> 48) - (rc >> 16 & 0xFFFFu) + 1);
+    unsigned cnt = 0, off = 0;
+    if (active) {
+        const unsigned j = rank[e];
+        const unsigned long long rc = rect_sorted[j];
+        cnt = ((rc >> 32 & 0xFFFFu) - (rc & 0xFFFFu) + 1) * ((rc >> 48) - (rc >> 16 & 0xFFFFu) + 1);
+        off = offs[j];
+    }
+    // The sum of the Gaussian's per-pair gradients, in a fixed order: a short list by its own lane,
+    // slot after slot; a long one (the nearest splats own thousands of tiles) by the whole warp,
+    // lane l taking slots l, l + 32, ..., then a fixed shuffle tree -- so one huge splat does not
+    // hold its warp for thousands of serial loads.
+    constexpr unsigned kSolo = 16;
     float g9[kG] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    const float* gp = grad_pair + static_cast<size_t>(offs[j]) * kG;
-    for (unsigned k = 0; k < cnt; ++k)
+    if (cnt <= kSolo) {
+        const float* gp = grad_pair + static_cast<size_t>(off) * kG;
+        for (unsigned k = 0; k < cnt; ++k)
 #pragma unroll
-        for (int c = 0; c < kG; ++c) g9[c] += gp[k * kG + c];
+            for (int c = 0; c < kG; ++c) g9[c] += gp[k * kG + c];
+    }
+    for (unsigned big = __ballot_sync(0xFFFFFFFFu, cnt > kSolo); big; big &= big - 1) {
+        const int src = __ffs(big) - 1;
+        const unsigned bc = __shfl_sync(0xFFFFFFFFu, cnt, src), bo = __shfl_sync(0xFFFFFFFFu, off, src);
+        const float* gp = grad_pair + static_cast<size_t>(bo) * kG;
+        float part[kG] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (unsigned k = lane; k < bc; k += 32)
+#pragma unroll
+            for (int c = 0; c < kG; ++c) part[c] += gp[k * kG + c];
+#pragma unroll
+        for (int c = 0; c < kG; ++c) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part[c] += __shfl_down_sync(0xFFFFFFFFu, part[c], o);
+            part[c] = __shfl_sync(0xFFFFFFFFu, part[c], 0);
+            if (lane == src) g9[c] = part[c];
+        }
+    }
+    if (!active) return;
 
     // ---- forward quantities (the preprocess kernel's, in the same order) ----
     float4 pg, sg, qn;
@@ -491,15 +552,17 @@ void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int
 
 void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
                            const unsigned* depth_key, const unsigned* rank, const unsigned* offs,
-                           const unsigned long long* rect_sorted, const float* grad_pair, const RawGrads& out,
-                           cudaStream_t stream) {
+                           const unsigned long long* rect_sorted, const float* grad_pair, unsigned* list,
+                           unsigned* list_count, const RawGrads& out, cudaStream_t stream) {
+    const unsigned lblocks = static_cast<unsigned>((raw.n + 255) / 256);
+    if (lblocks == 0) return;
+    visible_list_kernel<<<lblocks, 256, 0, stream>>>(raw.n, entry_base, depth_key, list, list_count);
     const unsigned blocks = static_cast<unsigned>((raw.n + 127) / 128);
-    if (blocks == 0) return;
     switch (cam.shDegree) {
-        case 0: gauss_backward_kernel<0><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, depth_key, rank, offs, rect_sorted, grad_pair, out); break;
-        case 1: gauss_backward_kernel<1><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, depth_key, rank, offs, rect_sorted, grad_pair, out); break;
-        case 2: gauss_backward_kernel<2><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, depth_key, rank, offs, rect_sorted, grad_pair, out); break;
-        default: gauss_backward_kernel<3><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, depth_key, rank, offs, rect_sorted, grad_pair, out); break;
+        case 0: gauss_backward_kernel<0><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
+        case 1: gauss_backward_kernel<1><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
+        case 2: gauss_backward_kernel<2><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
+        default: gauss_backward_kernel<3><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
     }
 }
 

@@ -1064,6 +1064,8 @@ struct aniso_b200_trainer {
     std::vector<DevBuf<float>> t_final;
     std::vector<DevBuf<unsigned>> n_contrib;
     DevBuf<float> grad_pair;
+    DevBuf<unsigned> vis_list;    // one view's visible Gaussians (the backward's work list)
+    DevBuf<unsigned> vis_counts;  // their count, one word per view
     // The state of the last forward, for its backward.
     bool has_forward = false;
     Plan<RawParams> plan;
@@ -1166,13 +1168,19 @@ int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const
     in.rank = A.rank.p;
     in.offs = A.offs.p;
     in.rect_sorted = A.rect_sorted.p;
+    int64_t max_n = 1;
+    for (const auto& sc : P.scenes) max_n = std::max<int64_t>(max_n, sc.src.n);
+    AB_TRY(t->vis_list.reserve(static_cast<size_t>(max_n)));
+    AB_TRY(t->vis_counts.reserve(P.views.size()));
+    AB_CUDA(cudaMemsetAsync(t->vis_counts.p, 0, P.views.size() * sizeof(unsigned), st));
     launch_blend_backward(in, static_cast<unsigned>(P.tiles), P.shape.tile_w, P.shape.tile_h, t->grad_pair.p, st);
     for (size_t k = 0; k < P.views.size(); ++k) {
         const unsigned s = P.views[k].scene;
         const aniso_b200_raw_grads& g = grads[s];
         const RawGrads out{g.means, g.log_scales, g.quats, g.opacity_logits, g.sh};
         launch_gauss_backward(P.scenes[s].src, P.views[k].cam, P.views[k].entry_base, A.ctrl.p, A.depth_key.p,
-                              A.rank.p, A.offs.p, A.rect_sorted.p, t->grad_pair.p, out, st);
+                              A.rank.p, A.offs.p, A.rect_sorted.p, t->grad_pair.p, t->vis_list.p, t->vis_counts.p + k,
+                              out, st);
     }
     AB_TRY(slot.mark(st));
     AB_CUDA(cudaGetLastError());

@@ -103,10 +103,11 @@ struct RawGrads {
 // grad_pair: 9 floats per pair, at the pair's depth-ordered slot.
 void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int tile_h, float* grad_pair,
                            cudaStream_t stream);
-// One view: its scene's Gaussians visible in it add their gradients to `out`.
+// One view: its scene's Gaussians visible in it add their gradients to `out`. list (the scene's n
+// words) and *list_count (zero on entry) are work space for the compacted visible list.
 void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
                            const unsigned* depth_key, const unsigned* rank, const unsigned* offs,
-                           const unsigned long long* rect_sorted, const float* grad_pair, const RawGrads& out,
-                           cudaStream_t stream);
+                           const unsigned long long* rect_sorted, const float* grad_pair, unsigned* list,
+                           unsigned* list_count, const RawGrads& out, cudaStream_t stream);
 
 }  // namespace ab2

@@ -12,6 +12,12 @@ written to device memory). `e2e` renders the same views through the public C ABI
 aniso_b200_render (the drop-in for GpuRenderer::render) into pinned host memory, so each view's
 device-to-host image copy is inside the timed region. Under torchrun each rank renders its own
 replica's 16 views (weak scaling, no collective); time is the max over ranks.
+
+Two more workloads of the same metric family ride along on rank 0 (skip with --no-extra):
+  "batched":  one 1M-Gaussian scene, 64 Fibonacci-sphere views of mixed resolution, rendered by one
+              autotuned, graph-replayed batch versus 64 plain per-view launches (views/s);
+  "fwd_bwd":  the 2.2M-Gaussian scene at 1280x720, forward + hand-written adjoint through the
+              torch.autograd.Function against an L2 loss (ms/view).
 """
 from __future__ import annotations
 
@@ -174,12 +180,135 @@ def cpu_baseline_leg(gauss, sh, cams, images):
     return base, {"max_abs_255": worst_abs, "psnr_db": worst_psnr, "views": views, "vs": "CPU renderer"}
 
 
+def kernels_per_frame(tiles: int) -> int:
+    """Our kernel launches per rendered frame: frame_begin, preprocess, 4 depth passes of 3
+    (upsweep, span scan, downsweep), pair count / offsets / expansion, the tile passes (3 each),
+    ranges, blend."""
+    tile_passes = max(1, (max(tiles - 1, 0).bit_length() + 7) // 8)
+    return 4 + 4 * 3 + 3 + 3 * tile_passes
+
+
+def measured_compute_peaks():
+    """ex2 and FP32 FMA rates of this GPU from the library's throughput probe (ops/s)."""
+    import ctypes
+
+    lib = ctypes.CDLL(os.path.join(ROOT, "aniso_b200", "libaniso_b200_peaks.so"))
+    ex2, fma = ctypes.c_double(), ctypes.c_double()
+    if lib.ab2_measure_peaks(ctypes.byref(ex2), ctypes.byref(fma)) != 0:
+        return None, None
+    return ex2.value, fma.value
+
+
+def batched_leg(torch, steps: int):
+    """Workload 4: 1M Gaussians, 64 sphere views of mixed resolution; batch vs per-view launches."""
+    from aniso_b200 import BatchRenderer, GpuRenderer, scenes
+    from aniso_b200._lib import AnisoError
+    from aniso_b200.autotune import time_batch, tune
+
+    raws, camsets = scenes.config(4)
+    cams = camsets[0]
+    r = GpuRenderer.from_raw(raws[0])
+    outs = [torch.empty((c.height, c.width, 3), dtype=torch.uint8, device="cuda") for c in cams]
+    ptrs = [o.data_ptr() for o in outs]
+    stream = torch.cuda.Stream()
+
+    def per_view():
+        for c, p in zip(cams, ptrs):
+            r.render_device(c, p, stream.cuda_stream)
+
+    for _ in range(3):
+        for _attempt in range(3):
+            per_view()
+            try:
+                r.sync()
+                break
+            except AnisoError as e:
+                if "pair capacity" not in str(e):
+                    raise
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        per_view()
+    e1.record(stream)
+    r.sync()
+    ms_pv = e0.elapsed_time(e1) / steps
+    ref = [o.cpu().numpy() for o in outs]
+    candidates = []
+    best = tune([r], [0] * len(cams), cams, cache_path=None, report=candidates)
+    b = BatchRenderer([r], [0] * len(cams), best)
+    ms_b = time_batch(b, cams, ptrs, stream, warmup=3, iters=steps)
+    same = all(np.array_equal(o.cpu().numpy(), x) for o, x in zip(outs, ref))
+    st = b.sync()
+    V = len(cams)
+    return {"workload": "1M-Gaussian SH3 scene, 64 Fibonacci-sphere views (radius 10), resolutions drawn from "
+                        "320x180/640x360/1280x720/1920x1080, f = 0.9 W",
+            "views_per_s": V * 1000.0 / ms_b, "views_per_s_per_view_launches": V * 1000.0 / ms_pv,
+            "speedup_vs_per_view": ms_pv / ms_b, "ms_per_batch": ms_b, "ms_per_64_plain_launches": ms_pv,
+            "gaussians_per_s": V * raws[0].n / (ms_b / 1000.0),
+            "tuned": {"tile": "%dx%d" % best.tile, "blend_batch": best.blend_batch, "cuda_graph": True},
+            "candidates_ms": {"%dx%d/%d" % (c["tile"][0], c["tile"][1], c["blend_batch"]): round(c["ms"], 3)
+                              for c in candidates},
+            "pairs": st["tile_pairs"], "images_equal_per_view": same}
+
+
+def fwd_bwd_leg(torch, steps: int):
+    """Workload 3: 2.2M Gaussians, 1280x720, L2 loss against the perturbed-scene target."""
+    from aniso_b200 import scenes
+    from aniso_b200.autograd import rasterize
+
+    raws, camsets = scenes.config(3)
+    raw, cam = raws[0], camsets[0][0]
+
+    def params(rw, grad):
+        n = rw.n
+        sh = np.concatenate([rw.f_dc.reshape(n, 1, 3), rw.f_rest.reshape(n, 3, 15).transpose(0, 2, 1)], 1)
+        arrs = [rw.xyz, rw.scale, rw.rot, rw.opacity, np.ascontiguousarray(sh)]
+        return [torch.tensor(a, dtype=torch.float32, device="cuda", requires_grad=grad) for a in arrs]
+
+    with torch.no_grad():
+        target = rasterize(*params(scenes.perturbed_target(raw), False), cam)
+    ps = params(raw, True)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        for p in ps:
+            p.grad = None
+        img = rasterize(*ps, cam)
+        ((img - target) ** 2).sum().backward()
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    with torch.no_grad():
+        for _ in range(3):
+            rasterize(*ps, cam)
+        e0.record(stream)
+        for _ in range(steps):
+            rasterize(*ps, cam)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms_f = e0.elapsed_time(e1) / steps
+    finite = all(bool(torch.isfinite(p.grad).all()) for p in ps)
+    return {"workload": "2.2M-Gaussian SH3 scene (30x8x30 box), 1280x720, L2 loss vs the perturbed-scene target, "
+                        "grads of all 59 raw parameters through torch.autograd.Function",
+            "ms_per_view_fwd_bwd": ms, "ms_per_view_fwd_train": ms_f, "gaussians": raw.n,
+            "grads_finite": finite, "target_ms": 3.0}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched and fwd+bwd workloads")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -286,7 +415,16 @@ def main():
         blend_bytes = pairs_per_step / V * 40 + W * H * 3
         achieved = blend_bytes / (blend_ms / 1000.0) / 1e9
         base, acc = cpu_baseline_leg(gauss, sh, cams, images)
-        kernels_per_frame = 11  # frame_begin, preprocess, 4 depth passes, duplicate, 2 tile passes, ranges, blend
+        tiles = ((W + 15) // 16) * ((H + 15) // 16)
+        ex2_peak, fma_peak = measured_compute_peaks()
+        # Algorithmic blend work: P * 256 pixel-splat evaluations per view (the upper bound; early
+        # termination counts as speed-up), one MUFU ex2 each.
+        evals = pairs_per_step / V * 256
+        evals_per_s = evals / (blend_ms / 1000.0)
+        extra = {}
+        if not args.no_extra:
+            extra["batched"] = batched_leg(torch, max(3, min(args.steps, 10)))
+            extra["fwd_bwd"] = fwd_bwd_leg(torch, max(3, min(args.steps, 10)))
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "ms_per_frame": ms_step / V,
@@ -306,15 +444,20 @@ def main():
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": BLEND_TRAFFIC_BYTES,
                          "note": "blend is FP32/MUFU-issue bound, not HBM bound; bytes per launch = P*40 + W*H*3"},
+            "compute_roofline": {"kernel": "blend", "bound": "mufu_ex2", "achieved": evals_per_s,
+                                 "peak": ex2_peak, "unit": "ex2/s", "frac": (evals_per_s / ex2_peak) if ex2_peak else None,
+                                 "fp32_fma_peak": fma_peak, "peak_source": "measured (libaniso_b200_peaks.so)",
+                                 "work": "P*256 pixel-splat evaluations per view, one ex2 each"},
             "cpu_baseline": base,
             "accuracy": acc,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": V * 136,
                     "d2h_bytes_per_step": V * (H * W * 3 + 64),
                     "path": "aniso_b200_render (GpuRenderer::render drop-in), pinned host output"},
-            "gpu_launches": kernels_per_frame * V * args.steps,
+            "gpu_launches": kernels_per_frame(tiles) * V * args.steps,
             "timed_images_match_host_api": same,
             "clocks": sampler.summary(),
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
