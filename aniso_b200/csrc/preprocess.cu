@@ -20,10 +20,12 @@ constexpr float kShC3_0 = -0.5900435899266435f, kShC3_1 = 2.890611442640554f, kS
                 kShC3_3 = 0.3731763325901154f, kShC3_4 = -0.4570457994644658f, kShC3_5 = 1.445305721320277f,
                 kShC3_6 = -0.5900435899266435f;
 
-// SH colour of degree D along (x, y, z): the basis of sh.cpp:18-58 / gpu_render.cu:56-83, summed in
-// the same order, then +0.5 and clamped at 0.
+// SH colour of degree D along (x, y, z): the basis of sh.cpp:18-58 / gpu_render.cu:56-83, then
+// +0.5 and clamped at 0. The coefficients are streamed straight from the Gaussian's 16-byte words
+// ([coefficient][channel] order), so nothing stays live across views; each channel still sums its
+// terms in ascending coefficient order, as the reference does.
 template <int D>
-__device__ __forceinline__ float3 sh_color(const float* sh, float x, float y, float z) {
+__device__ __forceinline__ float3 sh_color(const float4* __restrict__ shp, float x, float y, float z) {
     float b[16];
     b[0] = 0.28209479177387814f;
     if (D >= 1) {
@@ -39,15 +41,20 @@ __device__ __forceinline__ float3 sh_color(const float* sh, float x, float y, fl
             b[14] = kShC3_5 * z * (xx - yy); b[15] = kShC3_6 * x * (xx - 3 * yy);
         }
     }
-    constexpr int count = (D + 1) * (D + 1);
-    float3 c = make_float3(0.5f, 0.5f, 0.5f);
+    constexpr int kFloats = (D + 1) * (D + 1) * 3;
+    constexpr int kPlanes = (kFloats + 3) / 4;
+    float c[3] = {0.5f, 0.5f, 0.5f};
 #pragma unroll
-    for (int k = 0; k < count; ++k) {
-        c.x += b[k] * sh[k * 3 + 0];
-        c.y += b[k] * sh[k * 3 + 1];
-        c.z += b[k] * sh[k * 3 + 2];
+    for (int k = 0; k < kPlanes; ++k) {
+        const float4 f = shp[k];
+        const float v[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int idx = 4 * k + e;
+            if (idx < kFloats) c[idx % 3] += b[idx / 3] * v[e];
+        }
     }
-    return make_float3(fmaxf(c.x, 0.f), fmaxf(c.y, 0.f), fmaxf(c.z, 0.f));
+    return make_float3(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f), fmaxf(c[2], 0.f));
 }
 
 struct Projected {
@@ -58,32 +65,77 @@ struct Projected {
     int x0, y0, x1, y1;       // 16x16-tile rectangle
 };
 
+// The view-independent part of gpu_render.cu:101-111, evaluated once per Gaussian for all its
+// views with the same expressions in the same order: the 3D covariance S = M M^T with
+// M = R(q) diag(s * splat_scale), and tr(S) for the early screen test. S is kept as its upper
+// triangle: S[c][r] and S[r][c] are the same products summed in the same order, so equal bits.
+struct Cov3 {
+    float s00, s01, s02, s11, s12, s22;
+    float trace;
+    __device__ __forceinline__ float at(int r, int c) const {
+        const int lo = r < c ? r : c, hi = r < c ? c : r;
+        return lo == 0 ? (hi == 0 ? s00 : hi == 1 ? s01 : s02) : lo == 1 ? (hi == 1 ? s11 : s12) : s22;
+    }
+};
+
+__device__ __forceinline__ void covariance(const float4 sg, const float4 q, float splat_scale, Cov3& o) {
+    const float w = q.x, x = q.y, y = q.z, z = q.w;
+    const float Rq[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)},
+                            {2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)},
+                            {2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)}};
+    const float s[3] = {sg.x * splat_scale, sg.y * splat_scale, sg.z * splat_scale};
+    float M[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) M[r][c] = Rq[r][c] * s[c];
+    const auto dot = [&](int r, int c) { return M[r][0] * M[c][0] + M[r][1] * M[c][1] + M[r][2] * M[c][2]; };
+    o.s00 = dot(0, 0);
+    o.s01 = dot(0, 1);
+    o.s02 = dot(0, 2);
+    o.s11 = dot(1, 1);
+    o.s12 = dot(1, 2);
+    o.s22 = dot(2, 2);
+    o.trace = o.s00 + o.s11 + o.s22;
+}
+
 // The culling and projection of gpu_render.cu:93-135 (the rectangle in units of tile_w x tile_h
-// pixels; 16 x 16 is the reference's). Returns false when the Gaussian is culled.
-__device__ __forceinline__ bool project(const float4 pg, const float4 sg, const float4 q, const CamParams& cam,
-                                        int tile_w, int tile_h, Projected& o) {
+// pixels; 16 x 16 is the reference's), on the precomputed covariance. Returns false when the
+// Gaussian is culled.
+//
+// Before the exact screen test (which needs the 2D covariance, its eigenvalue and eight IEEE
+// divisions), a conservative one: lambda <= a + c + sqrt(0.1) <= ||T||_F^2 tr(S) + 0.6 + 0.317,
+// because tr(T S T^T) <= lambda_max(S) ||T||_F^2 <= tr(S) ||T||_F^2, evaluated with a rounded
+// reciprocal and widened (x1.001 under the root, +1 pixel for the ceiling, a relative margin on
+// the centre) so that it only culls what the exact test culls. NaN or infinite inputs never pass
+// it and fall through to the exact test.
+__device__ __forceinline__ bool project(const float4 pg, const Cov3& cov, const CamParams& cam, int tile_w, int tile_h,
+                                        Projected& o) {
     const float gx = pg.x, gy = pg.y, gz = pg.z;
     const float px = cam.R[0] * gx + cam.R[1] * gy + cam.R[2] * gz + cam.t[0];
     const float py = cam.R[3] * gx + cam.R[4] * gy + cam.R[5] * gz + cam.t[1];
     const float pz = cam.R[6] * gx + cam.R[7] * gy + cam.R[8] * gz + cam.t[2];
     if (pz < 0.2f) return false;
 
-    const float w = q.x, x = q.y, y = q.z, z = q.w;
-    const float Rq[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)},
-                            {2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)},
-                            {2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)}};
-    const float s[3] = {sg.x * cam.splatScale, sg.y * cam.splatScale, sg.z * cam.splatScale};
-    float M[3][3], S[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) M[r][c] = Rq[r][c] * s[c];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) S[r][c] = M[r][0] * M[c][0] + M[r][1] * M[c][1] + M[r][2] * M[c][2];
-
     const float limX = 1.3f * 0.5f * cam.width / cam.fx, limY = 1.3f * 0.5f * cam.height / cam.fy;
+    {
+        const float iz = __frcp_rn(pz);
+        const float ex = fminf(limX, fmaxf(-limX, px * iz)) * pz, ey = fminf(limY, fmaxf(-limY, py * iz)) * pz;
+        const float j00 = cam.fx * iz, j02 = -cam.fx * ex * iz * iz, j11 = cam.fy * iz, j12 = -cam.fy * ey * iz * iz;
+        float tn = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float t0 = j00 * cam.R[c] + j02 * cam.R[6 + c];
+            const float t1 = j11 * cam.R[3 + c] + j12 * cam.R[6 + c];
+            tn += t0 * t0 + t1 * t1;
+        }
+        const float rb = 3.0f * sqrtf((tn * cov.trace + 0.92f) * 1.001f) + 1.0f;
+        const float uu = cam.fx * px * iz + cam.cx, vv = cam.fy * py * iz + cam.cy;
+        const float du = 1e-5f * (fabsf(uu) + fabsf(cam.cx)) + 0.01f + rb;
+        const float dv = 1e-5f * (fabsf(vv) + fabsf(cam.cy)) + 0.01f + rb;
+        if (uu + du < 0.f || vv + dv < 0.f || uu - du >= cam.width || vv - dv >= cam.height) return false;
+    }
+
     const float tx = fminf(limX, fmaxf(-limX, px / pz)) * pz;
     const float ty = fminf(limY, fmaxf(-limY, py / pz)) * pz;
     const float J[2][3] = {{cam.fx / pz, 0, -cam.fx * tx / (pz * pz)}, {0, cam.fy / pz, -cam.fy * ty / (pz * pz)}};
@@ -96,7 +148,7 @@ __device__ __forceinline__ bool project(const float4 pg, const float4 sg, const 
 #pragma unroll
     for (int r = 0; r < 2; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) TS[r][c] = T[r][0] * S[0][c] + T[r][1] * S[1][c] + T[r][2] * S[2][c];
+        for (int c = 0; c < 3; ++c) TS[r][c] = T[r][0] * cov.at(0, c) + T[r][1] * cov.at(1, c) + T[r][2] * cov.at(2, c);
     const float a = TS[0][0] * T[0][0] + TS[0][1] * T[0][1] + TS[0][2] * T[0][2] + 0.3f;
     const float b = TS[0][0] * T[1][0] + TS[0][1] * T[1][1] + TS[0][2] * T[1][2];
     const float c = TS[1][0] * T[1][0] + TS[1][1] * T[1][1] + TS[1][2] * T[1][2] + 0.3f;
@@ -177,48 +229,48 @@ __global__ void __launch_bounds__(256, 3) preprocess_kernel(const BatchScene<Src
     if (i < sc.src.n) {
         float4 pg, sg, q;
         sc.src.load(i, pg, sg, q);
-        constexpr int planes = ((D + 1) * (D + 1) * 3 + 3) / 4;
-        float sh[planes * 4];
-        bool have_sh = false;
+        bool have_once = false;
+        float tau = 0.f, log2_opacity = 0.f;  // per Gaussian, once it is visible in some view
+        // The covariance once for all views (a view with another splat scale recomputes it).
+        Cov3 cov;
+        float cov_scale = nv > 0 ? s_cam[0].splatScale : 1.0f;
+        covariance(sg, q, cov_scale, cov);
         for (unsigned vk = 0; vk < nv; ++vk) {
             const CamParams& cam = vk < kMaxStagedViews ? s_cam[vk] : views[sc.view_begin + vk].cam;
             const unsigned e = views[sc.view_begin + vk].entry_base + static_cast<unsigned>(i);
+            if (cam.splatScale != cov_scale) {
+                cov_scale = cam.splatScale;
+                covariance(sg, q, cov_scale, cov);
+            }
             Projected p;
-            const bool vis = project(pg, sg, q, cam, tile_w, tile_h, p);
+            const bool vis = project(pg, cov, cam, tile_w, tile_h, p);
             if (kDebug) dbg.tiles_touched[e] = 0;
             if (!vis) {
                 depth_key[e] = kCulledKey;
                 continue;
             }
-            if (!have_sh) {
-#pragma unroll
-                for (int k = 0; k < planes; ++k) {
-                    const float4 f = sc.src.sh[i * sc.src.sh_planes + k];
-                    sh[4 * k + 0] = f.x;
-                    sh[4 * k + 1] = f.y;
-                    sh[4 * k + 2] = f.z;
-                    sh[4 * k + 3] = f.w;
-                }
-                have_sh = true;
+            if (!have_once) {
+                // alpha = min(0.99, opacity * exp(power)) >= 1/255 needs power >= -ln(255 opacity): a
+                // margin of 1% + 0.02 on that bound keeps the cut conservative under rounding. A NaN
+                // opacity gives alpha 0.99 everywhere (as fminf does in the reference), so no cut then.
+                tau = logf(255.0f * pg.w) * 1.01f + 0.02f;
+                if (isnan(tau)) tau = 3.0e38f;
+                log2_opacity = log2f(pg.w);
+                have_once = true;
             }
             // Colour along the unit direction from the camera centre (gpu_render.cu:137-139).
             float3 d = make_float3(pg.x - cam.eye[0], pg.y - cam.eye[1], pg.z - cam.eye[2]);
             const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-            const float3 rgb = sh_color<D>(sh, d.x / len, d.y / len, d.z / len);
+            const float3 rgb = sh_color<D>(sc.src.sh + i * sc.src.sh_planes, d.x / len, d.y / len, d.z / len);
 
             const float opacity = pg.w;
-            // alpha = min(0.99, opacity * exp(power)) >= 1/255 needs power >= -ln(255 opacity): a
-            // margin of 1% + 0.02 on that bound keeps the cut conservative under rounding. A NaN
-            // opacity gives alpha 0.99 everywhere (as fminf does in the reference), so no cut then.
-            float tau = logf(255.0f * opacity) * 1.01f + 0.02f;
-            if (isnan(tau)) tau = 3.0e38f;
             const unsigned bx = axis_bounds(p.u, p.a, tau, p.radius, cam.width);
             const unsigned by = axis_bounds(p.v, p.c, tau, p.radius, cam.height);
             constexpr float kHalfLog2e = -0.72134752044448170368f;  // -log2(e) / 2
             constexpr float kLog2e = -1.44269504088896340736f;      // -log2(e)
             SplatRecord r;
             r.r0 = make_float4(p.u, p.v, kHalfLog2e * p.conicA, kLog2e * p.conicB);
-            r.r1 = make_float4(kHalfLog2e * p.conicC, log2f(opacity), rgb.x, rgb.y);
+            r.r1 = make_float4(kHalfLog2e * p.conicC, log2_opacity, rgb.x, rgb.y);
             r.r2 = make_float4(rgb.z, __uint_as_float(bx), __uint_as_float(by), 0.f);
             rec[e] = r;
             rect16[e] = static_cast<unsigned long long>(p.x0) | (static_cast<unsigned long long>(p.y0) << 16) |

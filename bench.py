@@ -13,11 +13,13 @@ aniso_b200_render (the drop-in for GpuRenderer::render) into pinned host memory,
 device-to-host image copy is inside the timed region. Under torchrun each rank renders its own
 replica's 16 views (weak scaling, no collective); time is the max over ranks.
 
-Two more workloads of the same metric family ride along on rank 0 (skip with --no-extra):
+Three more workloads of the same metric family ride along on rank 0 (skip with --no-extra):
   "batched":  one 1M-Gaussian scene, 64 Fibonacci-sphere views of mixed resolution, rendered by one
               autotuned, graph-replayed batch versus 64 plain per-view launches (views/s);
   "fwd_bwd":  the 2.2M-Gaussian scene at 1280x720, forward + hand-written adjoint through the
-              torch.autograd.Function against an L2 loss (ms/view).
+              torch.autograd.Function against an L2 loss (ms/view);
+  "train_batch": 8 scenes (11.3M Gaussians), 32 views, one batched forward + adjoint versus the
+              views one by one (ms/view).
 """
 from __future__ import annotations
 
@@ -42,9 +44,9 @@ N_GAUSS = 740_000
 # the reference's published GPU forward on the 0.74M-Gaussian *train* scene at
 # 1280 wide, 2.3 ms/frame on an RTX 5090 (README.md:28) = 741,883 / 2.3 ms.
 PUBLISHED_GAUSSIANS_PER_S = 741_883 / 2.3e-3
-# dram__bytes_read.sum + dram__bytes_write.sum of one blend launch on ring view 0 (ncu, see
-# profiles/); None until captured.
-BLEND_TRAFFIC_BYTES = None
+# dram__bytes_read.sum + dram__bytes_write.sum of one blend launch on a ring view, from one ncu
+# capture (profiles/blend_740k_1280x720.md).
+BLEND_TRAFFIC_BYTES = 35_808_768
 
 
 def measured_peaks():
@@ -152,6 +154,10 @@ def reference_arm(args, rank):
                              "sample": "%d views of the 16 (one per step), reference render.cpp with "
                                        "std::thread::hardware_concurrency() threads" % args.steps},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        line["reference_gpu"] = reference_gpu_leg(gauss, sh, cams)
+    except Exception as e:  # no GPU in this arm's environment: the CPU figure stands alone
+        line["reference_gpu"] = {"unavailable": str(e).splitlines()[0][:200]}
     print(json.dumps(line), flush=True)
 
 
@@ -302,6 +308,97 @@ def fwd_bwd_leg(torch, steps: int):
             "grads_finite": finite, "target_ms": 3.0}
 
 
+def reference_gpu_leg(gauss, sh, cams, rounds: int = 2):
+    """Reference arm only: the reference's own GpuRenderer (gpu_render.cu with CUB, built for
+    sm_100a with --use_fast_math as its CMake ships it) on the same 16 views, the GPU bar. Its
+    RenderStats events cover preprocess + scan + the host read of the pair count, sort, blend; the
+    wall clock adds its device-to-host image copy."""
+    import oracle
+
+    if not oracle.ReferenceGPU.available(fast_math=True):
+        return {"unavailable": "oracle/_ref/libaniso_ref_gpu_fast.so not built (no reference sources)"}
+    ref = oracle.ReferenceGPU(fast_math=True)
+    h = ref.renderer(gauss, sh, 3)
+    try:
+        ref.render(h, cams[0])  # warm-up: grows its buffers
+        ev, frames = 0.0, 0
+        t = time.perf_counter()
+        for _ in range(rounds):
+            for cam in cams:
+                _, st = ref.render(h, cam)
+                ev += st["project_ms"] + st["sort_ms"] + st["blend_ms"]
+                frames += 1
+        wall = (time.perf_counter() - t) / frames
+    finally:
+        ref.destroy(h)
+    return {"impl": "reference aniso::GpuRenderer (src/gpu_render.cu, CUB scan + radix sort), sm_100a, fast-math",
+            "ms_per_frame_events": ev / frames, "ms_per_frame_wall": 1000 * wall,
+            "gaussians_per_s_events": N_GAUSS / (ev / frames / 1000.0), "frames": frames}
+
+
+def train_batch_leg(torch, steps: int):
+    """Workload 5: 8 scenes of uneven size (0.2M..3.0M), 4 views each (960x540 / 1280x720), random
+    N(0, 1) upstream gradients: one batched forward + adjoint for all 32 views versus the same
+    views one by one through the single-view autograd Function."""
+    from aniso_b200 import scenes
+    from aniso_b200.autograd import rasterize, rasterize_batch
+
+    raws, camsets = scenes.config(5)
+
+    def params(rw):
+        n = rw.n
+        sh = np.concatenate([rw.f_dc.reshape(n, 1, 3), rw.f_rest.reshape(n, 3, 15).transpose(0, 2, 1)], 1)
+        arrs = [rw.xyz, rw.scale, rw.rot, rw.opacity, np.ascontiguousarray(sh)]
+        return [torch.tensor(a, dtype=torch.float32, device="cuda", requires_grad=True) for a in arrs]
+
+    ps = [params(rw) for rw in raws]
+    cams = [c for cs in camsets for c in cs]
+    view_scene = [s for s, cs in enumerate(camsets) for _ in cs]
+    rng = np.random.default_rng(4)
+    ups = [torch.tensor(rng.standard_normal((c.height, c.width, 3)), dtype=torch.float32, device="cuda")
+           for c in cams]
+
+    def zero():
+        for group in ps:
+            for p in group:
+                p.grad = None
+
+    def batched():
+        zero()
+        imgs = rasterize_batch(ps, cams, view_scene)
+        torch.autograd.backward(imgs, ups)
+
+    def per_view():
+        zero()
+        for k, (c, s) in enumerate(zip(cams, view_scene)):
+            torch.autograd.backward([rasterize(*ps[s], c)], [ups[k]])
+
+    out = {}
+    for name, fn in (("batched", batched), ("per_view", per_view)):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / steps
+    grads_b = [p.grad.clone() for group in ps for p in group]  # from the last per-view run
+    batched()
+    same = all(torch.equal(a, p.grad) for a, p in zip(grads_b, [p for group in ps for p in group]))
+    V = len(cams)
+    return {"workload": "8 scenes of 0.2/0.4/0.7/1.0/1.5/2.0/2.5/3.0M Gaussians (SH3), 4 ring views each "
+                        "(960x540 and 1280x720 alternating), upstream dL/dimage ~ N(0,1), fp32",
+            "ms_per_view_batched": out["batched"] / V, "ms_per_view_per_view": out["per_view"] / V,
+            "speedup": out["per_view"] / out["batched"], "views": V,
+            "gaussians": sum(rw.n for rw in raws),
+            "grads_equal_per_view_sum": same,
+            "note": "batched gradients equal the per-view gradients summed in view order bit for bit; "
+                    "the per-view adjoint is checked against FP64 in tests/test_gradients.py"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -309,6 +406,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-extra", action="store_true", help="skip the batched and fwd+bwd workloads")
+    ap.add_argument("--only", choices=["batched", "fwd_bwd", "train_batch"], default=None,
+                    help="run one extra workload alone and print its JSON object (for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -322,6 +421,11 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
+    if args.only:
+        if rank == 0:
+            leg = {"batched": batched_leg, "fwd_bwd": fwd_bwd_leg, "train_batch": train_batch_leg}[args.only]
+            print(json.dumps({"leg": args.only, **leg(torch, args.steps)}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -425,6 +529,7 @@ def main():
         if not args.no_extra:
             extra["batched"] = batched_leg(torch, max(3, min(args.steps, 10)))
             extra["fwd_bwd"] = fwd_bwd_leg(torch, max(3, min(args.steps, 10)))
+            extra["train_batch"] = train_batch_leg(torch, 2)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "ms_per_frame": ms_step / V,

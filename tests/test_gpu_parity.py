@@ -263,3 +263,39 @@ def test_render_device_stream_ordered(ab, torch_cuda):
     r.sync()
     for h, o in zip(host, outs):
         np.testing.assert_array_equal(o.cpu().numpy(), h)
+
+
+@pytest.mark.slow
+def test_faster_than_the_reference_gpu_renderer(ab):
+    """The same 4 ring views of the 740k-Gaussian scene through the reference's GpuRenderer (its
+    own gpu_render.cu, CUB, built for sm_100a as shipped, with --use_fast_math) and through this
+    library's drop-in call, both host-to-host (each returns a host image): this one must be faster."""
+    import time
+
+    if not oracle.ReferenceGPU.available(fast_math=True):
+        pytest.skip("reference GPU library not built")
+    raws, camsets = scenes.config(2)
+    g, sh = scenes.activate(raws[0])
+    cams = camsets[0][:4]
+    ref = oracle.ReferenceGPU(fast_math=True)
+    h = ref.renderer(g, sh, 3)
+    r = ab.GpuRenderer(g, sh, 3)
+    try:
+        for c in cams:  # warm-up: both grow their buffers
+            ref.render(h, c)
+            r.render(c)
+        t = time.perf_counter()
+        for _ in range(3):
+            for c in cams:
+                ref.render(h, c)
+        t_ref = (time.perf_counter() - t) / (3 * len(cams))
+        t = time.perf_counter()
+        for _ in range(3):
+            for c in cams:
+                r.render(c)
+        t_ours = (time.perf_counter() - t) / (3 * len(cams))
+    finally:
+        ref.destroy(h)
+    print("host-to-host ms/frame: reference GpuRenderer %.3f, aniso_b200 %.3f (%.2fx)"
+          % (1e3 * t_ref, 1e3 * t_ours, t_ref / t_ours))
+    assert t_ours < t_ref
