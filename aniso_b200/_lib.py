@@ -46,6 +46,7 @@ EXPORTS = [
     "aniso_b200_train_batch_forward",
     "aniso_b200_train_batch_backward",
     "aniso_b200_sort_projection_noalloc",
+    "aniso_b200_scene_load_ply",
 ]
 
 
@@ -97,6 +98,7 @@ def _load():
         "aniso_b200_scene_create": [P, P, I64, I32, ctypes.POINTER(P)],
         "aniso_b200_scene_create_raw": [P, P, P, P, P, P, I64, I32, ctypes.POINTER(P)],
         "aniso_b200_scene_destroy": [P],
+        "aniso_b200_scene_load_ply": [ctypes.c_char_p, ctypes.POINTER(P)],
         "aniso_b200_render": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, ctypes.POINTER(Stats)],
         "aniso_b200_render_device": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, P],
         "aniso_b200_sync": [P, ctypes.POINTER(Stats)],

@@ -541,6 +541,124 @@ __global__ void ingest_raw_kernel(const float* __restrict__ xyz, const float* __
     }
 }
 
+// Where each needed value sits in a PLY vertex row (float columns, in file order).
+struct PlyColumns {
+    int stride;                  // floats per row
+    int x, y, z, opacity;
+    int scale[3], rot[4], dc[3];
+    int rest[72];                // f_rest_0.. (channel-major), 3((d+1)^2 - 1) of them, d <= 4
+};
+
+// ply_loader.cpp:113-134 on the device, straight from the file's vertex block (one row of `stride`
+// floats per Gaussian): position, exp(scale), sigmoid(opacity), the normalised quaternion, and
+// f_dc / f_rest reordered to [coefficient][channel]; packed into the 16-byte SoA words.
+__global__ void ingest_ply_kernel(const float* __restrict__ body, int64_t n, PlyColumns col, int coeffs, int planes,
+                                  float4* __restrict__ pos_op, float4* __restrict__ scale, float4* __restrict__ rot,
+                                  float4* __restrict__ sh) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* v = body + i * col.stride;
+    pos_op[i] = make_float4(v[col.x], v[col.y], v[col.z], 1.0f / (1.0f + expf(-v[col.opacity])));
+    scale[i] = make_float4(expf(v[col.scale[0]]), expf(v[col.scale[1]]), expf(v[col.scale[2]]), 0.f);
+    const float qw = v[col.rot[0]], qx = v[col.rot[1]], qy = v[col.rot[2]], qz = v[col.rot[3]];
+    const float nrm = sqrtf(qw * qw + qx * qx + qy * qy + qz * qz);
+    rot[i] = nrm > 0 ? make_float4(qw / nrm, qx / nrm, qy / nrm, qz / nrm) : make_float4(1.f, 0.f, 0.f, 0.f);
+    const int k3 = coeffs * 3, rest = coeffs - 1;
+    for (int p = 0; p < planes; ++p) {
+        float w[4];
+        for (int e = 0; e < 4; ++e) {
+            const int f = 4 * p + e;  // float index in [coefficient][channel] order
+            if (f >= k3) {
+                w[e] = 0.f;
+                continue;
+            }
+            const int k = f / 3, c = f % 3;
+            w[e] = k == 0 ? v[col.dc[c]] : v[col.rest[c * rest + (k - 1)]];
+        }
+        sh[i * planes + p] = make_float4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// The header rules and messages of ply_loader.cpp:20-65 and 77-104: binary little-endian, one
+// vertex element of float properties (others must be empty), the named columns present, the
+// f_rest count matching a degree 0..4.
+int parse_ply_header(FILE* f, const std::string& name, int64_t* count, PlyColumns* col, int* degree, long* body) {
+    char line[512];
+    if (!std::fgets(line, sizeof line, f) || std::strncmp(line, "ply", 3) != 0)
+        return fail(ANISO_B200_ERR_ARGUMENT, name + ": not a PLY file");
+    bool in_vertex = false, saw_format = false;
+    int64_t n = 0;
+    std::vector<std::string> props;
+    while (std::fgets(line, sizeof line, f)) {
+        std::string l(line);
+        while (!l.empty() && (l.back() == '\n' || l.back() == '\r')) l.pop_back();
+        char w0[64] = {0}, w1[128] = {0}, w2[128] = {0};
+        const int got = std::sscanf(l.c_str(), "%63s %127s %127s", w0, w1, w2);
+        if (got < 1) continue;
+        const std::string word = w0;
+        if (word == "format") {
+            if (std::string(w1) != "binary_little_endian")
+                return fail(ANISO_B200_ERR_ARGUMENT,
+                            name + ": only binary_little_endian PLY is supported, got " + std::string(w1));
+            saw_format = true;
+        } else if (word == "element") {
+            const long long c = got >= 3 ? std::atoll(w2) : 0;
+            in_vertex = std::string(w1) == "vertex";
+            if (in_vertex) n = c;
+            else if (c != 0) return fail(ANISO_B200_ERR_ARGUMENT, name + ": unexpected element '" + std::string(w1) + "'");
+        } else if (word == "property") {
+            if (!in_vertex) continue;
+            const std::string type = w1;
+            if (type != "float" && type != "float32")
+                return fail(ANISO_B200_ERR_ARGUMENT,
+                            name + ": property '" + std::string(w2) + "' has type " + type + ", expected float");
+            props.push_back(w2);
+        } else if (word == "end_header") {
+            if (!saw_format) return fail(ANISO_B200_ERR_ARGUMENT, name + ": missing format line");
+            *body = std::ftell(f);
+            const auto find = [&](const std::string& p, int* out) {
+                for (size_t k = 0; k < props.size(); ++k)
+                    if (props[k] == p) {
+                        *out = static_cast<int>(k);
+                        return 0;
+                    }
+                return fail(ANISO_B200_ERR_ARGUMENT, name + ": missing property '" + p + "'");
+            };
+            col->stride = static_cast<int>(props.size());
+            AB_TRY(find("x", &col->x));
+            AB_TRY(find("y", &col->y));
+            AB_TRY(find("z", &col->z));
+            AB_TRY(find("opacity", &col->opacity));
+            for (int k = 0; k < 3; ++k) AB_TRY(find("scale_" + std::to_string(k), &col->scale[k]));
+            for (int k = 0; k < 4; ++k) AB_TRY(find("rot_" + std::to_string(k), &col->rot[k]));
+            for (int k = 0; k < 3; ++k) AB_TRY(find("f_dc_" + std::to_string(k), &col->dc[k]));
+            int rest = 0;
+            while (rest < 72) {
+                int c = -1;
+                const std::string p = "f_rest_" + std::to_string(rest);
+                bool found = false;
+                for (size_t k = 0; k < props.size(); ++k)
+                    if (props[k] == p) {
+                        c = static_cast<int>(k);
+                        found = true;
+                        break;
+                    }
+                if (!found) break;
+                col->rest[rest++] = c;
+            }
+            *degree = -1;
+            for (int d = 0; d <= 4; ++d)
+                if (rest == 3 * ((d + 1) * (d + 1) - 1)) *degree = d;
+            if (*degree < 0)
+                return fail(ANISO_B200_ERR_ARGUMENT,
+                            name + ": " + std::to_string(rest) + " f_rest properties do not match any SH degree");
+            *count = n;
+            return 0;
+        }
+    }
+    return fail(ANISO_B200_ERR_ARGUMENT, name + ": header has no end_header");
+}
+
 // Scenes may store up to degree 4 (the degrees the reference loader accepts, ply_loader.cpp:67-73);
 // colour is evaluated up to degree 3, as both reference renderers do.
 int validate_degree(int d) {
@@ -693,6 +811,52 @@ int aniso_b200_scene_create_raw(const float* xyz, const float* f_dc, const float
     if (rc != 0) {
         delete s;
         if (out) *out = nullptr;
+        return rc;
+    }
+    *out = s;
+    return ANISO_B200_OK;
+}
+
+int aniso_b200_scene_load_ply(const char* path, aniso_b200_scene** out) {
+    if (!path || !out) return fail(ANISO_B200_ERR_ARGUMENT, "path/out is NULL");
+    const std::string name = path;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(ANISO_B200_ERR_ARGUMENT, name + ": cannot open");
+    int64_t n = 0;
+    int degree = 0;
+    long body_at = 0;
+    PlyColumns col{};
+    int rc = parse_ply_header(f, name, &n, &col, &degree, &body_at);
+    std::vector<float> body;
+    if (rc == 0) {
+        body.resize(static_cast<size_t>(n) * col.stride);
+        std::fseek(f, body_at, SEEK_SET);
+        const size_t got = body.empty() ? 0 : std::fread(body.data(), sizeof(float), body.size(), f);
+        if (got != body.size())
+            rc = fail(ANISO_B200_ERR_ARGUMENT, name + ": file is shorter than the header promises (" +
+                                                   std::to_string(n) + " Gaussians)");
+    }
+    std::fclose(f);
+    if (rc != 0) return rc;
+    aniso_b200_scene* s = nullptr;
+    rc = new_scene(n, degree, out, &s);
+    if (rc == 0 && n > 0) {
+        float* d = nullptr;
+        cudaError_t e = cudaMalloc(&d, body.size() * sizeof(float));
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d, body.data(), body.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess) {
+            ingest_ply_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s->stream>>>(
+                d, n, col, (degree + 1) * (degree + 1), s->planes, s->pos_op.p, s->scale.p, s->rot.p, s->sh.p);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (d) cudaFree(d);
+        if (e != cudaSuccess) rc = cuda_fail(e, "scene upload");
+    }
+    if (rc != 0) {
+        delete s;
+        *out = nullptr;
         return rc;
     }
     *out = s;

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
+import os
 
 import numpy as np
 
@@ -40,6 +41,22 @@ def c_camera(cam) -> _lib.Camera:
     c.fx, c.fy, c.cx, c.cy = float(cam.fx), float(cam.fy), float(cam.cx), float(cam.cy)
     c.width, c.height = int(cam.width), int(cam.height)
     return c
+
+
+def _ply_shape(path):
+    """(Gaussians, SH degree) from a PLY header (the library has already validated it)."""
+    n, rest = 0, 0
+    with open(path, "rb") as f:
+        for raw in f:
+            line = raw.decode("ascii", "replace").strip()
+            if line.startswith("element vertex"):
+                n = int(line.split()[2])
+            elif line.startswith("property") and line.split()[-1].startswith("f_rest_"):
+                rest += 1
+            elif line == "end_header":
+                break
+    deg = {0: 0, 9: 1, 24: 2, 45: 3, 72: 4}[rest]
+    return n, deg
 
 
 def _ptr(a: np.ndarray):
@@ -77,6 +94,17 @@ class GpuRenderer:
                                               raw.sh_degree, ctypes.byref(self._h)))
         self.n = raw.n
         self.sh_degree = raw.sh_degree
+        return self
+
+    @classmethod
+    def from_ply(cls, path) -> "GpuRenderer":
+        """Loads a 3DGS PLY like aniso::loadPly, with the de-interleave and activation on the device."""
+        self = cls.__new__(cls)
+        self._h = ctypes.c_void_p()
+        check(lib.aniso_b200_scene_load_ply(os.fsencode(path), ctypes.byref(self._h)))
+        n, deg = _ply_shape(path)
+        self.n = n
+        self.sh_degree = deg
         return self
 
     @staticmethod

@@ -357,3 +357,75 @@ def read_colmap_text(folder):
         cams.append(Camera(width, height, fx, fy, cx, cy, R, t, w[9]))
     cams.sort(key=lambda c: c.name)
     return cams
+
+
+# COLMAP model ids and their parameter counts (COLMAP's models.h; the table of camera.cpp:57-60).
+_COLMAP_PARAMS = [3, 4, 4, 5, 8, 8, 12, 5, 4, 5, 12]
+
+
+def _quat_to_matrix(qw, qx, qy, qz):
+    """camera.cpp:95-101: normalise in double, then the rotation matrix of the unit quaternion."""
+    nrm = np.sqrt(qw * qw + qx * qx + qy * qy + qz * qz)
+    w, x, y, z = qw / nrm, qx / nrm, qy / nrm, qz / nrm
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                     [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                     [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+
+
+def read_colmap_binary(folder):
+    """cameras.bin / images.bin as aniso::loadColmapCameras reads them (camera.cpp:61-140): PINHOLE
+    and SIMPLE_PINHOLE only, each image's 2D points skipped, Cameras sorted by image name."""
+    def take(f, fmt):
+        size = struct.calcsize(fmt)
+        b = f.read(size)
+        if len(b) != size:
+            raise ValueError("%s: truncated" % f.name)
+        return struct.unpack(fmt, b)
+
+    intr = {}
+    with open(os.path.join(folder, "cameras.bin"), "rb") as f:
+        (count,) = take(f, "<Q")
+        for _ in range(count):
+            cid, model, width, height = take(f, "<IiQQ")
+            if model < 0 or model >= len(_COLMAP_PARAMS):
+                raise ValueError("%s: unknown camera model %d" % (f.name, model))
+            p = take(f, "<%dd" % _COLMAP_PARAMS[model])
+            if model == 0:
+                intr[cid] = (width, height, p[0], p[0], p[1], p[2])
+            elif model == 1:
+                intr[cid] = (width, height, p[0], p[1], p[2], p[3])
+            else:
+                raise ValueError("%s: camera model %d has lens distortion; undistort the images first"
+                                 % (f.name, model))
+    cams = []
+    with open(os.path.join(folder, "images.bin"), "rb") as f:
+        (count,) = take(f, "<Q")
+        for _ in range(count):
+            take(f, "<I")
+            q = take(f, "<4d")
+            t = np.array(take(f, "<3d"))
+            (cid,) = take(f, "<I")
+            name = bytearray()
+            while True:
+                ch = f.read(1)
+                if not ch:
+                    raise ValueError("%s: truncated" % f.name)
+                if ch == b"\0":
+                    break
+                name += ch
+            (points,) = take(f, "<Q")
+            f.seek(points * 24, os.SEEK_CUR)
+            if cid not in intr:
+                raise ValueError("%s: image %s refers to a missing camera" % (f.name, name.decode()))
+            width, height, fx, fy, cx, cy = intr[cid]
+            cams.append(Camera(width, height, fx, fy, cx, cy, _quat_to_matrix(*q), t, name.decode()))
+    cams.sort(key=lambda c: c.name)
+    return cams
+
+
+def read_colmap(folder):
+    """A COLMAP sparse model in either form: the binary one when cameras.bin is there (what the
+    reference reads), else the text one (what the workload descriptions are written in)."""
+    if os.path.exists(os.path.join(folder, "cameras.bin")):
+        return read_colmap_binary(folder)
+    return read_colmap_text(folder)

@@ -77,6 +77,14 @@ int aniso_b200_scene_create_raw(const float* xyz, const float* f_dc, const float
                                 aniso_b200_scene** out);
 
 /* ~GpuRenderer (gpu_render.cu:294-297). Accepts NULL. */
+/* aniso::loadPly (ply_loader.cpp:77-141) followed by the GpuRenderer constructor, with the work on
+ * the device: the header is parsed on the host with the reference loader's rules and messages,
+ * the vertex block is uploaded as stored (rows of float properties, any order, unknown properties
+ * ignored), and one kernel de-interleaves, activates (exp, sigmoid, normalise) and reorders the SH
+ * into the scene's layout. The scene's SH degree is the file's (0..4). The device exp may differ
+ * from the host loader's std::exp in the last bit of an activated value. */
+int aniso_b200_scene_load_ply(const char* path, aniso_b200_scene** out);
+
 int aniso_b200_scene_destroy(aniso_b200_scene* scene);
 
 /* GpuRenderer::render(const Camera&, RenderStats*, const RenderOptions&) (gpu_render.h:30,

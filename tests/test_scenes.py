@@ -70,3 +70,31 @@ def test_workload_shapes(k, views):
     if k == 4:
         assert {(c.width, c.height) for c in cams[0]} <= set(scenes.RESOLUTIONS_4)
         assert all(abs(c.fx - 0.9 * c.width) < 1e-9 for c in cams[0])
+
+
+def test_colmap_binary_reader_equals_reference_loader(tmp_path, reference_cpu):
+    cams = scenes.fibonacci_cameras(9, 10.0, scenes.RESOLUTIONS_4, seed=3)
+    d = str(tmp_path / "sparse")
+    scenes.write_colmap(d, cams)
+    ours = scenes.read_colmap_binary(d)
+    ref = reference_cpu.load_colmap(d)
+    assert len(ours) == len(ref) == 9
+    assert [c.name for c in ours] == sorted(c.name for c in cams)
+    for a, row in zip(ours, ref):  # rows: width height fx fy cx cy R(9) t(3), sorted by image name
+        assert (a.width, a.height) == (row[0], row[1])
+        assert (a.fx, a.fy, a.cx, a.cy) == tuple(row[2:6])
+        np.testing.assert_array_equal(np.asarray(a.R), row[6:15].reshape(3, 3))  # same double arithmetic
+        np.testing.assert_array_equal(np.asarray(a.t), row[15:18])
+
+
+def test_read_colmap_picks_either_form(tmp_path):
+    cams = scenes.ring_cameras(5, 8.0, 640, 360, 500.0)
+    for binary, text in ((True, False), (False, True)):
+        d = str(tmp_path / ("b" if binary else "t"))
+        scenes.write_colmap(d, cams, binary=binary, text=text)
+        got = scenes.read_colmap(d)
+        assert [c.name for c in got] == sorted(c.name for c in cams)
+        for a in got:
+            b = next(c for c in cams if c.name == a.name)
+            np.testing.assert_allclose(np.asarray(a.R), np.asarray(b.R), atol=1e-12)
+            np.testing.assert_allclose(np.asarray(a.t), np.asarray(b.t), atol=1e-12)
