@@ -62,7 +62,8 @@ class Options(ctypes.Structure):
 
 class BatchOptions(ctypes.Structure):
     _fields_ = [("sh_degree", ctypes.c_int32), ("splat_scale", ctypes.c_float), ("tile_w", ctypes.c_int32),
-                ("tile_h", ctypes.c_int32), ("blend_batch", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
+                ("tile_h", ctypes.c_int32), ("blend_batch", ctypes.c_int32), ("use_graph", ctypes.c_int32),
+                ("radix_bits", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):

@@ -1,11 +1,11 @@
 """Launch-shape autotuner for batched rendering.
 
 For a batch (its scenes and its cameras), times every candidate launch shape -- tile shape
-(8x8, 16x16, 16x32), blend batch (128, 256 splats staged per round) -- with the batch's own CUDA
-graph, keeps the fastest, and caches the choice in a JSON file keyed by the GPU name and a
+(8x8, 16x16, 16x32), blend batch (128, 256 splats staged per round), radix digit width of the
+sort (8 or 9 bits) -- with the batch's own CUDA graph, keeps the fastest, and caches the choice in a JSON file keyed by the GPU name and a
 signature of the workload (Gaussian counts, view count, resolutions). Every candidate renders the
-same image (the tile shape only changes how pixels are grouped), so the choice is a pure speed
-decision; the tuner checks that the candidates agree on one view before it trusts them.
+same image (the tile shape only changes how pixels are grouped, the digit width how many passes the
+sort takes), so the choice is a pure speed decision; the tuner checks that the candidates agree on one view before it trusts them.
 
     best = tune(scenes, view_scene, cameras)            # -> BatchOptions
     batch = BatchRenderer(scenes, view_scene, best)
@@ -22,6 +22,7 @@ from .renderer import BatchOptions, BatchRenderer
 
 TILES = [(8, 8), (16, 16), (16, 32)]
 BLEND_BATCHES = [128, 256]
+RADIX_BITS = [8, 9]
 CACHE_PATH = os.path.join(os.path.expanduser("~"), ".cache", "aniso_b200", "autotune.json")
 
 
@@ -85,7 +86,8 @@ def tune(scenes, view_scene, cameras, sh_degree: int = 3, splat_scale: float = 1
     cache = _load_cache(cache_path) if cache_path else {}
     if not force and key in cache:
         c = cache[key]
-        return BatchOptions(sh_degree, splat_scale, tuple(c["tile"]), int(c["blend_batch"]), use_graph)
+        return BatchOptions(sh_degree, splat_scale, tuple(c["tile"]), int(c["blend_batch"]), use_graph,
+                            int(c.get("radix_bits", 8)))
 
     outs = [torch.empty((c.height, c.width, 3), dtype=torch.uint8, device="cuda") for c in cameras]
     ptrs = [o.data_ptr() for o in outs]
@@ -94,23 +96,26 @@ def tune(scenes, view_scene, cameras, sh_degree: int = 3, splat_scale: float = 1
     probe = None
     for tile in TILES:
         for bb in BLEND_BATCHES:
-            opt = BatchOptions(sh_degree, splat_scale, tile, bb, use_graph)
-            b = BatchRenderer(scenes, view_scene, opt)
-            ms = time_batch(b, cameras, ptrs, stream)
-            img = outs[0].cpu().numpy()
-            if probe is None:
-                probe = img
-            elif not np.array_equal(img, probe):
-                raise RuntimeError("launch shapes disagree on the image (tile %s, batch %d)" % (tile, bb))
-            results.append({"tile": list(tile), "blend_batch": bb, "ms": ms})
-            b.close()
+            for bits in RADIX_BITS:
+                opt = BatchOptions(sh_degree, splat_scale, tile, bb, use_graph, bits)
+                b = BatchRenderer(scenes, view_scene, opt)
+                ms = time_batch(b, cameras, ptrs, stream)
+                img = outs[0].cpu().numpy()
+                if probe is None:
+                    probe = img
+                elif not np.array_equal(img, probe):
+                    raise RuntimeError("launch shapes disagree on the image (tile %s, batch %d, %d-bit digits)"
+                                       % (tile, bb, bits))
+                results.append({"tile": list(tile), "blend_batch": bb, "radix_bits": bits, "ms": ms})
+                b.close()
     best = min(results, key=lambda r: r["ms"])
     if report is not None:
         report.extend(results)
     if cache_path:
         cache[key] = dict(best, candidates=results)
         _store_cache(cache_path, cache)
-    return BatchOptions(sh_degree, splat_scale, tuple(best["tile"]), int(best["blend_batch"]), use_graph)
+    return BatchOptions(sh_degree, splat_scale, tuple(best["tile"]), int(best["blend_batch"]), use_graph,
+                        int(best["radix_bits"]))
 
 
-__all__ = ["tune", "time_batch", "signature", "TILES", "BLEND_BATCHES", "CACHE_PATH"]
+__all__ = ["tune", "time_batch", "signature", "TILES", "BLEND_BATCHES", "RADIX_BITS", "CACHE_PATH"]

@@ -104,9 +104,6 @@ struct Arena {
     DevBuf<unsigned> sort_scratch;          // per-span digit counts of the pass in flight
     DevBuf<unsigned long long> span_sum;    // pairs per span of the pair-offset scan
 
-    // The vis_idx buffer that holds the depth-sorted visible list after the depth passes.
-    static int sorted_buf() { return (kMaxPasses - 1) & 1; }
-
     int init(int64_t count, unsigned cap) {
         n = count;
         const size_t nn = static_cast<size_t>(std::max<int64_t>(count, 1));
@@ -151,26 +148,27 @@ struct Arena {
 // expansion, tile passes over `tiles` global tiles, and ranges. *final_buf = the pair buffer that
 // holds the sorted pairs. keep_rank: also record each visible entry's depth-sorted position (the
 // adjoint reads it).
-int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank,
+int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank, int bits,
                  cudaStream_t st, int* final_buf) {
     Ctrl* ctrl = A.ctrl.p;
     const unsigned cap = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
-    for (int p = 0; p < kMaxPasses; ++p) {
+    const int depth_passes = (32 + bits - 1) / bits;  // 4 for 8- and 9-bit digits
+    for (int p = 0; p < depth_passes; ++p) {
         const int src = (p + 1) & 1, dst = p & 1;  // pass 0 reads depth_key and writes buffer 0
         launch_radix_pass(p == 0 ? A.depth_key.p : A.vis_key[src].p, p == 0 ? nullptr : A.vis_idx[src].p,
-                          p == kMaxPasses - 1 ? nullptr : A.vis_key[dst].p, A.vis_idx[dst].p, p == 0,
-                          p == 0 ? SortCount::kFixed : SortCount::kVisible, entries, p == 0 ? entries : cap,
-                          p * kRadixBits, A.sort_scratch.p, ctrl, st);
+                          p == depth_passes - 1 ? nullptr : A.vis_key[dst].p, A.vis_idx[dst].p, p == 0,
+                          p == 0 ? SortCount::kFixed : SortCount::kVisible, entries, p == 0 ? entries : cap, p * bits,
+                          bits, A.sort_scratch.p, ctrl, st);
     }
-    const int sorted = Arena::sorted_buf();
-    const int tile_passes = std::max(1, (bits_for(tiles - 1) + kRadixBits - 1) / kRadixBits);
+    const int sorted = (depth_passes - 1) & 1;
+    const int tile_passes = std::max(1, (bits_for(tiles - 1) + bits - 1) / bits);
     const DupBuffers dup{A.offs.p, keep_rank ? A.rank.p : nullptr, A.rect_sorted.p, A.chunk_start.p, A.span_sum.p};
     launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, dup, A.pair_key[0].p,
                      A.pair_val[0].p, st);
     for (int p = 0; p < tile_passes; ++p) {
         const int src = p & 1, dst = src ^ 1;
         launch_radix_pass(A.pair_key[src].p, A.pair_val[src].p, A.pair_key[dst].p, A.pair_val[dst].p, false,
-                          SortCount::kPairs, 0u, A.pair_cap, p * kRadixBits, A.sort_scratch.p, ctrl, st);
+                          SortCount::kPairs, 0u, A.pair_cap, p * bits, bits, A.sort_scratch.p, ctrl, st);
     }
     const int fin = tile_passes & 1;
     AB_TRY(A.ranges.reserve(tiles));
@@ -214,7 +212,7 @@ int pack_camera(int scene_degree, int rendered_degree, const aniso_b200_camera* 
 // ---- plans ---------------------------------------------------------------------------------
 
 struct PlanShape {
-    int tile_w = kTile, tile_h = kTile, blend_batch = 256, sh_degree = 3;
+    int tile_w = kTile, tile_h = kTile, blend_batch = 256, sh_degree = 3, radix_bits = kRadixBits;
     float splat_scale = 1.0f;
 };
 
@@ -225,7 +223,9 @@ int check_options(const aniso_b200_batch_options* o, PlanShape& shape) {
     shape.tile_w = o->tile_w ? o->tile_w : kTile;
     shape.tile_h = o->tile_h ? o->tile_h : kTile;
     shape.blend_batch = o->blend_batch ? o->blend_batch : 256;
+    shape.radix_bits = o->radix_bits ? o->radix_bits : kRadixBits;
     if (shape.sh_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
+    if (!radix_bits_supported(shape.radix_bits)) return fail(ANISO_B200_ERR_ARGUMENT, "radix_bits must be 8 or 9");
     if (!blend_shape_supported(shape.tile_w, shape.tile_h))
         return fail(ANISO_B200_ERR_ARGUMENT, "tile shape must be 8x8, 16x16 or 16x32");
     return 0;
@@ -302,7 +302,8 @@ struct Plan {
             if (views[k].cam.width != o.views[k].cam.width || views[k].cam.height != o.views[k].cam.height)
                 return false;
         return shape.tile_w == o.shape.tile_w && shape.tile_h == o.shape.tile_h &&
-               shape.blend_batch == o.shape.blend_batch && rendered_degree() == o.rendered_degree();
+               shape.blend_batch == o.shape.blend_batch && shape.radix_bits == o.shape.radix_bits &&
+               rendered_degree() == o.rendered_degree();
     }
 };
 
@@ -395,7 +396,8 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     launch_preprocess_any(scenes, P, views, A, dbg, st);
     if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
     int fin = 0;
-    AB_TRY(enqueue_sort(A, static_cast<unsigned>(P.entries), static_cast<unsigned>(P.tiles), tables, train, st, &fin));
+    AB_TRY(enqueue_sort(A, static_cast<unsigned>(P.entries), static_cast<unsigned>(P.tiles), tables, train,
+                        P.shape.radix_bits, st, &fin));
     if (ev) AB_CUDA(cudaEventRecord(ev[2], st));
     if (!stop_after_sort)
         launch_blend(static_cast<unsigned>(P.tiles), A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, views, tables,
@@ -1068,7 +1070,7 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.depth_key.p, A.rect16.p, st);
     int fin = 0;
     const unsigned T = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
-    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, st, &fin));
+    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, kRadixBits, st, &fin));
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaDeviceSynchronize());
     Ctrl h;

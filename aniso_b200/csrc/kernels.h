@@ -37,15 +37,16 @@ void launch_preprocess_raw(const BatchScene<RawParams>* scenes, unsigned n_scene
 // publishes, or the frame's pair total.
 enum class SortCount : int { kFixed = 0, kVisible = 1, kPairs = 2 };
 
-// One stable LSD radix pass over (key, value) u32 pairs, 8-bit digit at `shift` (three launches:
-// upsweep, per-digit span scan, downsweep). masked: the input is the N depth keys in entry order,
+// One stable LSD radix pass over (key, value) u32 pairs, a `bits`-bit digit (8 or 9) at `shift`
+// (three launches: upsweep, per-digit span scan, downsweep). masked: the input is the N depth keys in entry order,
 // culled ones dropped, the entry index as value (the first depth pass; it publishes the visible
 // count); keys_out may be NULL on the last pass. Grids are sized for `capacity` (`fixed` for
 // kFixed) items. scratch holds sort_scratch_words() words.
 size_t sort_scratch_words();
+bool radix_bits_supported(int bits);
 void launch_radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
-                       bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned* scratch,
-                       Ctrl* ctrl, cudaStream_t stream);
+                       bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, int bits,
+                       unsigned* scratch, Ctrl* ctrl, cudaStream_t stream);
 
 // Expands the depth-sorted visible list into (tile, entry) pairs in depth order; sets kFlagOverflow
 // (and writes no pairs) if they exceed capacity. Three kernels: per-span pair counts, pair offsets,

@@ -31,7 +31,7 @@ using namespace ab2;
 
 constexpr size_t kG = ANISO_B200_NOALLOC_MAX_GAUSSIANS;
 constexpr size_t kP = ANISO_B200_NOALLOC_MAX_PAIRS;
-constexpr size_t kScratchWords = 256 * 600 + 256;  // >= sort_scratch_words(), checked at setup
+constexpr size_t kScratchWords = 512 * 600;         // >= sort_scratch_words(), checked at setup
 constexpr size_t kSpanSums = 600;                    // >= sort_span_sums(), checked at setup
 constexpr size_t kChunkWords = kP / 1024 + 2;        // >= kP / expand_chunk_pairs() + 2, checked
 
@@ -166,8 +166,8 @@ extern "C" int aniso_b200_sort_projection_noalloc(int64_t n, const uint32_t* til
         const int src = (p + 1) & 1, dst = p & 1;
         launch_radix_pass(p == 0 ? depth_key : vis_key[src], p == 0 ? nullptr : vis_idx[src],
                           p == kMaxPasses - 1 ? nullptr : vis_key[dst], vis_idx[dst], p == 0,
-                          p == 0 ? SortCount::kFixed : SortCount::kVisible, un, un, p * kRadixBits, sort_scratch, ctrl,
-                          st);
+                          p == 0 ? SortCount::kFixed : SortCount::kVisible, un, un, p * kRadixBits, kRadixBits,
+                          sort_scratch, ctrl, st);
     }
     const BatchTables tab{tables, tables + 1, tables + 2, 1u};
     launch_duplicate(vis_idx[(kMaxPasses - 1) & 1], rect16, ctrl, cap, un, tab, dup, pair_key[0], pair_val[0], st);
@@ -176,7 +176,7 @@ extern "C" int aniso_b200_sort_projection_noalloc(int64_t n, const uint32_t* til
         const bool last = p == passes - 1;
         launch_radix_pass(pair_key[p & 1], pair_val[p & 1], last ? tiles : pair_key[(p + 1) & 1],
                           last ? values : pair_val[(p + 1) & 1], false, SortCount::kPairs, 0u, cap, p * kRadixBits,
-                          sort_scratch, ctrl, st);
+                          kRadixBits, sort_scratch, ctrl, st);
     }
     cudaError_t e = cudaMemsetAsync(ranges, 0, static_cast<size_t>(T) * 2 * sizeof(uint32_t), st);
     if (e == cudaSuccess) {

@@ -36,6 +36,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kItems = 8;
 constexpr int kBlockItems = kThreads * kItems;  // items one CTA ranks at a time
 constexpr int kMaxSpans = 4 * 148;
+constexpr int kMaxRadixBits = 9;  // digit widths: 8 or 9 bits
 constexpr int kScanItems = 4;
 constexpr int kScanBlock = kThreads * kScanItems;
 constexpr int kExpandItems = 8;
@@ -73,8 +74,8 @@ __device__ __forceinline__ void span_blocks(unsigned n, unsigned spans, unsigned
 }
 
 // Loads block t: lane `lane` of warp `warp` holds items base + warp*kItems*32 + k*32 + lane, so
-// (k, lane) order within a warp is ascending position. dg = the digit, or kRadix for no item.
-template <bool kMasked, bool kVals>
+// (k, lane) order within a warp is ascending position. dg = the digit (R digits), or R for no item.
+template <int R, bool kMasked, bool kVals>
 __device__ __forceinline__ void load_block(const unsigned* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
                                            unsigned t, unsigned n, int shift, int warp, int lane, unsigned (&key)[kItems],
                                            unsigned (&val)[kItems], unsigned (&dg)[kItems]) {
@@ -90,39 +91,43 @@ __device__ __forceinline__ void load_block(const unsigned* __restrict__ keys_in,
         } else if (kVals) {
             val[k] = valid ? vals_in[idx] : 0u;
         }
-        dg[k] = valid ? ((key[k] >> shift) & (kRadix - 1)) : kRadix;
+        dg[k] = valid ? ((key[k] >> shift) & (R - 1)) : R;
     }
 }
 
 // Digit counts of each span: counts[d * spans + b]. Counting needs no ranks, so each warp adds
 // into its own shared histogram with plain atomics (lanes of one warp that share a digit are
 // serialised by the hardware, which costs less than resolving peers first).
-template <bool kMasked>
+template <int BITS, bool kMasked>
 __global__ void __launch_bounds__(kThreads) upsweep_kernel(const unsigned* __restrict__ keys_in, SortCount src,
                                                            unsigned fixed, unsigned capacity, int shift,
                                                            unsigned spans, unsigned* __restrict__ counts,
                                                            const Ctrl* __restrict__ ctrl) {
-    __shared__ unsigned s_h[kWarps][kRadix];
+    constexpr int R = 1 << BITS;
+    __shared__ unsigned s_h[kWarps][R];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned n;
     if (!pass_items(ctrl, src, fixed, capacity, n)) return;
+    for (int d = tid; d < R; d += kThreads)
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) s_h[w][tid] = 0;
+        for (int w = 0; w < kWarps; ++w) s_h[w][d] = 0;
     __syncthreads();
     unsigned t0, t1;
     span_blocks(n, spans, blockIdx.x, t0, t1);
     for (unsigned t = t0; t < t1; ++t) {
         unsigned key[kItems], val[kItems], dg[kItems];
-        load_block<kMasked, false>(keys_in, nullptr, t, n, shift, warp, lane, key, val, dg);
+        load_block<R, kMasked, false>(keys_in, nullptr, t, n, shift, warp, lane, key, val, dg);
 #pragma unroll
         for (int k = 0; k < kItems; ++k)
-            if (dg[k] < kRadix) atomicAdd(&s_h[warp][dg[k]], 1u);
+            if (dg[k] < R) atomicAdd(&s_h[warp][dg[k]], 1u);
     }
     __syncthreads();
-    unsigned c = 0;
+    for (int d = tid; d < R; d += kThreads) {
+        unsigned c = 0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) c += s_h[w][tid];
-    counts[static_cast<size_t>(tid) * spans + blockIdx.x] = c;
+        for (int w = 0; w < kWarps; ++w) c += s_h[w][d];
+        counts[static_cast<size_t>(d) * spans + blockIdx.x] = c;
+    }
 }
 
 // One CTA per digit: exclusive scan of the digit's counts over the spans, in place, and its total.
@@ -146,7 +151,9 @@ __global__ void __launch_bounds__(kThreads) span_scan_kernel(unsigned* __restric
 }
 
 // Ranks, scatters and writes each block of the span. The masked pass publishes the visible count.
-template <bool kMasked, bool kKeysOut>
+// Thread tid owns digits [tid * DPT, tid * DPT + DPT) in the per-digit phases, so a block scan over
+// the threads' sums is a scan in digit order.
+template <int BITS, bool kMasked, bool kKeysOut>
 __global__ void __launch_bounds__(kThreads) downsweep_kernel(const unsigned* __restrict__ keys_in,
                                                              const unsigned* __restrict__ vals_in,
                                                              unsigned* __restrict__ keys_out,
@@ -154,60 +161,87 @@ __global__ void __launch_bounds__(kThreads) downsweep_kernel(const unsigned* __r
                                                              unsigned fixed, unsigned capacity, int shift,
                                                              unsigned spans, const unsigned* __restrict__ counts,
                                                              const unsigned* __restrict__ totals, Ctrl* ctrl) {
+    constexpr int R = 1 << BITS;
+    constexpr int DPT = R / kThreads;  // digits per thread: 1 (8-bit digits) or 2 (9-bit)
+    static_assert(DPT * kThreads == R, "digit count must be a multiple of the block size");
     __shared__ unsigned s_keys[kBlockItems];
     __shared__ unsigned s_vals[kBlockItems];
-    __shared__ unsigned s_wh[kWarps][kRadix];
-    __shared__ unsigned s_dstart[kRadix];
-    __shared__ unsigned s_gbase[kRadix];
+    __shared__ unsigned s_wh[kWarps][R];
+    __shared__ unsigned s_dstart[R];
+    __shared__ unsigned s_gbase[R];
     __shared__ unsigned s_tmp[kWarps];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned n;
     if (!pass_items(ctrl, src, fixed, capacity, n)) return;
-    const unsigned d = tid;  // this thread's digit in the per-digit phases
-    unsigned all;
-    const unsigned gstart = block_excl_scan<kThreads>(totals[d], s_tmp, all);
-    if (kMasked && blockIdx.x == 0 && tid == 0) ctrl->vis_count = all;
-    unsigned run = gstart + counts[static_cast<size_t>(d) * spans + blockIdx.x];  // next output of digit d
+    const int d0 = tid * DPT;
+    unsigned run[DPT];  // next global output position of each of this thread's digits
+    {
+        unsigned tot[DPT], sum = 0;
+#pragma unroll
+        for (int j = 0; j < DPT; ++j) {
+            tot[j] = totals[d0 + j];
+            sum += tot[j];
+        }
+        unsigned all;
+        unsigned g = block_excl_scan<kThreads>(sum, s_tmp, all);
+        if (kMasked && blockIdx.x == 0 && tid == 0) ctrl->vis_count = all;
+#pragma unroll
+        for (int j = 0; j < DPT; ++j) {
+            run[j] = g + counts[static_cast<size_t>(d0 + j) * spans + blockIdx.x];
+            g += tot[j];
+        }
+    }
     unsigned t0, t1;
     span_blocks(n, spans, blockIdx.x, t0, t1);
     const unsigned lt = lanemask_lt();
 
     for (unsigned t = t0; t < t1; ++t) {
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) s_wh[w][d] = 0;
+        for (int j = 0; j < DPT; ++j)
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) s_wh[w][d0 + j] = 0;
         unsigned key[kItems], val[kItems], dg[kItems];
-        load_block<kMasked, true>(keys_in, vals_in, t, n, shift, warp, lane, key, val, dg);
+        load_block<R, kMasked, true>(keys_in, vals_in, t, n, shift, warp, lane, key, val, dg);
         __syncthreads();
         // Warp-level stable ranking: items in (k, lane) order, i.e. ascending position.
         unsigned rank[kItems];
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg[k]);
-            const unsigned cnt = dg[k] < kRadix ? s_wh[warp][dg[k]] : 0u;
+            const unsigned cnt = dg[k] < R ? s_wh[warp][dg[k]] : 0u;
             rank[k] = cnt + __popc(peers & lt);
             __syncwarp();
-            if (dg[k] < kRadix && lane == 31 - __clz(peers)) s_wh[warp][dg[k]] = cnt + __popc(peers);
+            if (dg[k] < R && lane == 31 - __clz(peers)) s_wh[warp][dg[k]] = cnt + __popc(peers);
             __syncwarp();
         }
         __syncthreads();
         // Per digit: the offset of each warp's run, the block's digit count and the block-local start.
-        unsigned cnt = 0;
+        unsigned cnt[DPT], sum = 0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const unsigned c = s_wh[w][d];
-            s_wh[w][d] = cnt;
-            cnt += c;
+        for (int j = 0; j < DPT; ++j) {
+            cnt[j] = 0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) {
+                const unsigned c = s_wh[w][d0 + j];
+                s_wh[w][d0 + j] = cnt[j];
+                cnt[j] += c;
+            }
+            sum += cnt[j];
         }
         unsigned block_total;
-        const unsigned dstart = block_excl_scan<kThreads>(cnt, s_tmp, block_total);
-        s_dstart[d] = dstart;
-        s_gbase[d] = run - dstart;
-        run += cnt;
+        unsigned dstart = block_excl_scan<kThreads>(sum, s_tmp, block_total);
+#pragma unroll
+        for (int j = 0; j < DPT; ++j) {
+            s_dstart[d0 + j] = dstart;
+            s_gbase[d0 + j] = run[j] - dstart;
+            run[j] += cnt[j];
+            dstart += cnt[j];
+        }
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
-            if (dg[k] < kRadix) {
+            if (dg[k] < R) {
                 const unsigned pos = s_dstart[dg[k]] + s_wh[warp][dg[k]] + rank[k];
                 s_keys[pos] = key[k];
                 s_vals[pos] = val[k];
@@ -216,7 +250,7 @@ __global__ void __launch_bounds__(kThreads) downsweep_kernel(const unsigned* __r
         __syncthreads();
         for (unsigned p = tid; p < block_total; p += kThreads) {
             const unsigned k = s_keys[p];
-            const unsigned g = s_gbase[(k >> shift) & (kRadix - 1)] + p;
+            const unsigned g = s_gbase[(k >> shift) & (R - 1)] + p;
             if (kKeysOut) keys_out[g] = k;
             vals_out[g] = s_vals[p];
         }
@@ -493,31 +527,49 @@ unsigned spans_for(uint64_t max_items) {
 
 void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream) { frame_begin_kernel<<<1, 1, 0, stream>>>(ctrl); }
 
-size_t sort_scratch_words() { return static_cast<size_t>(kRadix) * kMaxSpans + kRadix; }
+size_t sort_scratch_words() { return static_cast<size_t>(1 << kMaxRadixBits) * (kMaxSpans + 1); }
 size_t sort_span_sums() { return kMaxSpans; }
 unsigned expand_chunk_pairs() { return kExpandChunk; }
+bool radix_bits_supported(int bits) { return bits == 8 || bits == 9; }
 
-void launch_radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
-                       bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned* scratch,
-                       Ctrl* ctrl, cudaStream_t stream) {
+namespace {
+template <int BITS>
+void radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out, bool masked,
+                SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned* scratch, Ctrl* ctrl,
+                cudaStream_t stream) {
+    constexpr int R = 1 << BITS;
     const unsigned spans = spans_for(src == SortCount::kFixed ? fixed : capacity);
     unsigned* counts = scratch;
-    unsigned* totals = scratch + static_cast<size_t>(kRadix) * kMaxSpans;
+    unsigned* totals = scratch + static_cast<size_t>(R) * kMaxSpans;
     if (masked)
-        upsweep_kernel<true><<<spans, kThreads, 0, stream>>>(keys_in, src, fixed, capacity, shift, spans, counts, ctrl);
+        upsweep_kernel<BITS, true><<<spans, kThreads, 0, stream>>>(keys_in, src, fixed, capacity, shift, spans, counts,
+                                                                   ctrl);
     else
-        upsweep_kernel<false><<<spans, kThreads, 0, stream>>>(keys_in, src, fixed, capacity, shift, spans, counts, ctrl);
-    span_scan_kernel<<<kRadix, kThreads, 0, stream>>>(counts, totals, spans, src, fixed, capacity, ctrl);
+        upsweep_kernel<BITS, false><<<spans, kThreads, 0, stream>>>(keys_in, src, fixed, capacity, shift, spans, counts,
+                                                                    ctrl);
+    span_scan_kernel<<<R, kThreads, 0, stream>>>(counts, totals, spans, src, fixed, capacity, ctrl);
     if (masked)
-        downsweep_kernel<true, true><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src, fixed,
-                                                                    capacity, shift, spans, counts, totals, ctrl);
+        downsweep_kernel<BITS, true, true><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src,
+                                                                          fixed, capacity, shift, spans, counts, totals,
+                                                                          ctrl);
     else if (keys_out)
-        downsweep_kernel<false, true><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src, fixed,
-                                                                     capacity, shift, spans, counts, totals, ctrl);
+        downsweep_kernel<BITS, false, true><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src,
+                                                                           fixed, capacity, shift, spans, counts,
+                                                                           totals, ctrl);
     else
-        downsweep_kernel<false, false><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src,
-                                                                      fixed, capacity, shift, spans, counts, totals,
-                                                                      ctrl);
+        downsweep_kernel<BITS, false, false><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src,
+                                                                            fixed, capacity, shift, spans, counts,
+                                                                            totals, ctrl);
+}
+}  // namespace
+
+void launch_radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
+                       bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, int bits,
+                       unsigned* scratch, Ctrl* ctrl, cudaStream_t stream) {
+    if (bits == 9)
+        radix_pass<9>(keys_in, vals_in, keys_out, vals_out, masked, src, fixed, capacity, shift, scratch, ctrl, stream);
+    else
+        radix_pass<8>(keys_in, vals_in, keys_out, vals_out, masked, src, fixed, capacity, shift, scratch, ctrl, stream);
 }
 
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,

@@ -218,17 +218,19 @@ def keys_of(tiles: np.ndarray, values: np.ndarray, depth: np.ndarray) -> np.ndar
 
 @dataclasses.dataclass
 class BatchOptions:
-    """aniso_b200_batch_options: colour options plus the launch shape (tile, blend batch, graph)."""
+    """aniso_b200_batch_options: colour options plus the launch shape (tile, blend batch, graph,
+    radix digit width)."""
 
     sh_degree: int = 3
     splat_scale: float = 1.0
     tile: tuple[int, int] = (16, 16)
     blend_batch: int = 256
     use_graph: bool = False
+    radix_bits: int = 8
 
     def c(self) -> _lib.BatchOptions:
         return _lib.BatchOptions(int(self.sh_degree), float(self.splat_scale), int(self.tile[0]), int(self.tile[1]),
-                                 int(self.blend_batch), 1 if self.use_graph else 0)
+                                 int(self.blend_batch), 1 if self.use_graph else 0, int(self.radix_bits))
 
 
 def c_cameras(cameras) -> ctypes.Array:

@@ -251,9 +251,10 @@ def batched_leg(torch, steps: int):
             "views_per_s": V * 1000.0 / ms_b, "views_per_s_per_view_launches": V * 1000.0 / ms_pv,
             "speedup_vs_per_view": ms_pv / ms_b, "ms_per_batch": ms_b, "ms_per_64_plain_launches": ms_pv,
             "gaussians_per_s": V * raws[0].n / (ms_b / 1000.0),
-            "tuned": {"tile": "%dx%d" % best.tile, "blend_batch": best.blend_batch, "cuda_graph": True},
-            "candidates_ms": {"%dx%d/%d" % (c["tile"][0], c["tile"][1], c["blend_batch"]): round(c["ms"], 3)
-                              for c in candidates},
+            "tuned": {"tile": "%dx%d" % best.tile, "blend_batch": best.blend_batch, "radix_bits": best.radix_bits,
+                      "cuda_graph": True},
+            "candidates_ms": {"%dx%d/%d/%db" % (c["tile"][0], c["tile"][1], c["blend_batch"], c["radix_bits"]):
+                              round(c["ms"], 3) for c in candidates},
             "pairs": st["tile_pairs"], "images_equal_per_view": same}
 
 

@@ -133,6 +133,7 @@ typedef struct aniso_b200_batch_options {
     int32_t tile_h;      /*   the image is the same for every shape */
     int32_t blend_batch; /* splats staged per blend round: < 256 the smaller, >= 256 the larger set */
     int32_t use_graph;   /* 1: record the launch sequence once as a CUDA graph and replay it */
+    int32_t radix_bits;  /* digit width of the sort's LSD passes: 8 (the default for 0) or 9 */
 } aniso_b200_batch_options;
 
 /* A batch of n_views views; view k shows scene scenes[view_scene[k]]. The views of one scene must

@@ -67,15 +67,16 @@ def test_batch_views_equal_single_renders(ab, torch):
     assert st["tile_pairs"] > 0
 
 
-@pytest.mark.parametrize("tile,batch", [((8, 8), 128), ((8, 8), 256), ((16, 16), 128), ((16, 32), 256),
-                                        ((16, 32), 512)])
-def test_image_independent_of_launch_shape(ab, torch, tile, batch):
+@pytest.mark.parametrize("tile,batch,bits", [((8, 8), 128, 8), ((8, 8), 256, 9), ((16, 16), 128, 9),
+                                             ((16, 16), 256, 9), ((16, 32), 256, 8), ((16, 32), 512, 9)])
+def test_image_independent_of_launch_shape(ab, torch, tile, batch, bits):
     clouds, view_scene, cams = mixed_views()
     rs = [ab.GpuRenderer(g, sh, d) for g, sh, d in clouds]
     single = [rs[s].render(c) for s, c in zip(view_scene, cams)]
-    _, imgs, _ = render_batch(ab, torch, rs, view_scene, cams, ab.BatchOptions(tile=tile, blend_batch=batch))
+    _, imgs, _ = render_batch(ab, torch, rs, view_scene, cams,
+                              ab.BatchOptions(tile=tile, blend_batch=batch, radix_bits=bits))
     for k, (a, b) in enumerate(zip(imgs, single)):
-        np.testing.assert_array_equal(a, b, err_msg="view %d, tile %s" % (k, tile))
+        np.testing.assert_array_equal(a, b, err_msg="view %d, tile %s, %d-bit digits" % (k, tile, bits))
 
 
 def test_graph_replay_follows_new_cameras(ab, torch):
