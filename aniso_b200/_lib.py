@@ -47,6 +47,7 @@ EXPORTS = [
     "aniso_b200_train_batch_backward",
     "aniso_b200_sort_projection_noalloc",
     "aniso_b200_scene_load_ply",
+    "aniso_b200_adam_step",
 ]
 
 
@@ -79,7 +80,14 @@ class RawParams(ctypes.Structure):
 
 class RawGrads(ctypes.Structure):
     _fields_ = [("means", ctypes.c_void_p), ("log_scales", ctypes.c_void_p), ("quats", ctypes.c_void_p),
-                ("opacity_logits", ctypes.c_void_p), ("sh", ctypes.c_void_p)]
+                ("opacity_logits", ctypes.c_void_p), ("sh", ctypes.c_void_p), ("grad2d", ctypes.c_void_p),
+                ("visible", ctypes.c_void_p)]
+
+
+class AdamGroup(ctypes.Structure):
+    _fields_ = [("param", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("exp_avg", ctypes.c_void_p),
+                ("exp_avg_sq", ctypes.c_void_p), ("count", ctypes.c_int64), ("lr", ctypes.c_float),
+                ("lr_head", ctypes.c_float), ("row", ctypes.c_int32), ("head", ctypes.c_int32), ("eps", ctypes.c_float)]
 
 
 class AnisoError(RuntimeError):
@@ -100,6 +108,7 @@ def _load():
         "aniso_b200_scene_create_raw": [P, P, P, P, P, P, I64, I32, ctypes.POINTER(P)],
         "aniso_b200_scene_destroy": [P],
         "aniso_b200_scene_load_ply": [ctypes.c_char_p, ctypes.POINTER(P)],
+        "aniso_b200_adam_step": [ctypes.POINTER(AdamGroup), I32, I32, ctypes.c_float, ctypes.c_float, P],
         "aniso_b200_render": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, ctypes.POINTER(Stats)],
         "aniso_b200_render_device": [P, ctypes.POINTER(Camera), ctypes.POINTER(Options), P, P],
         "aniso_b200_sync": [P, ctypes.POINTER(Stats)],

@@ -85,7 +85,7 @@ def _raw_params(means, log_scales, quats, opacity_logits, sh) -> _lib.RawParams:
 
 class RasterizeFunction(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, means, log_scales, quats, opacity_logits, sh, camera, options):
+    def forward(ctx, means, log_scales, quats, opacity_logits, sh, camera, options, stats=None):
         means, log_scales, quats = means.contiguous(), log_scales.contiguous(), quats.contiguous()
         opacity_logits, sh = opacity_logits.contiguous(), sh.contiguous()
         params = _raw_params(means, log_scales, quats, opacity_logits, sh)
@@ -103,6 +103,7 @@ class RasterizeFunction(torch.autograd.Function):
         ctx.lease = _Lease(trainer)
         if not any(ctx.needs_input_grad[:5]):
             ctx.lease.release()
+        ctx.stats = stats
         ctx.save_for_backward(means, log_scales, quats, opacity_logits, sh)
         return img
 
@@ -110,7 +111,8 @@ class RasterizeFunction(torch.autograd.Function):
     def backward(ctx, grad_img):
         means, log_scales, quats, opacity_logits, sh = ctx.saved_tensors
         grads = [torch.zeros_like(t) for t in (means, log_scales, quats, opacity_logits, sh)]
-        g = _lib.RawGrads(*[t.data_ptr() for t in grads])
+        extra = [ctx.stats[0].data_ptr(), ctx.stats[1].data_ptr()] if ctx.stats is not None else []
+        g = _lib.RawGrads(*[t.data_ptr() for t in grads], *extra)
         gi = grad_img.contiguous().float()
         stream = torch.cuda.current_stream(means.device).cuda_stream
         if ctx.lease.trainer is None:
@@ -121,13 +123,23 @@ class RasterizeFunction(torch.autograd.Function):
         finally:
             # The next forward on this trainer is ordered after the backward's kernels (same stream).
             ctx.lease.release()
-        return (*grads, None, None)
+        return (*grads, None, None, None)
 
 
-def rasterize(means, log_scales, quats, opacity_logits, sh, camera, sh_degree: int = 3, splat_scale: float = 1.0):
-    """Differentiable render of one view: (H, W, 3) float32 colour."""
+def rasterize(means, log_scales, quats, opacity_logits, sh, camera, sh_degree: int = 3, splat_scale: float = 1.0,
+              stats=None):
+    """Differentiable render of one view: (H, W, 3) float32 colour.
+
+    stats: optional (grad2d, visible) float32 CUDA tensors of shape (n,); the backward adds to them
+    each Gaussian's |dL/d(screen position)| in NDC units and 1 where it was visible -- what a
+    densification strategy accumulates."""
+    if stats is not None:
+        n = means.shape[0]
+        for t in stats:
+            if tuple(t.shape) != (n,) or t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous():
+                raise ValueError("stats must be two contiguous float32 CUDA tensors of shape (n,)")
     return RasterizeFunction.apply(means, log_scales, quats, opacity_logits, sh, camera,
-                                   RenderOptions(sh_degree, splat_scale))
+                                   RenderOptions(sh_degree, splat_scale), stats)
 
 
 class RasterizeBatchFunction(torch.autograd.Function):

@@ -413,6 +413,13 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
 
     // ---- record parameters -> conic, opacity, colour ----
     const float gu = g9[0], gv = g9[1];
+    // What densification reads (gsplat's DefaultStrategy): the screen-space gradient in NDC units
+    // (x width/2, x height/2), its norm added over views, and the number of views that saw it.
+    if (out.grad2d) {
+        const float nu = gu * (0.5f * cam.width), nv = gv * (0.5f * cam.height);
+        accumulate(&out.grad2d[i], sqrtf(nu * nu + nv * nv));
+        accumulate(&out.visible[i], 1.0f);
+    }
     const float gA = g9[2] * kHalfLog2e, gB = g9[3] * kNegLog2e, gC = g9[4] * kHalfLog2e;
     const float go = g9[5] / (o * kLn2);  // L = log2(o)
     float* gsh = out.sh + static_cast<size_t>(i) * raw.sh_planes * 4;

@@ -1318,6 +1318,9 @@ int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const
         if (P.scenes[s].src.n > 0 && (!grads[s].means || !grads[s].log_scales || !grads[s].quats ||
                                       !grads[s].opacity_logits || !grads[s].sh))
             return fail(ANISO_B200_ERR_ARGUMENT, "a gradient pointer is NULL");
+    for (size_t s = 0; s < P.scenes.size(); ++s)
+        if (grads[s].grad2d && !grads[s].visible)
+            return fail(ANISO_B200_ERR_ARGUMENT, "grad2d needs its visible counts");
     Arena& A = t->arena;
     const Ctrl& h = *t->host_ctrl;
     AB_TRY(t->grad_pair.reserve(std::max<uint64_t>(h.pair_total, 1) * 9));
@@ -1343,7 +1346,8 @@ int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const
     for (size_t k = 0; k < P.views.size(); ++k) {
         const unsigned s = P.views[k].scene;
         const aniso_b200_raw_grads& g = grads[s];
-        const RawGrads out{g.means, g.log_scales, g.quats, g.opacity_logits, g.sh};
+        const RawGrads out{g.means, g.log_scales, g.quats, g.opacity_logits, g.sh, g.grad2d,
+                           g.grad2d ? g.visible : nullptr};
         launch_gauss_backward(P.scenes[s].src, P.views[k].cam, P.views[k].entry_base, A.ctrl.p, A.depth_key.p,
                               A.rank.p, A.offs.p, A.rect_sorted.p, t->grad_pair.p, t->vis_list.p, t->vis_counts.p + k,
                               out, st);

@@ -100,6 +100,8 @@ struct RawGrads {
     float* quats;
     float* logits;
     float* sh;
+    float* grad2d;   // optional (NULL): per Gaussian, |dL/d(screen position)| in NDC units, added over views
+    float* visible;  // with grad2d: per Gaussian, the number of views it was visible in, added
 };
 // grad_pair: 9 floats per pair, at the pair's depth-ordered slot.
 void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int tile_h, float* grad_pair,

@@ -183,6 +183,11 @@ typedef struct aniso_b200_raw_grads {
     float* quats;
     float* opacity_logits;
     float* sh;
+    /* Optional (NULL to skip), for densification: per Gaussian, the norm of dL/d(screen position)
+     * in NDC units (pixels x width/2, x height/2, as gsplat's DefaultStrategy normalises it) and the
+     * number of views it was visible in, both added to over the views of a backward. */
+    float* grad2d;
+    float* visible;
 } aniso_b200_raw_grads;
 
 int aniso_b200_trainer_create(aniso_b200_trainer** out);
@@ -211,6 +216,30 @@ int aniso_b200_train_batch_forward(aniso_b200_trainer* trainer, const aniso_b200
                                    float* const* images_device, void* stream);
 int aniso_b200_train_batch_backward(aniso_b200_trainer* trainer, const float* const* grad_images_device,
                                     const aniso_b200_raw_grads* grads, void* stream);
+
+/* ---- the optimizer step of a training loop (no counterpart in the reference: its training drives
+ * one torch.optim.Adam per parameter group, pipeline/train_gsplat.py:165-167) ----------------- */
+
+/* One parameter group: `count` floats of DEVICE arrays param / grad / exp_avg / exp_avg_sq, learning
+ * rate lr and eps. Optionally the first `head` floats of every `row` floats use lr_head instead
+ * (the SH tensor: coefficient 0 and the rest have different rates); head = 0 for none. */
+typedef struct aniso_b200_adam_group {
+    float* param;
+    const float* grad;
+    float* exp_avg;
+    float* exp_avg_sq;
+    int64_t count;
+    float lr;
+    float lr_head;
+    int32_t row;
+    int32_t head;
+    float eps;
+} aniso_b200_adam_group;
+
+/* Adam (torch.optim.Adam's update, no weight decay) for step number `step` (from 1) over up to 8
+ * groups in one launch, enqueued on `stream`. */
+int aniso_b200_adam_step(const aniso_b200_adam_group* groups, int32_t n_groups, int32_t step, float beta1,
+                         float beta2, void* stream);
 
 /* ---- introspection used by the parity tests (no counterpart in gpu_render.h) ---------------- */
 
