@@ -443,19 +443,35 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
         }
         float gdir[3] = {0.f, 0.f, 0.f};
         const float grgb[3] = {g9[6], g9[7], g9[8]};
+        float gc3[3];
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
             float pre = 0.5f;
 #pragma unroll
             for (int k = 0; k < count; ++k) pre += bs[k] * shv[k * 3 + ch];
             const float gc = pre > 0.f ? grgb[ch] : 0.f;  // rgb = max(0, pre)
+            gc3[ch] = gc;
 #pragma unroll
             for (int k = 0; k < count; ++k) {
-                accumulate(&gsh[k * 3 + ch], bs[k] * gc);
                 gdir[0] += shv[k * 3 + ch] * bxs[k] * gc;
                 gdir[1] += shv[k * 3 + ch] * bys[k] * gc;
                 gdir[2] += shv[k * 3 + ch] * bzs[k] * gc;
             }
+        }
+        // d rgb / d sh = basis (x) gc, added 16 bytes at a time: float f of the row is coefficient f/3,
+        // channel f%3 (each element still gets its own rounded add).
+        constexpr int kFloats = count * 3;
+        float4* gsh4 = reinterpret_cast<float4*>(gsh);
+#pragma unroll
+        for (int pl = 0; pl < (kFloats + 3) / 4; ++pl) {
+            float4 o = gsh4[pl];
+            float w[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int f = 4 * pl + e;
+                if (f < kFloats) w[e] = __fadd_rn(w[e], bs[f / 3] * gc3[f % 3]);
+            }
+            gsh4[pl] = make_float4(w[0], w[1], w[2], w[3]);
         }
         const float dd = ux * gdir[0] + uy * gdir[1] + uz * gdir[2];
         gm[0] += (gdir[0] - ux * dd) / len;
@@ -541,10 +557,10 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
     // q_n = q / |q|
     const float dq = qw * gqw + qx * gqx + qy * gqy + qz * gqz;
     const float il = qlen > 0 ? 1.0f / qlen : 0.f;
-    accumulate(&out.quats[4 * i], (gqw - qw * dq) * il);
-    accumulate(&out.quats[4 * i + 1], (gqx - qx * dq) * il);
-    accumulate(&out.quats[4 * i + 2], (gqy - qy * dq) * il);
-    accumulate(&out.quats[4 * i + 3], (gqz - qz * dq) * il);
+    float4* gq4 = reinterpret_cast<float4*>(out.quats) + i;
+    const float4 oq = *gq4;
+    *gq4 = make_float4(__fadd_rn(oq.x, (gqw - qw * dq) * il), __fadd_rn(oq.y, (gqx - qx * dq) * il),
+                       __fadd_rn(oq.z, (gqy - qy * dq) * il), __fadd_rn(oq.w, (gqz - qz * dq) * il));
 }
 
 }  // namespace

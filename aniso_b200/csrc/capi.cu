@@ -1318,9 +1318,12 @@ int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const
         if (P.scenes[s].src.n > 0 && (!grads[s].means || !grads[s].log_scales || !grads[s].quats ||
                                       !grads[s].opacity_logits || !grads[s].sh))
             return fail(ANISO_B200_ERR_ARGUMENT, "a gradient pointer is NULL");
-    for (size_t s = 0; s < P.scenes.size(); ++s)
+    for (size_t s = 0; s < P.scenes.size(); ++s) {
         if (grads[s].grad2d && !grads[s].visible)
             return fail(ANISO_B200_ERR_ARGUMENT, "grad2d needs its visible counts");
+        if ((reinterpret_cast<uintptr_t>(grads[s].quats) | reinterpret_cast<uintptr_t>(grads[s].sh)) & 15)
+            return fail(ANISO_B200_ERR_ARGUMENT, "the quats and sh gradients must be 16-byte aligned");
+    }
     Arena& A = t->arena;
     const Ctrl& h = *t->host_ctrl;
     AB_TRY(t->grad_pair.reserve(std::max<uint64_t>(h.pair_total, 1) * 9));

@@ -175,8 +175,8 @@ typedef struct aniso_b200_raw_params {
     int32_t sh_degree;
 } aniso_b200_raw_params;
 
-/* Gradient outputs, DEVICE pointers with the shapes of aniso_b200_raw_params. The caller zeroes
- * them; entries of Gaussians culled in the view are left untouched. */
+/* Gradient outputs, DEVICE pointers with the shapes of aniso_b200_raw_params (quats and sh 16-byte
+ * aligned). The caller zeroes them; entries of Gaussians culled in the view are left untouched. */
 typedef struct aniso_b200_raw_grads {
     float* means;
     float* log_scales;
