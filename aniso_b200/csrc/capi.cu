@@ -248,8 +248,9 @@ struct Plan {
         const int S = static_cast<int>(srcs.size());
         if (S <= 0 || n_views <= 0 || !view_scene || !cameras)
             return fail(ANISO_B200_ERR_ARGUMENT, "a batch needs at least one scene and one view");
-        int rendered = std::min(sh.sh_degree, 3);
-        for (int s = 0; s < S; ++s) rendered = std::min(rendered, deg[s]);
+        // Each view is coloured up to min(option, its scene's degree, 3), as gpu_render.cu:314 does
+        // per scene; the preprocess kernel is instantiated for the largest of them.
+        const int wanted = std::min(sh.sh_degree, 3);
         views.assign(n_views, ViewInfo{});
         scenes.assign(S, BatchScene<Src>{});
         entry_base.assign(n_views, 0);
@@ -264,7 +265,8 @@ struct Plan {
             else if (last[s] != k - 1) return fail(ANISO_B200_ERR_ARGUMENT, "the views of a scene must be consecutive");
             last[s] = k;
             ViewInfo& v = views[k];
-            AB_TRY(pack_camera(deg[s], rendered, &cameras[k], sh.splat_scale, sh.tile_w, sh.tile_h, v.cam));
+            AB_TRY(pack_camera(deg[s], std::min(wanted, deg[s]), &cameras[k], sh.splat_scale, sh.tile_w, sh.tile_h,
+                               v.cam));
             v.scene = static_cast<unsigned>(s);
             v.n = static_cast<unsigned>(srcs[s].n);
             v.entry_base = static_cast<unsigned>(entries);
@@ -288,7 +290,12 @@ struct Plan {
         return 0;
     }
 
-    int rendered_degree() const { return views.empty() ? 0 : views[0].cam.shDegree; }
+    // The largest degree any view is coloured with (the preprocess kernel's instantiation).
+    int rendered_degree() const {
+        int d = 0;
+        for (const auto& v : views) d = std::max(d, v.cam.shDegree);
+        return d;
+    }
     size_t blob_bytes() const {
         return views.size() * sizeof(ViewInfo) + scenes.size() * sizeof(BatchScene<Src>) +
                3 * views.size() * sizeof(unsigned);

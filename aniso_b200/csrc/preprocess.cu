@@ -57,6 +57,16 @@ __device__ __forceinline__ float3 sh_color(const float4* __restrict__ shp, float
     return make_float3(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f), fmaxf(c[2], 0.f));
 }
 
+// The colour at the view's own degree (<= D, and <= the scene's stored degree, so the words read
+// are the Gaussian's own): views of scenes with different degrees share one launch.
+template <int D>
+__device__ __forceinline__ float3 sh_color_upto(int degree, const float4* __restrict__ shp, float x, float y, float z) {
+    if (D >= 3 && degree >= 3) return sh_color<3>(shp, x, y, z);
+    if (D >= 2 && degree == 2) return sh_color<(D >= 2 ? 2 : 0)>(shp, x, y, z);
+    if (D >= 1 && degree == 1) return sh_color<(D >= 1 ? 1 : 0)>(shp, x, y, z);
+    return sh_color<0>(shp, x, y, z);
+}
+
 struct Projected {
     float u, v, depth;
     float a, b, c, det;       // 2D covariance (with the 0.3 low-pass) and its determinant
@@ -261,7 +271,8 @@ __global__ void __launch_bounds__(256, 3) preprocess_kernel(const BatchScene<Src
             // Colour along the unit direction from the camera centre (gpu_render.cu:137-139).
             float3 d = make_float3(pg.x - cam.eye[0], pg.y - cam.eye[1], pg.z - cam.eye[2]);
             const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-            const float3 rgb = sh_color<D>(sc.src.sh + i * sc.src.sh_planes, d.x / len, d.y / len, d.z / len);
+            const float3 rgb = sh_color_upto<D>(cam.shDegree, sc.src.sh + i * sc.src.sh_planes, d.x / len, d.y / len,
+                                                d.z / len);
 
             const float opacity = pg.w;
             const unsigned bx = axis_bounds(p.u, p.a, tau, p.radius, cam.width);

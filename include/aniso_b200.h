@@ -127,7 +127,7 @@ size_t aniso_b200_last_error(char* buf, size_t len);
 typedef struct aniso_b200_batch aniso_b200_batch;
 
 typedef struct aniso_b200_batch_options {
-    int32_t sh_degree;   /* colour up to this SH degree, clamped to every scene's and to 3 */
+    int32_t sh_degree;   /* colour up to this SH degree, clamped to each view's scene's and to 3 */
     float splat_scale;   /* as aniso_b200_options */
     int32_t tile_w;      /* tile shape: 8x8, 16x16 (the reference's, and the default for 0) or 16x32; */
     int32_t tile_h;      /*   the image is the same for every shape */

@@ -67,6 +67,31 @@ def test_batch_views_equal_single_renders(ab, torch):
     assert st["tile_pairs"] > 0
 
 
+def test_scenes_of_different_degrees_in_one_batch(ab, torch):
+    """Each view is coloured at its own scene's degree, as a single render of that scene is."""
+    g3, sh3, _ = kat.random_cloud(6000, seed=7)
+    g1, sh1 = g3[:4000].copy(), np.ascontiguousarray(sh3[:4000].reshape(4000, 16, 3)[:, :4]).reshape(4000, 12)
+    g0, sh0 = g3[2000:].copy(), np.ascontiguousarray(sh3[2000:].reshape(4000, 16, 3)[:, :1]).reshape(4000, 3)
+    rs = [ab.GpuRenderer(g3, sh3, 3), ab.GpuRenderer(g1, sh1, 1), ab.GpuRenderer(g0, sh0, 0)]
+    cams = [kat.gpu_test_camera(160, 120), kat.gpu_test_camera(200, 150), kat.gpu_test_camera(128, 96)]
+    view_scene = [0, 1, 2]
+    for opt in (3, 2):
+        single = [rs[s].render(c, options=ab.RenderOptions(sh_degree=opt)) for s, c in zip(view_scene, cams)]
+        _, imgs, _ = render_batch(ab, torch, rs, view_scene, cams, ab.BatchOptions(sh_degree=opt))
+        for k, (a, b) in enumerate(zip(imgs, single)):
+            np.testing.assert_array_equal(a, b, err_msg="view %d, option %d" % (k, opt))
+
+
+def test_more_views_than_staged_cameras(ab, torch):
+    """A scene seen by more views than the preprocess kernel keeps in shared memory (64)."""
+    g, sh, d = kat.random_cloud(3000, seed=8)
+    r = ab.GpuRenderer(g, sh, d)
+    cams = [kat.gpu_test_camera(64 + (k % 5) * 8, 48 + (k % 3) * 8) for k in range(80)]
+    _, imgs, _ = render_batch(ab, torch, [r], [0] * 80, cams, ab.BatchOptions(use_graph=True))
+    for k in (0, 63, 64, 79):
+        np.testing.assert_array_equal(imgs[k], r.render(cams[k]), err_msg="view %d" % k)
+
+
 @pytest.mark.parametrize("tile,batch,bits", [((8, 8), 128, 8), ((8, 8), 256, 9), ((16, 16), 128, 9),
                                              ((16, 16), 256, 9), ((16, 32), 256, 8), ((16, 32), 512, 9)])
 def test_image_independent_of_launch_shape(ab, torch, tile, batch, bits):
