@@ -299,3 +299,32 @@ def test_faster_than_the_reference_gpu_renderer(ab):
     print("host-to-host ms/frame: reference GpuRenderer %.3f, aniso_b200 %.3f (%.2fx)"
           % (1e3 * t_ref, 1e3 * t_ours, t_ref / t_ours))
     assert t_ours < t_ref
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (7, 5), (17, 9), (3840, 2160)])
+def test_image_sizes_vs_cpu(ab, w, h):
+    """Frames smaller than one tile, ragged tile edges, and 4K (240 x 135 tiles of 16)."""
+    g, sh, deg = kat.random_cloud(20000, seed=9)
+    cam = kat.gpu_test_camera(w, h)
+    img = ab.GpuRenderer(g, sh, deg).render(cam)
+    assert img.shape == (h, w, 3)
+    assert_image_parity(img, cpu_render(g, sh, deg, cam)[0], "%dx%d" % (w, h))
+
+
+def test_empty_scene_renders_black(ab):
+    r = ab.GpuRenderer(np.zeros((0, 11), np.float32), np.zeros((0, 48), np.float32), 3)
+    st = {}
+    img = r.render(kat.gpu_test_camera(320, 240), st)
+    assert not img.any() and st["tile_pairs"] == 0 and st["visible"] == 0
+
+
+def test_degree4_scene_vs_cpu(ab):
+    """The loader accepts degree 4 (ply_loader.cpp:67-73); colour is evaluated up to degree 3."""
+    g, sh3, _ = kat.random_cloud(8000, seed=10)
+    rng = np.random.default_rng(11)
+    sh = np.zeros((8000, 25, 3), np.float32)
+    sh[:, :16] = sh3.reshape(8000, 16, 3)
+    sh[:, 16:] = rng.normal(0, 0.3, (8000, 9, 3))
+    cam = kat.gpu_test_camera(256, 192)
+    img = ab.GpuRenderer(g, sh.reshape(8000, 75), 4).render(cam)
+    assert_image_parity(img, cpu_render(g, sh.reshape(8000, 75), 4, cam)[0], "degree 4")
