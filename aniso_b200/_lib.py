@@ -35,6 +35,7 @@ EXPORTS = [
     "aniso_b200_sort_projection",
     "aniso_b200_profile",
     "aniso_b200_profile_read",
+    "aniso_b200_frame_kernels",
     "aniso_b200_trainer_create",
     "aniso_b200_trainer_destroy",
     "aniso_b200_train_forward",
@@ -131,6 +132,7 @@ def _load():
         "aniso_b200_sort_projection_noalloc": [I64, P, P, P, I32, I32, P, P, U64, P, P, P],
         "aniso_b200_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(I64)],
+        "aniso_b200_frame_kernels": [P, ctypes.POINTER(ctypes.c_int32)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -111,6 +111,7 @@ __device__ __forceinline__ bool pixel_step(PixelState& s, unsigned pos, float p,
 
 template <int TW, int TH>
 __global__ void __launch_bounds__(TW * TH / 2) blend_backward_kernel(BackwardIn in, float* __restrict__ grad_pair) {
+    chain_entry();
     constexpr int kThreads = TW * TH / 2;
     constexpr int kWarps = kThreads / 32;
     constexpr int kWarpsX = TW / 8;
@@ -300,6 +301,7 @@ __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16],
 __global__ void __launch_bounds__(256) visible_list_kernel(int64_t n, unsigned entry_base,
                                                            const unsigned* __restrict__ depth_key,
                                                            unsigned* __restrict__ list, unsigned* counter) {
+    chain_entry();
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const bool vis = i < n && depth_key[entry_base + static_cast<unsigned>(i)] != kCulledKey;
@@ -319,6 +321,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
                                                              const unsigned* __restrict__ offs,
                                                              const unsigned long long* __restrict__ rect_sorted,
                                                              const float* __restrict__ grad_pair, RawGrads out) {
+    chain_entry();
     const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
     const unsigned count = *list_count;
@@ -568,9 +571,10 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
 void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int tile_h, float* grad_pair,
                            cudaStream_t stream) {
     if (tiles == 0) return;
-    if (tile_w == 8) blend_backward_kernel<8, 8><<<tiles, 32, 0, stream>>>(in, grad_pair);
-    else if (tile_h == 32) blend_backward_kernel<16, 32><<<tiles, 256, 0, stream>>>(in, grad_pair);
-    else blend_backward_kernel<16, 16><<<tiles, 128, 0, stream>>>(in, grad_pair);
+    if (tile_w == 8) launch_chained(blend_backward_kernel<8, 8>, dim3(tiles), dim3(32), stream, in, grad_pair);
+    else if (tile_h == 32)
+        launch_chained(blend_backward_kernel<16, 32>, dim3(tiles), dim3(256), stream, in, grad_pair);
+    else launch_chained(blend_backward_kernel<16, 16>, dim3(tiles), dim3(128), stream, in, grad_pair);
 }
 
 void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
@@ -579,13 +583,18 @@ void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned 
                            unsigned* list_count, const RawGrads& out, cudaStream_t stream) {
     const unsigned lblocks = static_cast<unsigned>((raw.n + 255) / 256);
     if (lblocks == 0) return;
-    visible_list_kernel<<<lblocks, 256, 0, stream>>>(raw.n, entry_base, depth_key, list, list_count);
-    const unsigned blocks = static_cast<unsigned>((raw.n + 127) / 128);
+    launch_chained(visible_list_kernel, dim3(lblocks), dim3(256), stream, raw.n, entry_base, depth_key, list,
+                   list_count);
+    const dim3 grid(static_cast<unsigned>((raw.n + 127) / 128)), block(128);
     switch (cam.shDegree) {
-        case 0: gauss_backward_kernel<0><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
-        case 1: gauss_backward_kernel<1><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
-        case 2: gauss_backward_kernel<2><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
-        default: gauss_backward_kernel<3><<<blocks, 128, 0, stream>>>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
+        case 0: launch_chained(gauss_backward_kernel<0>, grid, block, stream, raw, cam, entry_base, ctrl, list, list_count,
+                                rank, offs, rect_sorted, grad_pair, out); break;
+        case 1: launch_chained(gauss_backward_kernel<1>, grid, block, stream, raw, cam, entry_base, ctrl, list, list_count,
+                                rank, offs, rect_sorted, grad_pair, out); break;
+        case 2: launch_chained(gauss_backward_kernel<2>, grid, block, stream, raw, cam, entry_base, ctrl, list, list_count,
+                                rank, offs, rect_sorted, grad_pair, out); break;
+        default: launch_chained(gauss_backward_kernel<3>, grid, block, stream, raw, cam, entry_base, ctrl, list, list_count,
+                                rank, offs, rect_sorted, grad_pair, out); break;
     }
 }
 

@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
                                                             const unsigned* __restrict__ vals,
                                                             const SplatRecord* __restrict__ rec, const Ctrl* ctrl,
                                                             const ViewInfo* __restrict__ views, BatchTables tables) {
+    chain_entry();
     constexpr int kThreads = TW * TH / 2;  // two pixels per lane
     constexpr int kWarpsX = TW / 8;
     __shared__ float4 s_r0[kBatch];
@@ -169,9 +170,11 @@ template <int TW, int TH, int kBatch>
 void launch_shape(unsigned tiles, const uint2* ranges, const unsigned* vals, const SplatRecord* rec, const Ctrl* ctrl,
                   const ViewInfo* views, const BatchTables& tables, bool train, cudaStream_t stream) {
     if (train)
-        blend_kernel<TW, TH, kBatch, true><<<tiles, TW * TH / 2, 0, stream>>>(ranges, vals, rec, ctrl, views, tables);
+        launch_chained(blend_kernel<TW, TH, kBatch, true>, dim3(tiles), dim3(TW * TH / 2), stream, ranges, vals, rec,
+                       ctrl, views, tables);
     else
-        blend_kernel<TW, TH, kBatch, false><<<tiles, TW * TH / 2, 0, stream>>>(ranges, vals, rec, ctrl, views, tables);
+        launch_chained(blend_kernel<TW, TH, kBatch, false>, dim3(tiles), dim3(TW * TH / 2), stream, ranges, vals, rec,
+                       ctrl, views, tables);
 }
 
 }  // namespace

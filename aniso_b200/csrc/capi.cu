@@ -2,8 +2,9 @@
 //
 // Everything renders through one plan: V views of S scenes. A frame is a fixed, host-sync-free
 // sequence of launches on one stream (capturable in a CUDA graph): upload of the plan's view
-// table, frame_begin, preprocess, 4 depth onesweep passes, pair scan, pair expansion, 1-4 tile
-// onesweep passes, tile ranges, blend. Data-dependent sizes (visible entries, pairs) stay on the
+// table, clearing of the tile ranges, then a chain of kernels launched with programmatic stream
+// serialisation: frame_begin, preprocess, 4 depth LSD passes, pair scan, pair expansion, 1-4 tile
+// LSD passes, tile ranges, blend. Data-dependent sizes (visible entries, pairs) stay on the
 // device; grids are sized for capacity and surplus blocks exit at once. The reference instead reads
 // the pair count back mid-frame (gpu_render.cu:329) to size its buffers; here a frame whose pairs
 // exceed the capacity sets an overflow flag instead of writing them, and the host grows the
@@ -15,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -86,7 +88,7 @@ int bits_for(uint32_t v) {  // bits needed to hold v
 }
 
 constexpr uint64_t kMaxEntries = 0xFFFFFFFFull;  // entry and tile indices are 32-bit
-constexpr uint64_t kMaxPairs = 0x3FFFFFFFull;    // look-back status values are 32-bit; keep headroom
+constexpr uint64_t kMaxPairs = 0x3FFFFFFFull;    // pair positions and the span arithmetic are 32-bit
 
 // Work buffers of one frame at a time, sized for `n` entries and a pair capacity.
 struct Arena {
@@ -115,7 +117,7 @@ struct Arena {
             AB_TRY(vis_idx[k].reserve(nn));
         }
         AB_TRY(ctrl.reserve(1, true));
-        AB_TRY(sort_scratch.reserve(sort_scratch_words()));
+        AB_TRY(sort_scratch.reserve(2 * sort_scratch_words()));  // two count matrices and the totals
         AB_TRY(span_sum.reserve(sort_span_sums()));
         AB_TRY(offs.reserve(nn));
         AB_TRY(rank.reserve(nn));
@@ -144,35 +146,99 @@ struct Arena {
     }
 };
 
-// Depth passes over `entries` depth keys (the first compacts the visible ones), pair scan and
-// expansion, tile passes over `tiles` global tiles, and ranges. *final_buf = the pair buffer that
-// holds the sorted pairs. keep_rank: also record each visible entry's depth-sorted position (the
-// adjoint reads it).
-int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank, int bits,
-                 cudaStream_t st, int* final_buf) {
-    Ctrl* ctrl = A.ctrl.p;
-    const unsigned cap = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
-    const int depth_passes = (32 + bits - 1) / bits;  // 4 for 8- and 9-bit digits
-    for (int p = 0; p < depth_passes; ++p) {
-        const int src = (p + 1) & 1, dst = p & 1;  // pass 0 reads depth_key and writes buffer 0
-        launch_radix_pass(p == 0 ? A.depth_key.p : A.vis_key[src].p, p == 0 ? nullptr : A.vis_idx[src].p,
-                          p == depth_passes - 1 ? nullptr : A.vis_key[dst].p, A.vis_idx[dst].p, p == 0,
-                          p == 0 ? SortCount::kFixed : SortCount::kVisible, entries, p == 0 ? entries : cap, p * bits,
-                          bits, A.sort_scratch.p, ctrl, st);
-    }
-    const int sorted = (depth_passes - 1) & 1;
-    const int tile_passes = std::max(1, (bits_for(tiles - 1) + bits - 1) / bits);
-    const DupBuffers dup{A.offs.p, keep_rank ? A.rank.p : nullptr, A.rect_sorted.p, A.chunk_start.p, A.span_sum.p};
-    launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, dup, A.pair_key[0].p,
-                     A.pair_val[0].p, st);
-    for (int p = 0; p < tile_passes; ++p) {
-        const int src = p & 1, dst = src ^ 1;
-        launch_radix_pass(A.pair_key[src].p, A.pair_val[src].p, A.pair_key[dst].p, A.pair_val[dst].p, false,
-                          SortCount::kPairs, 0u, A.pair_cap, p * bits, bits, A.sort_scratch.p, ctrl, st);
-    }
-    const int fin = tile_passes & 1;
+// Clears the frame's tile ranges (a tile without pairs keeps [0, 0)). Enqueued ahead of the
+// frame's kernel chain, so that no memset sits between two chained kernels.
+int clear_ranges(Arena& A, unsigned tiles, cudaStream_t st) {
     AB_TRY(A.ranges.reserve(tiles));
     AB_CUDA(cudaMemsetAsync(A.ranges.p, 0, static_cast<size_t>(tiles) * sizeof(uint2), st));
+    return 0;
+}
+
+// Largest pass (in items, host capacity) whose digits the kernels that write its keys count, in
+// place of an upsweep launch. Below it a pass is latency-bound and one atomic add per key costs less
+// than a counting kernel; above it the counting kernel's streaming read is the cheaper of the two.
+constexpr uint64_t kProducerCountMax = 1ull << 22;
+
+// Depth passes: four 8-bit digits over the 32-bit depth keys (9-bit digits would need four too).
+constexpr int kDepthPasses = 4;
+constexpr int kDepthBits = 8;
+
+// Digit widths of the tile passes: as few passes as digits of at most max_bits (8 or 9) allow, each
+// pass 8 bits wide unless 9 are needed to stay within that count (17 tile bits: 9 + 8).
+int tile_pass_widths(unsigned tiles, int max_bits, int widths[4]) {
+    const int total = std::max(1, bits_for(tiles > 0 ? tiles - 1 : 0));
+    const int n = (total + max_bits - 1) / max_bits;
+    for (int k = 0, shift = 0; k < n; ++k) {
+        widths[k] = total - shift > 8 * (n - k) ? 9 : 8;
+        shift += widths[k];
+    }
+    return n;
+}
+
+unsigned* count_matrix(Arena& A, int q) { return A.sort_scratch.p + (q & 1) * sort_count_words(); }
+
+// The digit counts of the first depth pass when the preprocess accumulates them (the frame is
+// small enough), else {NULL}. *zero_words: the cells frame_begin must clear for it.
+PassCounts first_pass_counts(Arena& A, unsigned entries, unsigned* zero_words) {
+    *zero_words = 0;
+    if (entries == 0 || entries > kProducerCountMax) return PassCounts{};
+    const unsigned spans = sort_spans(entries);
+    *zero_words = spans << kDepthBits;
+    return PassCounts{count_matrix(A, 0), spans, 0u, (1u << kDepthBits) - 1};
+}
+
+// Depth passes over `entries` depth keys (the first compacts the visible ones), pair scan and
+// expansion, tile passes over `tiles` global tiles, and ranges (cleared beforehand by
+// clear_ranges). *final_buf = the pair buffer that holds the sorted pairs. keep_rank: also record
+// each visible entry's depth-sorted position (the adjoint reads it). first_counted: the depth
+// keys' producer accumulated the first depth pass's digit counts (first_pass_counts). In a small
+// frame the expansion likewise counts the first tile pass, the last depth pass's span scan clearing
+// that count matrix first; every other pass has its own upsweep. (Counting in the downsweeps too
+// was measured slower: keys written next to each other often share the next digit, the high depth
+// digits taking few values, so one atomic per key contends -- 0.177 ms against 0.139 ms for the
+// sort of the 740k / 1280x720 frame.)
+int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank, int bits,
+                 bool first_counted, cudaStream_t st, int* final_buf) {
+    Ctrl* ctrl = A.ctrl.p;
+    const unsigned cap = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
+    unsigned* totals = A.sort_scratch.p + 2 * sort_count_words();
+    int tile_bits[4];
+    const int tile_passes = tile_pass_widths(tiles, bits, tile_bits);
+    const bool expand_counts = A.pair_cap <= kProducerCountMax;
+    const unsigned tile_spans = sort_spans(A.pair_cap);
+    const PassCounts first_tile =
+        expand_counts ? PassCounts{count_matrix(A, kDepthPasses), tile_spans, 0u, (1u << tile_bits[0]) - 1}
+                      : PassCounts{};
+
+    for (int p = 0; p < kDepthPasses; ++p) {
+        const int src = (p + 1) & 1, dst = p & 1;  // pass 0 reads depth_key and writes buffer 0
+        const unsigned* keys_in = p == 0 ? A.depth_key.p : A.vis_key[src].p;
+        const SortCount count = p == 0 ? SortCount::kFixed : SortCount::kVisible;
+        const unsigned capacity = p == 0 ? entries : cap;
+        if (!(p == 0 && first_counted))
+            launch_radix_count(keys_in, p == 0, count, entries, capacity, p * kDepthBits, kDepthBits,
+                               count_matrix(A, p), ctrl, st);
+        const bool last = p == kDepthPasses - 1;
+        launch_radix_scatter(keys_in, p == 0 ? nullptr : A.vis_idx[src].p, last ? nullptr : A.vis_key[dst].p,
+                             A.vis_idx[dst].p, p == 0, count, entries, capacity, p * kDepthBits, kDepthBits,
+                             count_matrix(A, p), totals, last ? first_tile.counts : nullptr,
+                             last && expand_counts ? tile_spans << tile_bits[0] : 0u, ctrl, st);
+    }
+    const int sorted = (kDepthPasses - 1) & 1;
+    const DupBuffers dup{A.offs.p, keep_rank ? A.rank.p : nullptr, A.rect_sorted.p, A.chunk_start.p, A.span_sum.p};
+    launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, dup, A.pair_key[0].p,
+                     A.pair_val[0].p, st, first_tile);
+    for (int t = 0, shift = 0; t < tile_passes; shift += tile_bits[t], ++t) {
+        const int q = kDepthPasses + t;
+        const int src = t & 1, dst = src ^ 1;
+        if (!(t == 0 && expand_counts))
+            launch_radix_count(A.pair_key[src].p, false, SortCount::kPairs, 0u, A.pair_cap, shift, tile_bits[t],
+                               count_matrix(A, q), ctrl, st);
+        launch_radix_scatter(A.pair_key[src].p, A.pair_val[src].p, A.pair_key[dst].p, A.pair_val[dst].p, false,
+                             SortCount::kPairs, 0u, A.pair_cap, shift, tile_bits[t], count_matrix(A, q), totals,
+                             nullptr, 0u, ctrl, st);
+    }
+    const int fin = tile_passes & 1;
     launch_ranges(A.pair_key[fin].p, ctrl, A.pair_cap, A.ranges.p, st);
     *final_buf = fin;
     return 0;
@@ -380,14 +446,16 @@ struct Slot {
 };
 
 void launch_preprocess_any(const BatchScene<SceneView>* sc, const Plan<SceneView>& P, const ViewInfo* views, Arena& A,
-                           const DebugProjection* dbg, cudaStream_t st) {
+                           const DebugProjection* dbg, const PassCounts& counts, cudaStream_t st) {
     launch_preprocess(sc, static_cast<unsigned>(P.scenes.size()), P.pre_blocks, views, P.rendered_degree(),
-                      P.shape.tile_w, P.shape.tile_h, A.rec.p, A.rect16.p, A.depth_key.p, dbg, st);
+                      P.shape.tile_w, P.shape.tile_h, A.rec.p, A.rect16.p, A.depth_key.p, dbg, counts,
+                      static_cast<unsigned>(P.entries), st);
 }
 void launch_preprocess_any(const BatchScene<RawParams>* sc, const Plan<RawParams>& P, const ViewInfo* views,
-                           Arena& A, const DebugProjection*, cudaStream_t st) {
+                           Arena& A, const DebugProjection*, const PassCounts& counts, cudaStream_t st) {
     launch_preprocess_raw(sc, static_cast<unsigned>(P.scenes.size()), P.pre_blocks, views, P.rendered_degree(),
-                          P.shape.tile_w, P.shape.tile_h, A.rec.p, A.rect16.p, A.depth_key.p, st);
+                          P.shape.tile_w, P.shape.tile_h, A.rec.p, A.rect16.p, A.depth_key.p, counts,
+                          static_cast<unsigned>(P.entries), st);
 }
 
 // Enqueues one frame of a plan. ev (4 events, may be NULL) brackets the stages.
@@ -398,13 +466,16 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     const BatchScene<Src>* scenes = nullptr;
     BatchTables tables;
     AB_TRY(slot.fill(P, st, &views, &scenes, tables));
+    AB_TRY(clear_ranges(A, static_cast<unsigned>(P.tiles), st));
     if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
-    launch_frame_begin(A.ctrl.p, st);
-    launch_preprocess_any(scenes, P, views, A, dbg, st);
+    unsigned zero_words = 0;
+    const PassCounts first = first_pass_counts(A, static_cast<unsigned>(P.entries), &zero_words);
+    launch_frame_begin(A.ctrl.p, first.counts, zero_words, st);
+    launch_preprocess_any(scenes, P, views, A, dbg, first, st);
     if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
     int fin = 0;
     AB_TRY(enqueue_sort(A, static_cast<unsigned>(P.entries), static_cast<unsigned>(P.tiles), tables, train,
-                        P.shape.radix_bits, st, &fin));
+                        P.shape.radix_bits, first.counts != nullptr, st, &fin));
     if (ev) AB_CUDA(cudaEventRecord(ev[2], st));
     if (!stop_after_sort)
         launch_blend(static_cast<unsigned>(P.tiles), A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, views, tables,
@@ -456,6 +527,18 @@ constexpr int kSlots = 8;
 namespace ab2 {
 // For entry points defined in other files: sets the aniso_b200_last_error message, returns code.
 int report_error(int code, const char* msg) { return fail(code, msg); }
+
+static thread_local uint64_t t_chained_launches = 0;
+uint64_t chained_launches() { return t_chained_launches; }
+void note_chained_launch() { ++t_chained_launches; }
+
+bool chain_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("ANISO_B200_CHAIN");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
 }  // namespace ab2
 
 // ---- scenes ------------------------------------------------------------------------------------
@@ -476,6 +559,7 @@ struct aniso_b200_scene {
     bool profiling = false;
     std::vector<cudaEvent_t> prof_ev;
     size_t prof_frames = 0;
+    int32_t frame_kernels = 0;  // kernels the last frame launched
 
     SceneView view() const {
         SceneView v;
@@ -886,8 +970,10 @@ int aniso_b200_render(aniso_b200_scene* s, const aniso_b200_camera* camera, cons
     AB_TRY(s->image.reserve(bytes));
     P.views[0].rgb8 = s->image.p;
     for (int attempt = 0; attempt < 3; ++attempt) {
+        const uint64_t k0 = chained_launches();
         AB_TRY(enqueue_plan(s->arena, s->slot(), P, s->stream, stats ? s->ev : nullptr, nullptr, false, false,
                             nullptr));
+        s->frame_kernels = static_cast<int32_t>(chained_launches() - k0);
         AB_CUDA(cudaMemcpyAsync(rgb_host, s->image.p, bytes, cudaMemcpyDeviceToHost, s->stream));
         AB_TRY(read_ctrl(s->arena, s->host_ctrl, s->stream));
         int again = 0;
@@ -925,7 +1011,16 @@ int aniso_b200_render_device(aniso_b200_scene* s, const aniso_b200_camera* camer
         ev = &s->prof_ev[4 * s->prof_frames++];
     }
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    return enqueue_plan(s->arena, s->slot(), P, st, ev, nullptr, false, false, nullptr);
+    const uint64_t k0 = chained_launches();
+    const int rc = enqueue_plan(s->arena, s->slot(), P, st, ev, nullptr, false, false, nullptr);
+    s->frame_kernels = static_cast<int32_t>(chained_launches() - k0);
+    return rc;
+}
+
+int aniso_b200_frame_kernels(aniso_b200_scene* s, int32_t* kernels) {
+    if (!s || !kernels) return fail(ANISO_B200_ERR_ARGUMENT, "scene/kernels is NULL");
+    *kernels = s->frame_kernels;
+    return ANISO_B200_OK;
 }
 
 int aniso_b200_profile(aniso_b200_scene* s, int32_t enable) {
@@ -1003,7 +1098,7 @@ int aniso_b200_debug_projection(aniso_b200_scene* s, const aniso_b200_camera* ca
     Slot& slot = s->slot();
     AB_TRY(slot.fill(P, s->stream, &views, &scenes, tables));
     launch_frame_begin(A.ctrl.p, s->stream);
-    launch_preprocess_any(scenes, P, views, A, &dbg, s->stream);
+    launch_preprocess_any(scenes, P, views, A, &dbg, PassCounts{}, s->stream);
     AB_TRY(slot.mark(s->stream));
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaStreamSynchronize(s->stream));
@@ -1073,11 +1168,12 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     }
     cudaStream_t st = nullptr;
     const BatchTables tables{dtab.p, dtab.p + 1, dtab.p + 2, 1u};
+    const unsigned T = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
+    AB_TRY(clear_ranges(A, T, st));
     launch_frame_begin(A.ctrl.p, st);
     launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.depth_key.p, A.rect16.p, st);
     int fin = 0;
-    const unsigned T = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
-    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, kRadixBits, st, &fin));
+    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, kRadixBits, false, st, &fin));
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaDeviceSynchronize());
     Ctrl h;

@@ -20,18 +20,24 @@ struct DebugProjection {
     unsigned* tiles_touched = nullptr;
 };
 
-// Clears the frame's control block (counts and flags; the flags are folded into the sticky ones).
+// Clears the frame's control block (counts and flags; the flags are folded into the sticky ones),
+// and `zero_words` words at `zero` (the first LSD pass's digit counts, which the preprocess adds to).
 void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
+void launch_frame_begin(Ctrl* ctrl, unsigned* zero, unsigned zero_words, cudaStream_t stream);
 
 // Projection of every (view, Gaussian) entry of a batch; `blocks` = sum over scenes of
-// ceil(n / 256) (scene s starts at block scenes[s].block_base).
+// ceil(n / 256) (scene s starts at block scenes[s].block_base). counts.counts set: each visible
+// entry's depth key is also added to the digit counts of the first depth pass, whose items are the
+// `entries` depth keys in entry order.
 void launch_preprocess(const BatchScene<SceneView>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
                        int sh_degree, int tile_w, int tile_h, SplatRecord* rec, unsigned long long* rect16,
-                       unsigned* depth_key, const DebugProjection* dbg, cudaStream_t stream);
+                       unsigned* depth_key, const DebugProjection* dbg, const PassCounts& counts, unsigned entries,
+                       cudaStream_t stream);
 // The same projection of the optimizer's raw tensors (activated in the kernel).
 void launch_preprocess_raw(const BatchScene<RawParams>* scenes, unsigned n_scenes, unsigned blocks,
                            const ViewInfo* views, int sh_degree, int tile_w, int tile_h, SplatRecord* rec,
-                           unsigned long long* rect16, unsigned* depth_key, cudaStream_t stream);
+                           unsigned long long* rect16, unsigned* depth_key, const PassCounts& counts,
+                           unsigned entries, cudaStream_t stream);
 
 // Where a sort pass finds its item count: a host value, the visible count the first depth pass
 // publishes, or the frame's pair total.
@@ -47,10 +53,25 @@ bool radix_bits_supported(int bits);
 void launch_radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
                        bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, int bits,
                        unsigned* scratch, Ctrl* ctrl, cudaStream_t stream);
+// The same pass in two parts, for passes whose digit counts the key producer accumulates
+// (PassCounts, common.cuh): launch_radix_count is the upsweep alone (writes every (digit, span)
+// cell of `counts`); launch_radix_scatter the span scan and the downsweep over counts that are
+// complete. The span scan also clears `zero_words` words at `zero` (a later pass's counts, which
+// a producer accumulates). One count matrix is sort_count_words() words; the pass's span count is
+// sort_spans(capacity or fixed).
+size_t sort_count_words();
+unsigned sort_spans(uint64_t max_items);
+void launch_radix_count(const unsigned* keys_in, bool masked, SortCount src, unsigned fixed, unsigned capacity,
+                        int shift, int bits, unsigned* counts, Ctrl* ctrl, cudaStream_t stream);
+void launch_radix_scatter(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
+                          bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, int bits,
+                          unsigned* counts, unsigned* totals, unsigned* zero, unsigned zero_words, Ctrl* ctrl,
+                          cudaStream_t stream);
 
 // Expands the depth-sorted visible list into (tile, entry) pairs in depth order; sets kFlagOverflow
 // (and writes no pairs) if they exceed capacity. Three kernels: per-span pair counts, pair offsets,
-// and an expansion with a fixed number of pairs per CTA.
+// and an expansion with a fixed number of pairs per CTA, which with first.counts set also adds the
+// pairs' tile keys to the first tile pass's digit counts (cleared beforehand).
 struct DupBuffers {
     unsigned* offs;                   // [N] exclusive pair offset of each depth-sorted entry
     unsigned* rank;                   // [N] depth-sorted position of each visible entry (or NULL)
@@ -62,7 +83,7 @@ size_t sort_span_sums();
 unsigned expand_chunk_pairs();
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
                       unsigned max_visible, const BatchTables& tables, const DupBuffers& buf, unsigned* pair_key,
-                      unsigned* pair_val, cudaStream_t stream);
+                      unsigned* pair_val, cudaStream_t stream, const PassCounts& first = PassCounts{});
 
 // ranges[tile] = [start, end) over the sorted tile keys (gpu_render.cu:164-177); ranges must be
 // zeroed before.

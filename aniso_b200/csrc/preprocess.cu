@@ -217,7 +217,9 @@ __global__ void __launch_bounds__(256, 3) preprocess_kernel(const BatchScene<Src
                                                             unsigned n_scenes, const ViewInfo* __restrict__ views,
                                                             int tile_w, int tile_h, SplatRecord* __restrict__ rec,
                                                             unsigned long long* __restrict__ rect16,
-                                                            unsigned* __restrict__ depth_key, DebugProjection dbg) {
+                                                            unsigned* __restrict__ depth_key, DebugProjection dbg,
+                                                            PassCounts counts, unsigned entries) {
+    chain_entry();
     __shared__ CamParams s_cam[kMaxStagedViews];
     __shared__ unsigned s_scene;
     const int tid = threadIdx.x;
@@ -290,6 +292,7 @@ __global__ void __launch_bounds__(256, 3) preprocess_kernel(const BatchScene<Src
             // kCulledKey never collides. The first depth pass compacts the visible entries.
             const unsigned depth_bits = __float_as_uint(p.depth);
             depth_key[e] = depth_bits;
+            if (counts.counts) count_key(counts, (entries + kSortBlockItems - 1) / kSortBlockItems, e, depth_bits);
             if (kDebug) {
                 dbg.uv[e] = make_float2(p.u, p.v);
                 dbg.conic_opacity[e] = make_float4(p.conicA, p.conicB, p.conicC, opacity);
@@ -308,13 +311,18 @@ template <bool kDebug, class Src>
 void launch_preprocess_t(const BatchScene<Src>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
                          int sh_degree, int tile_w, int tile_h, SplatRecord* rec,
                          unsigned long long* rect16, unsigned* depth_key, const DebugProjection& dbg,
-                         cudaStream_t stream) {
+                         const PassCounts& counts, unsigned entries, cudaStream_t stream) {
     if (blocks == 0) return;
+    const dim3 grid(blocks), block(256);
     switch (sh_degree) {
-        case 0: preprocess_kernel<0, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, rec, rect16, depth_key, dbg); break;
-        case 1: preprocess_kernel<1, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, rec, rect16, depth_key, dbg); break;
-        case 2: preprocess_kernel<2, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, rec, rect16, depth_key, dbg); break;
-        default: preprocess_kernel<3, kDebug, Src><<<blocks, 256, 0, stream>>>(scenes, n_scenes, views, tile_w, tile_h, rec, rect16, depth_key, dbg); break;
+        case 0: launch_chained(preprocess_kernel<0, kDebug, Src>, grid, block, stream, scenes, n_scenes, views, tile_w,
+                               tile_h, rec, rect16, depth_key, dbg, counts, entries); break;
+        case 1: launch_chained(preprocess_kernel<1, kDebug, Src>, grid, block, stream, scenes, n_scenes, views, tile_w,
+                               tile_h, rec, rect16, depth_key, dbg, counts, entries); break;
+        case 2: launch_chained(preprocess_kernel<2, kDebug, Src>, grid, block, stream, scenes, n_scenes, views, tile_w,
+                               tile_h, rec, rect16, depth_key, dbg, counts, entries); break;
+        default: launch_chained(preprocess_kernel<3, kDebug, Src>, grid, block, stream, scenes, n_scenes, views, tile_w,
+                                tile_h, rec, rect16, depth_key, dbg, counts, entries); break;
     }
 }
 
@@ -322,20 +330,22 @@ void launch_preprocess_t(const BatchScene<Src>* scenes, unsigned n_scenes, unsig
 
 void launch_preprocess(const BatchScene<SceneView>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
                        int sh_degree, int tile_w, int tile_h, SplatRecord* rec, unsigned long long* rect16,
-                       unsigned* depth_key, const DebugProjection* dbg, cudaStream_t stream) {
+                       unsigned* depth_key, const DebugProjection* dbg, const PassCounts& counts, unsigned entries,
+                       cudaStream_t stream) {
     if (dbg)
         launch_preprocess_t<true>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, rec, rect16,
-                                  depth_key, *dbg, stream);
+                                  depth_key, *dbg, counts, entries, stream);
     else
         launch_preprocess_t<false>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, rec, rect16,
-                                   depth_key, DebugProjection{}, stream);
+                                   depth_key, DebugProjection{}, counts, entries, stream);
 }
 
 void launch_preprocess_raw(const BatchScene<RawParams>* scenes, unsigned n_scenes, unsigned blocks,
                            const ViewInfo* views, int sh_degree, int tile_w, int tile_h, SplatRecord* rec,
-                           unsigned long long* rect16, unsigned* depth_key, cudaStream_t stream) {
+                           unsigned long long* rect16, unsigned* depth_key, const PassCounts& counts,
+                           unsigned entries, cudaStream_t stream) {
     launch_preprocess_t<false>(scenes, n_scenes, blocks, views, sh_degree, tile_w, tile_h, rec, rect16,
-                               depth_key, DebugProjection{}, stream);
+                               depth_key, DebugProjection{}, counts, entries, stream);
 }
 
 }  // namespace ab2

@@ -41,13 +41,20 @@ constexpr int kScanItems = 4;
 constexpr int kScanBlock = kThreads * kScanItems;
 constexpr int kExpandItems = 8;
 constexpr int kExpandChunk = kThreads * kExpandItems;  // pairs per expansion CTA
+static_assert(kBlockItems == kSortBlockItems, "an LSD block is kSortBlockItems items");
+static_assert(kExpandChunk == kSortBlockItems, "an expansion CTA writes exactly one LSD block of pairs");
 
-__global__ void frame_begin_kernel(Ctrl* ctrl) {
-    ctrl->sticky_flags |= ctrl->flags;
-    if (ctrl->pair_total > ctrl->max_pair_total) ctrl->max_pair_total = ctrl->pair_total;
-    ctrl->pair_total = 0;
-    ctrl->vis_count = 0;
-    ctrl->flags = 0;
+// Clears the control block and `zero_words` words at `zero` (the first pass's digit counts).
+__global__ void frame_begin_kernel(Ctrl* ctrl, unsigned* __restrict__ zero, unsigned zero_words) {
+    chain_entry();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctrl->sticky_flags |= ctrl->flags;
+        if (ctrl->pair_total > ctrl->max_pair_total) ctrl->max_pair_total = ctrl->pair_total;
+        ctrl->pair_total = 0;
+        ctrl->vis_count = 0;
+        ctrl->flags = 0;
+    }
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < zero_words; i += gridDim.x * blockDim.x) zero[i] = 0;
 }
 
 // Items of this frame's pass; false when the frame overflowed (nothing after duplication runs).
@@ -103,20 +110,22 @@ __global__ void __launch_bounds__(kThreads) upsweep_kernel(const unsigned* __res
                                                            unsigned fixed, unsigned capacity, int shift,
                                                            unsigned spans, unsigned* __restrict__ counts,
                                                            const Ctrl* __restrict__ ctrl) {
+    chain_entry();
     constexpr int R = 1 << BITS;
     __shared__ unsigned s_h[kWarps][R];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned n;
     if (!pass_items(ctrl, src, fixed, capacity, n)) return;
+    unsigned t0, t1;
+    span_blocks(n, spans, blockIdx.x, t0, t1);
+    unsigned key[kItems], val[kItems], dg[kItems];
+    if (t0 < t1) load_block<R, kMasked, false>(keys_in, nullptr, t0, n, shift, warp, lane, key, val, dg);
     for (int d = tid; d < R; d += kThreads)
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) s_h[w][d] = 0;
     __syncthreads();
-    unsigned t0, t1;
-    span_blocks(n, spans, blockIdx.x, t0, t1);
     for (unsigned t = t0; t < t1; ++t) {
-        unsigned key[kItems], val[kItems], dg[kItems];
-        load_block<R, kMasked, false>(keys_in, nullptr, t, n, shift, warp, lane, key, val, dg);
+        if (t != t0) load_block<R, kMasked, false>(keys_in, nullptr, t, n, shift, warp, lane, key, val, dg);
 #pragma unroll
         for (int k = 0; k < kItems; ++k)
             if (dg[k] < R) atomicAdd(&s_h[warp][dg[k]], 1u);
@@ -131,10 +140,15 @@ __global__ void __launch_bounds__(kThreads) upsweep_kernel(const unsigned* __res
 }
 
 // One CTA per digit: exclusive scan of the digit's counts over the spans, in place, and its total.
+// All CTAs together also clear `zero_words` words at `zero`: the next pass's counts, which the
+// downsweep after this kernel accumulates (their previous reader, the downsweep before, is done).
 __global__ void __launch_bounds__(kThreads) span_scan_kernel(unsigned* __restrict__ counts, unsigned* __restrict__ totals,
                                                              unsigned spans, SortCount src, unsigned fixed,
-                                                             unsigned capacity, const Ctrl* __restrict__ ctrl) {
+                                                             unsigned capacity, const Ctrl* __restrict__ ctrl,
+                                                             unsigned* __restrict__ zero, unsigned zero_words) {
+    chain_entry();
     __shared__ unsigned s_tmp[kWarps];
+    for (unsigned i = blockIdx.x * kThreads + threadIdx.x; i < zero_words; i += gridDim.x * kThreads) zero[i] = 0;
     unsigned n;
     if (!pass_items(ctrl, src, fixed, capacity, n)) return;
     unsigned* row = counts + static_cast<size_t>(blockIdx.x) * spans;
@@ -152,15 +166,17 @@ __global__ void __launch_bounds__(kThreads) span_scan_kernel(unsigned* __restric
 
 // Ranks, scatters and writes each block of the span. The masked pass publishes the visible count.
 // Thread tid owns digits [tid * DPT, tid * DPT + DPT) in the per-digit phases, so a block scan over
-// the threads' sums is a scan in digit order.
+// the threads' sums is a scan in digit order. Four CTAs per SM (64 registers) keep all
+// kMaxSpans = 4 x 148 spans of a large pass resident in one wave.
 template <int BITS, bool kMasked, bool kKeysOut>
-__global__ void __launch_bounds__(kThreads) downsweep_kernel(const unsigned* __restrict__ keys_in,
-                                                             const unsigned* __restrict__ vals_in,
-                                                             unsigned* __restrict__ keys_out,
-                                                             unsigned* __restrict__ vals_out, SortCount src,
-                                                             unsigned fixed, unsigned capacity, int shift,
-                                                             unsigned spans, const unsigned* __restrict__ counts,
-                                                             const unsigned* __restrict__ totals, Ctrl* ctrl) {
+__global__ void __launch_bounds__(kThreads, 4) downsweep_kernel(const unsigned* __restrict__ keys_in,
+                                                                const unsigned* __restrict__ vals_in,
+                                                                unsigned* __restrict__ keys_out,
+                                                                unsigned* __restrict__ vals_out, SortCount src,
+                                                                unsigned fixed, unsigned capacity, int shift,
+                                                                unsigned spans, const unsigned* __restrict__ counts,
+                                                                const unsigned* __restrict__ totals, Ctrl* ctrl) {
+    chain_entry();
     constexpr int R = 1 << BITS;
     constexpr int DPT = R / kThreads;  // digits per thread: 1 (8-bit digits) or 2 (9-bit)
     static_assert(DPT * kThreads == R, "digit count must be a multiple of the block size");
@@ -174,6 +190,9 @@ __global__ void __launch_bounds__(kThreads) downsweep_kernel(const unsigned* __r
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned n;
     if (!pass_items(ctrl, src, fixed, capacity, n)) return;
+    unsigned t0, t1;
+    span_blocks(n, spans, blockIdx.x, t0, t1);
+    if (t0 == t1 && !(kMasked && blockIdx.x == 0)) return;  // an empty span (span 0 publishes the count)
     const int d0 = tid * DPT;
     unsigned run[DPT];  // next global output position of each of this thread's digits
     {
@@ -192,8 +211,6 @@ __global__ void __launch_bounds__(kThreads) downsweep_kernel(const unsigned* __r
             g += tot[j];
         }
     }
-    unsigned t0, t1;
-    span_blocks(n, spans, blockIdx.x, t0, t1);
     const unsigned lt = lanemask_lt();
 
     for (unsigned t = t0; t < t1; ++t) {
@@ -286,6 +303,7 @@ __global__ void __launch_bounds__(kThreads) pair_count_kernel(const unsigned* __
                                                               unsigned* __restrict__ rank,
                                                               unsigned long long* __restrict__ rect_sorted,
                                                               unsigned long long* __restrict__ span_sum) {
+    chain_entry();
     __shared__ unsigned long long s_tmp[kWarps];
     const unsigned long long V = ctrl->vis_count;
     const unsigned lo = static_cast<unsigned>(V * blockIdx.x / spans);
@@ -326,6 +344,7 @@ __global__ void __launch_bounds__(kThreads) pair_offsets_kernel(const unsigned l
                                                                 const unsigned long long* __restrict__ span_sum,
                                                                 unsigned* __restrict__ offs,
                                                                 unsigned* __restrict__ chunk_start) {
+    chain_entry();
     __shared__ unsigned long long s_tmp64[kWarps];
     __shared__ unsigned s_tmp[kWarps];
     const unsigned b = blockIdx.x;
@@ -369,50 +388,13 @@ __global__ void __launch_bounds__(kThreads) pair_offsets_kernel(const unsigned l
     }
 }
 
-// Expands the depth-sorted list into (tile, entry) pairs: CTA b writes pairs
-// [b * kExpandChunk, (b + 1) * kExpandChunk), each thread kExpandItems consecutive ones (one
-// search for its first pair, then a walk), row-major over each rectangle as gpu_render.cu:155-160
-// does. Tile ids are global over the batch.
-__global__ void __launch_bounds__(kThreads) expand_kernel(const unsigned* __restrict__ sorted_idx,
-                                                          const unsigned long long* __restrict__ rect_sorted,
-                                                          const unsigned* __restrict__ offs,
-                                                          const unsigned* __restrict__ chunk_start,
-                                                          const Ctrl* __restrict__ ctrl, unsigned capacity,
-                                                          BatchTables tables, unsigned* __restrict__ pair_key,
-                                                          unsigned* __restrict__ pair_val) {
-    __shared__ unsigned s_off[kExpandChunk + 2];
-    __shared__ unsigned s_idx[kExpandChunk + 1];
-    __shared__ unsigned s_org[kExpandChunk + 1];       // global tile of the rectangle's corner
-    __shared__ unsigned short s_w[kExpandChunk + 1];   // rectangle width in tiles
-    __shared__ unsigned short s_tx[kExpandChunk + 1];  // tiles per row of the entry's view
-    const int tid = threadIdx.x;
-    if (ctrl->flags & kFlagOverflow) return;
-    const unsigned long long P64 = ctrl->pair_total;
-    if (P64 > capacity) return;
-    const unsigned P = static_cast<unsigned>(P64);
-    const unsigned base = blockIdx.x * kExpandChunk;
-    if (base >= P) return;
-    const unsigned V = ctrl->vis_count;
-    const unsigned j0 = chunk_start[blockIdx.x];
-    const unsigned j1 = base + kExpandChunk < P ? chunk_start[blockIdx.x + 1] : V - 1;
-    const unsigned G = j1 - j0 + 1;  // <= kExpandChunk + 1: every entry owns at least one pair
-    for (unsigned k = tid; k < G; k += kThreads) {
-        const unsigned long long r = rect_sorted[j0 + k];
-        const unsigned e = sorted_idx[j0 + k];
-        const unsigned v = find_segment(tables.entry_base, tables.n_views, e);
-        const unsigned tx = tables.tiles_x[v];
-        const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu;
-        s_off[k] = offs[j0 + k];
-        s_idx[k] = e;
-        s_org[k] = tables.tile_base[v] + y0 * tx + x0;
-        s_w[k] = static_cast<unsigned short>(x1 - x0 + 1);
-        s_tx[k] = static_cast<unsigned short>(tx);
-    }
-    if (tid == 0) s_off[G] = j1 + 1 < V ? offs[j1 + 1] : P;
-    __syncthreads();
-
-    const unsigned p0 = base + tid * kExpandItems;
-    if (p0 >= P) return;
+// The kExpandItems pairs from position p0 (< P) of one expansion CTA (the CTA's entries staged in
+// shared memory); hist: also counts each pair's digit there.
+__device__ __forceinline__ void expand_run(unsigned p0, unsigned P, unsigned G, const unsigned* s_off,
+                                           const unsigned* s_idx, const unsigned* s_org, const unsigned short* s_w,
+                                           const unsigned short* s_tx, unsigned* __restrict__ pair_key,
+                                           unsigned* __restrict__ pair_val, unsigned* hist, unsigned shift,
+                                           unsigned mask) {
     unsigned lo = 0, hi = G - 1;  // last k with s_off[k] <= p0
     while (lo < hi) {
         const unsigned mid = (lo + hi + 1) >> 1;
@@ -457,12 +439,76 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(const unsigned* __rest
                 pair_val[p0 + i] = val[i];
             }
     }
+    if (hist)
+#pragma unroll
+        for (int i = 0; i < kExpandItems; ++i)
+            if (p0 + i < P) atomicAdd(&hist[(key[i] >> shift) & mask], 1u);
+}
+
+// Expands the depth-sorted list into (tile, entry) pairs: CTA b writes pairs
+// [b * kExpandChunk, (b + 1) * kExpandChunk), each thread kExpandItems consecutive ones (one
+// search for its first pair, then a walk), row-major over each rectangle as gpu_render.cu:155-160
+// does. Tile ids are global over the batch. With first.counts set, the CTA also adds its pairs'
+// digits to the first tile pass's counts: its pairs are exactly LSD block b, all in one span, so
+// it counts them in shared memory and adds each non-zero digit count once.
+__global__ void __launch_bounds__(kThreads) expand_kernel(const unsigned* __restrict__ sorted_idx,
+                                                          const unsigned long long* __restrict__ rect_sorted,
+                                                          const unsigned* __restrict__ offs,
+                                                          const unsigned* __restrict__ chunk_start,
+                                                          const Ctrl* __restrict__ ctrl, unsigned capacity,
+                                                          BatchTables tables, unsigned* __restrict__ pair_key,
+                                                          unsigned* __restrict__ pair_val, PassCounts first) {
+    chain_entry();
+    __shared__ unsigned s_off[kExpandChunk + 2];
+    __shared__ unsigned s_idx[kExpandChunk + 1];
+    __shared__ unsigned s_org[kExpandChunk + 1];       // global tile of the rectangle's corner
+    __shared__ unsigned short s_w[kExpandChunk + 1];   // rectangle width in tiles
+    __shared__ unsigned short s_tx[kExpandChunk + 1];  // tiles per row of the entry's view
+    __shared__ unsigned s_hist[1 << kMaxRadixBits];
+    const int tid = threadIdx.x;
+    if (ctrl->flags & kFlagOverflow) return;
+    const unsigned long long P64 = ctrl->pair_total;
+    if (P64 > capacity) return;
+    const unsigned P = static_cast<unsigned>(P64);
+    const unsigned base = blockIdx.x * kExpandChunk;
+    if (base >= P) return;
+    const unsigned V = ctrl->vis_count;
+    const unsigned j0 = chunk_start[blockIdx.x];
+    const unsigned j1 = base + kExpandChunk < P ? chunk_start[blockIdx.x + 1] : V - 1;
+    const unsigned G = j1 - j0 + 1;  // <= kExpandChunk + 1: every entry owns at least one pair
+    for (unsigned k = tid; k < G; k += kThreads) {
+        const unsigned long long r = rect_sorted[j0 + k];
+        const unsigned e = sorted_idx[j0 + k];
+        const unsigned v = find_segment(tables.entry_base, tables.n_views, e);
+        const unsigned tx = tables.tiles_x[v];
+        const unsigned x0 = r & 0xFFFFu, y0 = (r >> 16) & 0xFFFFu, x1 = (r >> 32) & 0xFFFFu;
+        s_off[k] = offs[j0 + k];
+        s_idx[k] = e;
+        s_org[k] = tables.tile_base[v] + y0 * tx + x0;
+        s_w[k] = static_cast<unsigned short>(x1 - x0 + 1);
+        s_tx[k] = static_cast<unsigned short>(tx);
+    }
+    if (tid == 0) s_off[G] = j1 + 1 < V ? offs[j1 + 1] : P;
+    const bool count = first.counts != nullptr;
+    if (count)
+        for (unsigned d = tid; d <= first.mask; d += kThreads) s_hist[d] = 0;
+    __syncthreads();
+
+    const unsigned p0 = base + tid * kExpandItems;
+    if (p0 < P) expand_run(p0, P, G, s_off, s_idx, s_org, s_w, s_tx, pair_key, pair_val, count ? s_hist : nullptr,
+                           first.shift, first.mask);
+    if (!count) return;
+    __syncthreads();
+    const unsigned span = span_of(base, first.spans, (P + kSortBlockItems - 1) / kSortBlockItems);
+    for (unsigned d = tid; d <= first.mask; d += kThreads)
+        if (s_hist[d]) atomicAdd(&first.counts[d * first.spans + span], s_hist[d]);
 }
 
 // ranges[tile] = [first, last + 1) over the sorted tile keys; four keys per thread and step.
 __global__ void __launch_bounds__(kThreads) ranges_kernel(const unsigned* __restrict__ keys,
                                                           const Ctrl* __restrict__ ctrl, unsigned capacity,
                                                           uint2* __restrict__ ranges) {
+    chain_entry();
     if (ctrl->flags & kFlagOverflow) return;
     const unsigned long long pt = ctrl->pair_total;
     if (pt > capacity) return;
@@ -506,6 +552,7 @@ __global__ void __launch_bounds__(kThreads) projection_keys_kernel(int64_t n, co
                                                                    const uint4* __restrict__ rect,
                                                                    unsigned* __restrict__ depth_key,
                                                                    unsigned long long* __restrict__ rect16) {
+    chain_entry();
     const int64_t i = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
     if (i >= n) return;
     unsigned key = kCulledKey;
@@ -525,79 +572,111 @@ unsigned spans_for(uint64_t max_items) {
 
 }  // namespace
 
-void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream) { frame_begin_kernel<<<1, 1, 0, stream>>>(ctrl); }
+void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream) {
+    launch_chained(frame_begin_kernel, dim3(1), dim3(1), stream, ctrl, static_cast<unsigned*>(nullptr), 0u);
+}
+
+void launch_frame_begin(Ctrl* ctrl, unsigned* zero, unsigned zero_words, cudaStream_t stream) {
+    const unsigned blocks = std::max(1u, std::min((zero_words + kThreads * 4 - 1) / (kThreads * 4), 148u));
+    launch_chained(frame_begin_kernel, dim3(blocks), dim3(kThreads), stream, ctrl, zero, zero_words);
+}
 
 size_t sort_scratch_words() { return static_cast<size_t>(1 << kMaxRadixBits) * (kMaxSpans + 1); }
+size_t sort_count_words() { return static_cast<size_t>(1 << kMaxRadixBits) * kMaxSpans; }
 size_t sort_span_sums() { return kMaxSpans; }
+unsigned sort_spans(uint64_t max_items) { return spans_for(max_items); }
 unsigned expand_chunk_pairs() { return kExpandChunk; }
 bool radix_bits_supported(int bits) { return bits == 8 || bits == 9; }
 
 namespace {
 template <int BITS>
-void radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out, bool masked,
-                SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned* scratch, Ctrl* ctrl,
-                cudaStream_t stream) {
+void count_pass(const unsigned* keys_in, bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift,
+                unsigned* counts, Ctrl* ctrl, cudaStream_t stream) {
+    const unsigned spans = spans_for(src == SortCount::kFixed ? fixed : capacity);
+    const dim3 grid(spans), block(kThreads);
+    if (masked)
+        launch_chained(upsweep_kernel<BITS, true>, grid, block, stream, keys_in, src, fixed, capacity, shift, spans,
+                       counts, ctrl);
+    else
+        launch_chained(upsweep_kernel<BITS, false>, grid, block, stream, keys_in, src, fixed, capacity, shift, spans,
+                       counts, ctrl);
+}
+
+template <int BITS>
+void scatter_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out, bool masked,
+                  SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned* counts, unsigned* totals,
+                  unsigned* zero, unsigned zero_words, Ctrl* ctrl, cudaStream_t stream) {
     constexpr int R = 1 << BITS;
     const unsigned spans = spans_for(src == SortCount::kFixed ? fixed : capacity);
-    unsigned* counts = scratch;
-    unsigned* totals = scratch + static_cast<size_t>(R) * kMaxSpans;
+    const dim3 grid(spans), block(kThreads);
+    launch_chained(span_scan_kernel, dim3(R), block, stream, counts, totals, spans, src, fixed, capacity, ctrl, zero,
+                   zero_words);
     if (masked)
-        upsweep_kernel<BITS, true><<<spans, kThreads, 0, stream>>>(keys_in, src, fixed, capacity, shift, spans, counts,
-                                                                   ctrl);
-    else
-        upsweep_kernel<BITS, false><<<spans, kThreads, 0, stream>>>(keys_in, src, fixed, capacity, shift, spans, counts,
-                                                                    ctrl);
-    span_scan_kernel<<<R, kThreads, 0, stream>>>(counts, totals, spans, src, fixed, capacity, ctrl);
-    if (masked)
-        downsweep_kernel<BITS, true, true><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src,
-                                                                          fixed, capacity, shift, spans, counts, totals,
-                                                                          ctrl);
+        launch_chained(downsweep_kernel<BITS, true, true>, grid, block, stream, keys_in, vals_in, keys_out, vals_out,
+                       src, fixed, capacity, shift, spans, counts, totals, ctrl);
     else if (keys_out)
-        downsweep_kernel<BITS, false, true><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src,
-                                                                           fixed, capacity, shift, spans, counts,
-                                                                           totals, ctrl);
+        launch_chained(downsweep_kernel<BITS, false, true>, grid, block, stream, keys_in, vals_in, keys_out, vals_out,
+                       src, fixed, capacity, shift, spans, counts, totals, ctrl);
     else
-        downsweep_kernel<BITS, false, false><<<spans, kThreads, 0, stream>>>(keys_in, vals_in, keys_out, vals_out, src,
-                                                                            fixed, capacity, shift, spans, counts,
-                                                                            totals, ctrl);
+        launch_chained(downsweep_kernel<BITS, false, false>, grid, block, stream, keys_in, vals_in, keys_out, vals_out,
+                       src, fixed, capacity, shift, spans, counts, totals, ctrl);
 }
 }  // namespace
 
 void launch_radix_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
                        bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, int bits,
                        unsigned* scratch, Ctrl* ctrl, cudaStream_t stream) {
+    unsigned* totals = scratch + sort_count_words();
+    launch_radix_count(keys_in, masked, src, fixed, capacity, shift, bits, scratch, ctrl, stream);
+    launch_radix_scatter(keys_in, vals_in, keys_out, vals_out, masked, src, fixed, capacity, shift, bits, scratch,
+                         totals, nullptr, 0, ctrl, stream);
+}
+
+void launch_radix_count(const unsigned* keys_in, bool masked, SortCount src, unsigned fixed, unsigned capacity,
+                        int shift, int bits, unsigned* counts, Ctrl* ctrl, cudaStream_t stream) {
+    if (bits == 9) count_pass<9>(keys_in, masked, src, fixed, capacity, shift, counts, ctrl, stream);
+    else count_pass<8>(keys_in, masked, src, fixed, capacity, shift, counts, ctrl, stream);
+}
+
+void launch_radix_scatter(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
+                          bool masked, SortCount src, unsigned fixed, unsigned capacity, int shift, int bits,
+                          unsigned* counts, unsigned* totals, unsigned* zero, unsigned zero_words, Ctrl* ctrl,
+                          cudaStream_t stream) {
     if (bits == 9)
-        radix_pass<9>(keys_in, vals_in, keys_out, vals_out, masked, src, fixed, capacity, shift, scratch, ctrl, stream);
+        scatter_pass<9>(keys_in, vals_in, keys_out, vals_out, masked, src, fixed, capacity, shift, counts, totals, zero,
+                        zero_words, ctrl, stream);
     else
-        radix_pass<8>(keys_in, vals_in, keys_out, vals_out, masked, src, fixed, capacity, shift, scratch, ctrl, stream);
+        scatter_pass<8>(keys_in, vals_in, keys_out, vals_out, masked, src, fixed, capacity, shift, counts, totals, zero,
+                        zero_words, ctrl, stream);
 }
 
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
                       unsigned max_visible, const BatchTables& tables, const DupBuffers& buf, unsigned* pair_key,
-                      unsigned* pair_val, cudaStream_t stream) {
+                      unsigned* pair_val, cudaStream_t stream, const PassCounts& first) {
     if (max_visible == 0) return;
     const unsigned spans = spans_for(max_visible);
-    pair_count_kernel<<<spans, kThreads, 0, stream>>>(sorted_idx, rect16, ctrl, spans, buf.rank, buf.rect_sorted,
-                                                      buf.span_sum);
-    pair_offsets_kernel<<<spans, kThreads, 0, stream>>>(buf.rect_sorted, ctrl, spans, capacity, buf.span_sum,
-                                                        buf.offs, buf.chunk_start);
+    launch_chained(pair_count_kernel, dim3(spans), dim3(kThreads), stream, sorted_idx, rect16, ctrl, spans, buf.rank,
+                   buf.rect_sorted, buf.span_sum);
+    launch_chained(pair_offsets_kernel, dim3(spans), dim3(kThreads), stream, buf.rect_sorted, ctrl, spans, capacity,
+                   buf.span_sum, buf.offs, buf.chunk_start);
     const unsigned expand_blocks = (capacity + kExpandChunk - 1) / kExpandChunk;
-    expand_kernel<<<expand_blocks, kThreads, 0, stream>>>(sorted_idx, buf.rect_sorted, buf.offs, buf.chunk_start, ctrl,
-                                                          capacity, tables, pair_key, pair_val);
+    launch_chained(expand_kernel, dim3(expand_blocks), dim3(kThreads), stream, sorted_idx, buf.rect_sorted, buf.offs,
+                   buf.chunk_start, ctrl, capacity, tables, pair_key, pair_val, first);
 }
 
 void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capacity, uint2* ranges,
                    cudaStream_t stream) {
     const unsigned groups = (capacity + 4u * kThreads - 1) / (4u * kThreads);
     const unsigned blocks = std::max(1u, std::min(groups, 148u * 8u));
-    ranges_kernel<<<blocks, kThreads, 0, stream>>>(sorted_keys, ctrl, capacity, ranges);
+    launch_chained(ranges_kernel, dim3(blocks), dim3(kThreads), stream, sorted_keys, ctrl, capacity, ranges);
 }
 
 void launch_projection_keys(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
                             unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream) {
     const unsigned blocks = static_cast<unsigned>((n + kThreads - 1) / kThreads);
     if (blocks == 0) return;
-    projection_keys_kernel<<<blocks, kThreads, 0, stream>>>(n, tiles_touched, depth, rect, depth_key, rect16);
+    launch_chained(projection_keys_kernel, dim3(blocks), dim3(kThreads), stream, n, tiles_touched, depth, rect,
+                   depth_key, rect16);
 }
 
 }  // namespace ab2

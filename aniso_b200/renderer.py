@@ -158,6 +158,12 @@ class GpuRenderer:
         check(lib.aniso_b200_profile_read(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(f)))
         return {"project_ms": a.value, "sort_ms": b.value, "blend_ms": c.value, "frames": f.value}
 
+    def frame_kernels(self) -> int:
+        """Kernels the last render / render_device frame launched (the library's own)."""
+        k = ctypes.c_int32()
+        check(lib.aniso_b200_frame_kernels(self._h, ctypes.byref(k)))
+        return k.value
+
     def sync(self) -> dict:
         st = _lib.Stats()
         check(lib.aniso_b200_sync(self._h, ctypes.byref(st)))

@@ -116,6 +116,11 @@ int aniso_b200_profile(aniso_b200_scene* scene, int32_t enable);
 int aniso_b200_profile_read(aniso_b200_scene* scene, double* project_ms, double* sort_ms, double* blend_ms,
                             int64_t* frames);
 
+/* The number of kernels the scene's last aniso_b200_render / aniso_b200_render_device frame
+ * launched (no counterpart in gpu_render.h): the library's own kernels only, not its memory
+ * copies and clears. 0 before the first frame. */
+int aniso_b200_frame_kernels(aniso_b200_scene* scene, int32_t* kernels);
+
 /* Copies the last error message (NUL-terminated, truncated to len) and returns its full length. */
 size_t aniso_b200_last_error(char* buf, size_t len);
 
