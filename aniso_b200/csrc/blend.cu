@@ -10,7 +10,8 @@
 // B200 mapping (the kernel is FP32-issue bound, so the layout minimises instructions per pixel):
 //   * each warp owns one 8x8 pixel block -- exactly one tile of the CPU renderer -- with two
 //     horizontally adjacent pixels per lane; the row terms of the exponent (with log2(opacity)
-//     folded in) are shared, so each pixel's exponent is two FMAs;
+//     folded in) are shared, and the two pixels' offsets and FMAs are packed FP32x2 instructions
+//     (three for both pixels' exponents);
 //   * the block stages kBatch splat records per round in shared memory and, per splat, a mask of
 //     the warp blocks it can touch: its pixel bounds (the CPU 8x8-tile rectangle cut by the
 //     ellipse where alpha can reach 1/255, with a margin) against each 8x8 block. The 8x8 part
@@ -149,11 +150,11 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
                     const float4 a = s_r0[jj];
                     const float4 k = s_r1[jj];
                     const float bb = s_b[jj];
-                    float p0, p1;
-                    splat_exponents(a, k, __fsub_rn(px0, a.x), __fsub_rn(py, a.y), p0, p1);
+                    float2 dx;
+                    const float2 pp = splat_exponents2(a, k, make_float2(px0, px0 + 1.0f), __fsub_rn(py, a.y), dx);
                     const unsigned pos = base + jj + 1;
-                    blend_px<kTrain>(p0, k.y, k.z, k.w, bb, T0, r0, g0, b0c, tf0, last0, pos);
-                    blend_px<kTrain>(p1, k.y, k.z, k.w, bb, T1, r1, g1, b1c, tf1, last1, pos);
+                    blend_px<kTrain>(pp.x, k.y, k.z, k.w, bb, T0, r0, g0, b0c, tf0, last0, pos);
+                    blend_px<kTrain>(pp.y, k.y, k.z, k.w, bb, T1, r1, g1, b1c, tf1, last1, pos);
                 }
                 if (!__any_sync(0xFFFFFFFFu, T0 + T1 > 0.f)) {
                     warp_done = true;

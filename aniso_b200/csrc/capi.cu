@@ -351,7 +351,7 @@ struct Plan {
             scenes[s].view_begin = first[s] < 0 ? 0u : static_cast<unsigned>(first[s]);
             scenes[s].view_end = first[s] < 0 ? 0u : static_cast<unsigned>(last[s] + 1);
             scenes[s].block_base = pre_blocks;
-            if (first[s] >= 0) pre_blocks += chunks_of(static_cast<uint64_t>(srcs[s].n), 256);
+            if (first[s] >= 0) pre_blocks += chunks_of(static_cast<uint64_t>(srcs[s].n), preprocess_gaussians_per_block());
         }
         return 0;
     }

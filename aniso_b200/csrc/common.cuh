@@ -262,17 +262,21 @@ struct SplatRecord {
     float4 r0, r1, r2;
 };
 
-// The base-2 exponents of a splat at two horizontally adjacent pixel centres (dx0, dy) and
-// (dx0 + 1, dy): A2 dx^2 + B2 dx dy + C2 dy^2 + L from the record (r0 = u, v, A2, B2; r1 = C2, L, ..).
-// Written with explicit roundings so the forward and backward blends compute the same bits (the
-// backward replays the forward's alpha tests).
-__device__ __forceinline__ void splat_exponents(const float4& r0, const float4& r1, float dx0, float dy, float& p0,
-                                                float& p1) {
+// The base-2 exponents of a splat at a lane's two horizontally adjacent pixel centres
+// px = (x + 0.5, x + 1.5) of one row (dy = py - v already formed): A2 dx^2 + B2 dx dy + C2 dy^2 + L
+// from the record (r0 = u, v, A2, B2; r1 = C2, L, ..), dx = px - u returned too. The row terms are
+// shared; the per-pixel operations go as packed FP32x2 instructions (sm_100: one instruction for
+// both pixels, per component the rounding of the scalar __fsub_rn / __fmaf_rn). Written with
+// explicit roundings so the forward and backward blends compute the same bits (the backward
+// replays the forward's alpha tests). Measured: 0.344 -> 0.335 ms per 740k frame, the 64-view
+// batch 9.5 -> 9.0 ms.
+__device__ __forceinline__ float2 splat_exponents2(const float4& r0, const float4& r1, float2 px, float dy,
+                                                   float2& dx) {
+    dx = __fadd2_rn(px, make_float2(-r0.x, -r0.x));
     const float t1 = __fmul_rn(r0.w, dy);
     const float t3 = __fmaf_rn(__fmul_rn(r1.x, dy), dy, r1.y);
-    p0 = __fmaf_rn(dx0, __fmaf_rn(r0.z, dx0, t1), t3);
-    const float dx1 = __fadd_rn(dx0, 1.0f);
-    p1 = __fmaf_rn(dx1, __fmaf_rn(r0.z, dx1, t1), t3);
+    const float2 in = __ffma2_rn(make_float2(r0.z, r0.z), dx, make_float2(t1, t1));
+    return __ffma2_rn(dx, in, make_float2(t3, t3));
 }
 
 // alpha of a splat from its exponent; valid = the reference's tests pass (power <= 0 is p <= L,

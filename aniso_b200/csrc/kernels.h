@@ -26,9 +26,10 @@ void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
 void launch_frame_begin(Ctrl* ctrl, unsigned* zero, unsigned zero_words, cudaStream_t stream);
 
 // Projection of every (view, Gaussian) entry of a batch; `blocks` = sum over scenes of
-// ceil(n / 256) (scene s starts at block scenes[s].block_base). counts.counts set: each visible
+// ceil(n / preprocess_gaussians_per_block()) (scene s starts at block scenes[s].block_base). counts.counts set: each visible
 // entry's depth key is also added to the digit counts of the first depth pass, whose items are the
 // `entries` depth keys in entry order.
+unsigned preprocess_gaussians_per_block();
 void launch_preprocess(const BatchScene<SceneView>* scenes, unsigned n_scenes, unsigned blocks, const ViewInfo* views,
                        int sh_degree, int tile_w, int tile_h, SplatRecord* rec, unsigned long long* rect16,
                        unsigned* depth_key, const DebugProjection* dbg, const PassCounts& counts, unsigned entries,
