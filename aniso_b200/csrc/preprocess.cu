@@ -20,6 +20,24 @@ constexpr float kShC3_0 = -0.5900435899266435f, kShC3_1 = 2.890611442640554f, kS
                 kShC3_3 = 0.3731763325901154f, kShC3_4 = -0.4570457994644658f, kShC3_5 = 1.445305721320277f,
                 kShC3_6 = -0.5900435899266435f;
 
+// MUFU approximations (relative error ~2^-22) for quantities that carry their own margins or only
+// feed the colour, never the reference's bit-exact geometry (depth, conic, radius, rectangle).
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // SH colour of degree D along (x, y, z): the basis of sh.cpp:18-58 / gpu_render.cu:56-83, then
 // +0.5 and clamped at 0. The coefficients are streamed straight from the Gaussian's 16-byte words
 // ([coefficient][channel] order), so nothing stays live across views; each channel still sums its
@@ -122,7 +140,7 @@ __device__ __forceinline__ bool early_screen(float px, float py, float pz, float
         const float t1 = j11 * cam.R[3 + c] + j12 * cam.R[6 + c];
         tn += t0 * t0 + t1 * t1;
     }
-    const float rb = 3.0f * sqrtf((tn * cov.trace + 0.92f) * 1.001f) + 1.0f;
+    const float rb = 3.0f * sqrt_approx((tn * cov.trace + 0.92f) * 1.001f) + 1.0f;
     const float uu = cam.fx * px * iz + cam.cx, vv = cam.fy * py * iz + cam.cy;
     const float du = 1e-5f * (fabsf(uu) + fabsf(cam.cx)) + 0.01f + rb;
     const float dv = 1e-5f * (fabsf(vv) + fabsf(cam.cy)) + 0.01f + rb;
@@ -206,7 +224,7 @@ __device__ __forceinline__ unsigned axis_bounds(float centre, float cov, float t
     const int t1 = min(tiles8 - 1, (int)(centre + radius) / kCpuTile);
     int lo = t0 * kCpuTile, hi = min(t1 * kCpuTile + kCpuTile - 1, size - 1);
     if (tau >= 0.f) {
-        const float h = sqrtf(2.0f * tau * cov) * 1.001f + 0.05f;
+        const float h = sqrt_approx(2.0f * tau * cov) * 1.001f + 0.05f;
         const float flo = fminf(fmaxf(ceilf(centre - h - 0.5f), -1.0f), (float)size);
         const float fhi = fminf(fmaxf(floorf(centre + h - 0.5f), -1.0f), (float)size);
         lo = max(lo, (int)flo);
@@ -228,35 +246,34 @@ constexpr int kPreWarps = kPreThreads / 32;
 constexpr int kPreGroups = 1;  // groups of 32 Gaussians each warp tests (2 and 4 measured slower)
 constexpr int kPreGaussians = kPreThreads * kPreGroups;  // Gaussians per CTA
 
-// The projection of one entry that passed the early test, by any lane of the warp (the Gaussian
-// is re-read -- from L1/L2, its owner lane just read it -- and its covariance recomputed): the
-// exact test, then colour, blend record, rectangle and depth key, all indexed by entry.
+// The projection of one entry that passed the early test, by any lane of the warp (the Gaussian's
+// activated position / opacity and covariance come from its owner lane through shared memory):
+// the exact test, then colour, blend record, rectangle and depth key, all indexed by entry.
 template <int D, bool kDebug, class Src>
-__device__ __forceinline__ void project_entry(const Src& src, int64_t i, const CamParams& cam, unsigned e, int tile_w,
+__device__ __forceinline__ void project_entry(const Src& src, int64_t i, const float4 pg, const Cov3& cov,
+                                              const CamParams& cam, unsigned e, int tile_w,
                                               int tile_h, SplatRecord* __restrict__ rec,
                                               unsigned long long* __restrict__ rect16, unsigned* __restrict__ depth_key,
                                               const DebugProjection& dbg, const PassCounts& counts,
                                               unsigned count_blocks) {
-    float4 pg, sg, q;
-    src.load(i, pg, sg, q);
-    Cov3 cov;
-    covariance(sg, q, cam.splatScale, cov);
     Projected p;
     if (!project(pg, cov, cam, tile_w, tile_h, p)) {
         depth_key[e] = kCulledKey;
         if (kDebug) dbg.tiles_touched[e] = 0;
         return;
     }
-    // alpha = min(0.99, opacity * exp(power)) >= 1/255 needs power >= -ln(255 opacity): a margin of
-    // 1% + 0.02 on that bound keeps the cut conservative under rounding. A NaN opacity gives alpha
-    // 0.99 everywhere (as fminf does in the reference), so no cut then.
-    float tau = logf(255.0f * pg.w) * 1.01f + 0.02f;
+    // log2(opacity) for the record. alpha = min(0.99, opacity * exp(power)) >= 1/255 needs
+    // power >= -ln(255 opacity) = -ln2 (log2(opacity) + log2(255)): a margin of 1% + 0.02 on that
+    // bound keeps the cut conservative under rounding. A NaN opacity gives alpha 0.99 everywhere
+    // (as fminf does in the reference), so no cut then.
+    const float log2_opacity = lg2_approx(pg.w);
+    float tau = (log2_opacity + 7.99435343685885793f) * (0.69314718055994530942f * 1.01f) + 0.02f;
     if (isnan(tau)) tau = 3.0e38f;
-    const float log2_opacity = log2f(pg.w);
-    // Colour along the unit direction from the camera centre (gpu_render.cu:137-139).
+    // Colour along the unit direction from the camera centre (gpu_render.cu:137-139), normalised by
+    // one reciprocal square root (the colour is compared to a tolerance, not bit for bit).
     float3 d = make_float3(pg.x - cam.eye[0], pg.y - cam.eye[1], pg.z - cam.eye[2]);
-    const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-    const float3 rgb = sh_color_upto<D>(cam.shDegree, src.sh + i * src.sh_planes, d.x / len, d.y / len, d.z / len);
+    const float il = rsqrt_approx(d.x * d.x + d.y * d.y + d.z * d.z);
+    const float3 rgb = sh_color_upto<D>(cam.shDegree, src.sh + i * src.sh_planes, d.x * il, d.y * il, d.z * il);
 
     const unsigned bx = axis_bounds(p.u, p.a, tau, p.radius, cam.width);
     const unsigned by = axis_bounds(p.v, p.c, tau, p.radius, cam.height);
@@ -307,6 +324,9 @@ __global__ void __launch_bounds__(kPreThreads, 4) preprocess_kernel(const BatchS
     __shared__ CamParams s_cam[kMaxStagedViews];
     __shared__ unsigned s_ebase[kMaxStagedViews];
     __shared__ unsigned s_queue[kPreWarps][64];
+    __shared__ float4 s_pos[kPreWarps][32 * kPreGroups];     // activated position + opacity
+    __shared__ float4 s_cova[kPreWarps][32 * kPreGroups];    // s00, s01, s02, s11
+    __shared__ float4 s_covb[kPreWarps][32 * kPreGroups];    // s12, s22, trace, splat scale
     __shared__ unsigned s_scene;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
@@ -344,6 +364,9 @@ __global__ void __launch_bounds__(kPreThreads, 4) preprocess_kernel(const BatchS
             cov_scale = nv > 0 ? s_cam[0].splatScale : 1.0f;
             covariance(sg, q, cov_scale, cov);
         }
+        s_pos[warp][g * 32 + lane] = pg;
+        s_cova[warp][g * 32 + lane] = make_float4(cov.s00, cov.s01, cov.s02, cov.s11);
+        s_covb[warp][g * 32 + lane] = make_float4(cov.s12, cov.s22, cov.trace, cov_scale);
         for (unsigned vk = 0; vk < nv;) {
             // Test views until the queue holds a warp's worth of items (or the views run out).
             for (; vk < nv && queued < 32; ++vk) {
@@ -387,8 +410,16 @@ __global__ void __launch_bounds__(kPreThreads, 4) preprocess_kernel(const BatchS
                     const CamParams& cam = ivk < kMaxStagedViews ? s_cam[ivk] : views[sc.view_begin + ivk].cam;
                     const unsigned e = (ivk < kMaxStagedViews ? s_ebase[ivk] : views[sc.view_begin + ivk].entry_base) +
                                        static_cast<unsigned>(gi);
-                    project_entry<D, kDebug>(sc.src, gi, cam, e, tile_w, tile_h, rec, rect16, depth_key, dbg, counts,
-                                             count_blocks);
+                    const float4 ip = s_pos[warp][item & 0xFFu];
+                    const float4 ca = s_cova[warp][item & 0xFFu], cb = s_covb[warp][item & 0xFFu];
+                    Cov3 icov{ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z};
+                    if (cam.splatScale != cb.w) {  // a view with another splat scale than the first
+                        float4 pg2, sg, q;
+                        sc.src.load(gi, pg2, sg, q);
+                        covariance(sg, q, cam.splatScale, icov);
+                    }
+                    project_entry<D, kDebug>(sc.src, gi, ip, icov, cam, e, tile_w, tile_h, rec, rect16, depth_key, dbg,
+                                             counts, count_blocks);
                 }
                 queued -= take;
                 __syncwarp();
