@@ -328,3 +328,28 @@ def test_degree4_scene_vs_cpu(ab):
     cam = kat.gpu_test_camera(256, 192)
     img = ab.GpuRenderer(g, sh.reshape(8000, 75), 4).render(cam)
     assert_image_parity(img, cpu_render(g, sh.reshape(8000, 75), 4, cam)[0], "degree 4")
+
+
+def test_unchained_launches_render_the_same_bytes(ab, tmp_path):
+    """Frames launched with programmatic stream serialisation (the default) and plainly
+    (ANISO_B200_CHAIN=0, read once per process, hence a child process) give identical images."""
+    import os
+    import subprocess
+    import sys
+
+    g, sh, d = kat.random_cloud(30000, seed=13)
+    cam = kat.gpu_test_camera(640, 360)
+    chained = ab.GpuRenderer(g, sh, d).render(cam)
+    np.save(tmp_path / "g.npy", g)
+    np.save(tmp_path / "sh.npy", sh)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); sys.path.insert(0, %r); import kat, aniso_b200; "
+            "g = np.load(%r); sh = np.load(%r); "
+            "img = aniso_b200.GpuRenderer(g, sh, %d).render(kat.gpu_test_camera(640, 360)); np.save(%r, img)"
+            % (root, os.path.join(root, "tests"), str(tmp_path / "g.npy"), str(tmp_path / "sh.npy"), d,
+               str(tmp_path / "img.npy")))
+    env = dict(os.environ, ANISO_B200_CHAIN="0")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    np.testing.assert_array_equal(np.load(tmp_path / "img.npy"), chained)
+    assert chained.any()
