@@ -82,7 +82,7 @@ class RawParams(ctypes.Structure):
 class RawGrads(ctypes.Structure):
     _fields_ = [("means", ctypes.c_void_p), ("log_scales", ctypes.c_void_p), ("quats", ctypes.c_void_p),
                 ("opacity_logits", ctypes.c_void_p), ("sh", ctypes.c_void_p), ("grad2d", ctypes.c_void_p),
-                ("visible", ctypes.c_void_p)]
+                ("visible", ctypes.c_void_p), ("fresh", ctypes.c_int32)]
 
 
 class AdamGroup(ctypes.Structure):

@@ -110,9 +110,10 @@ class RasterizeFunction(torch.autograd.Function):
     @staticmethod
     def backward(ctx, grad_img):
         means, log_scales, quats, opacity_logits, sh = ctx.saved_tensors
+        # Fresh zeroed buffers: the backward stores into them without reading them (fresh = 1).
         grads = [torch.zeros_like(t) for t in (means, log_scales, quats, opacity_logits, sh)]
-        extra = [ctx.stats[0].data_ptr(), ctx.stats[1].data_ptr()] if ctx.stats is not None else []
-        g = _lib.RawGrads(*[t.data_ptr() for t in grads], *extra)
+        extra = [ctx.stats[0].data_ptr(), ctx.stats[1].data_ptr()] if ctx.stats is not None else [None, None]
+        g = _lib.RawGrads(*[t.data_ptr() for t in grads], *extra, 1)
         gi = grad_img.contiguous().float()
         stream = torch.cuda.current_stream(means.device).cuda_stream
         if ctx.lease.trainer is None:
@@ -175,8 +176,10 @@ class RasterizeBatchFunction(torch.autograd.Function):
     def backward(ctx, *grad_imgs):
         tensors = ctx.saved_tensors
         S = ctx.n_scenes
+        # Fresh zeroed buffers: each scene's first view stores without reading them (fresh = 1).
         grads = [torch.zeros_like(t) for t in tensors]
-        g = (_lib.RawGrads * S)(*[_lib.RawGrads(*[t.data_ptr() for t in grads[5 * s:5 * s + 5]]) for s in range(S)])
+        g = (_lib.RawGrads * S)(*[_lib.RawGrads(*[t.data_ptr() for t in grads[5 * s:5 * s + 5]], None, None, 1)
+                                  for s in range(S)])
         # Views outside the loss arrive as zero images (autograd materialises unused outputs' grads).
         gi = [gimg.contiguous().float() for gimg in grad_imgs]
         ptrs = (ctypes.c_void_p * len(gi))(*[t.data_ptr() for t in gi])

@@ -280,6 +280,12 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_backward_kernel(BackwardIn 
 // Adds one view's gradient to the caller's buffer. The add is rounded on its own (never fused with
 // the product that formed v), so accumulating views here equals summing per-view gradients.
 __device__ __forceinline__ void accumulate(float* p, float v) { *p = __fadd_rn(*p, v); }
+// The same where the old value is known to be zero (the first view of a fresh gradient) and is not
+// read: 0 + v rounds as the add would.
+template <bool kFresh>
+__device__ __forceinline__ void add_grad(float* p, float v) {
+    *p = __fadd_rn(kFresh ? 0.f : *p, v);
+}
 
 template <int D>
 __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16], float bx[16], float by[16],
@@ -350,7 +356,7 @@ __global__ void __launch_bounds__(256) visible_list_kernel(int64_t n, unsigned e
         if (vis[k]) list[at++] = static_cast<unsigned>(i0 + k * 256);
 }
 
-template <int D>
+template <int D, bool kFresh>
 __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamParams cam, unsigned entry_base,
                                                              const Ctrl* ctrl, const unsigned* __restrict__ list,
                                                              const unsigned* __restrict__ list_count,
@@ -504,7 +510,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
         float4* gsh4 = reinterpret_cast<float4*>(gsh);
 #pragma unroll
         for (int pl = 0; pl < (kFloats + 3) / 4; ++pl) {
-            float4 o = gsh4[pl];
+            const float4 o = kFresh ? make_float4(0.f, 0.f, 0.f, 0.f) : gsh4[pl];
             float w[4] = {o.x, o.y, o.z, o.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
@@ -518,7 +524,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
         gm[1] += (gdir[1] - uy * dd) / len;
         gm[2] += (gdir[2] - uz * dd) / len;
     }
-    accumulate(&out.logits[i], go * o * (1.0f - o));
+    add_grad<kFresh>(&out.logits[i], go * o * (1.0f - o));
 
     // ---- conic (A, B, C) = (c, -b, a) / det -> 2D covariance (a, b, c) ----
     const float id2 = 1.0f / (det * det);
@@ -565,9 +571,9 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
     gm[0] += W[0] * gpx + W[3] * gpy + W[6] * gpz;
     gm[1] += W[1] * gpx + W[4] * gpy + W[7] * gpz;
     gm[2] += W[2] * gpx + W[5] * gpy + W[8] * gpz;
-    accumulate(&out.means[3 * i], gm[0]);
-    accumulate(&out.means[3 * i + 1], gm[1]);
-    accumulate(&out.means[3 * i + 2], gm[2]);
+    add_grad<kFresh>(&out.means[3 * i], gm[0]);
+    add_grad<kFresh>(&out.means[3 * i + 1], gm[1]);
+    add_grad<kFresh>(&out.means[3 * i + 2], gm[2]);
 
     // ---- S = M M^T -> M = R(q) diag(s) -> s, R(q) ----
     float gM[3][3];
@@ -585,7 +591,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
             gR[r][k] = gM[r][k] * s[k];
             gs += gM[r][k] * Rq[r][k];
         }
-        accumulate(&out.log_scales[3 * i + k], gs * s[k]);  // s = exp(log s) * splat_scale
+        add_grad<kFresh>(&out.log_scales[3 * i + k], gs * s[k]);  // s = exp(log s) * splat_scale
     }
     const float gqw = 2.0f * (-qz * gR[0][1] + qy * gR[0][2] + qz * gR[1][0] - qx * gR[1][2] - qy * gR[2][0] + qx * gR[2][1]);
     const float gqx = 2.0f * (qy * gR[0][1] + qz * gR[0][2] + qy * gR[1][0] - 2.0f * qx * gR[1][1] - qw * gR[1][2] +
@@ -598,7 +604,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamP
     const float dq = qw * gqw + qx * gqx + qy * gqy + qz * gqz;
     const float il = qlen > 0 ? 1.0f / qlen : 0.f;
     float4* gq4 = reinterpret_cast<float4*>(out.quats) + i;
-    const float4 oq = *gq4;
+    const float4 oq = kFresh ? make_float4(0.f, 0.f, 0.f, 0.f) : *gq4;
     *gq4 = make_float4(__fadd_rn(oq.x, (gqw - qw * dq) * il), __fadd_rn(oq.y, (gqx - qx * dq) * il),
                        __fadd_rn(oq.z, (gqy - qy * dq) * il), __fadd_rn(oq.w, (gqz - qz * dq) * il));
 }
@@ -614,6 +620,27 @@ void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int
     else launch_chained(blend_backward_kernel<16, 16>, dim3(tiles), dim3(128), stream, in, grad_pair);
 }
 
+namespace {
+// The fresh and the accumulating gradient passes are separate instantiations: a run-time flag
+// inside the kernel made the accumulating one (a batch's later views) slower.
+template <bool kFresh>
+void launch_gauss_backward_t(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
+                             const unsigned* list, const unsigned* list_count, const unsigned* rank,
+                             const unsigned* offs, const unsigned long long* rect_sorted, const float* grad_pair,
+                             const RawGrads& out, dim3 grid, dim3 block, cudaStream_t stream) {
+    switch (cam.shDegree) {
+        case 0: launch_chained(gauss_backward_kernel<0, kFresh>, grid, block, stream, raw, cam, entry_base, ctrl, list,
+                               list_count, rank, offs, rect_sorted, grad_pair, out); break;
+        case 1: launch_chained(gauss_backward_kernel<1, kFresh>, grid, block, stream, raw, cam, entry_base, ctrl, list,
+                               list_count, rank, offs, rect_sorted, grad_pair, out); break;
+        case 2: launch_chained(gauss_backward_kernel<2, kFresh>, grid, block, stream, raw, cam, entry_base, ctrl, list,
+                               list_count, rank, offs, rect_sorted, grad_pair, out); break;
+        default: launch_chained(gauss_backward_kernel<3, kFresh>, grid, block, stream, raw, cam, entry_base, ctrl,
+                                list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
+    }
+}
+}  // namespace
+
 void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
                            const unsigned* depth_key, const unsigned* rank, const unsigned* offs,
                            const unsigned long long* rect_sorted, const float* grad_pair, unsigned* list,
@@ -623,16 +650,12 @@ void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned 
     launch_chained(visible_list_kernel, dim3(lblocks), dim3(256), stream, raw.n, entry_base, depth_key, list,
                    list_count);
     const dim3 grid(static_cast<unsigned>((raw.n + 127) / 128)), block(128);
-    switch (cam.shDegree) {
-        case 0: launch_chained(gauss_backward_kernel<0>, grid, block, stream, raw, cam, entry_base, ctrl, list, list_count,
-                                rank, offs, rect_sorted, grad_pair, out); break;
-        case 1: launch_chained(gauss_backward_kernel<1>, grid, block, stream, raw, cam, entry_base, ctrl, list, list_count,
-                                rank, offs, rect_sorted, grad_pair, out); break;
-        case 2: launch_chained(gauss_backward_kernel<2>, grid, block, stream, raw, cam, entry_base, ctrl, list, list_count,
-                                rank, offs, rect_sorted, grad_pair, out); break;
-        default: launch_chained(gauss_backward_kernel<3>, grid, block, stream, raw, cam, entry_base, ctrl, list, list_count,
-                                rank, offs, rect_sorted, grad_pair, out); break;
-    }
+    if (out.fresh)
+        launch_gauss_backward_t<true>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair,
+                                      out, grid, block, stream);
+    else
+        launch_gauss_backward_t<false>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted,
+                                       grad_pair, out, grid, block, stream);
 }
 
 }  // namespace ab2

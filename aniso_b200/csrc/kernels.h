@@ -124,12 +124,14 @@ struct RawGrads {
     float* sh;
     float* grad2d;   // optional (NULL): per Gaussian, |dL/d(screen position)| in NDC units, added over views
     float* visible;  // with grad2d: per Gaussian, the number of views it was visible in, added
+    bool fresh;      // the buffers hold zeros (the scene's first view of a fresh gradient): store, do not read
 };
 // grad_pair: 9 floats per pair, at the pair's depth-ordered slot.
 void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int tile_h, float* grad_pair,
                            cudaStream_t stream);
-// One view: its scene's Gaussians visible in it add their gradients to `out`. list (the scene's n
-// words) and *list_count (zero on entry) are work space for the compacted visible list.
+// One view: its scene's Gaussians visible in it add their gradients to `out` (with out.fresh,
+// whose entries are zero, without reading them). list (the scene's n words) and *list_count (zero
+// on entry) are work space for the compacted visible list.
 void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
                            const unsigned* depth_key, const unsigned* rank, const unsigned* offs,
                            const unsigned long long* rect_sorted, const float* grad_pair, unsigned* list,

@@ -10,16 +10,19 @@
 //      the first pass reads all N keys in entry order and drops the culled ones as it ranks;
 //   3. a pair-offset scan over those V, then an expansion, in depth order, into P (tile, entry)
 //      pairs with the same number of pairs per block (the nearest splats own thousands of tiles);
-//   4. ceil(bits(tiles) / 8) LSD passes stably sort the pairs by tile;
+//   4. ceil(bits(tiles) / 8) LSD passes (or / 9 with 9-bit digits allowed, each pass 8 bits wide
+//      unless 9 are needed) stably sort the pairs by tile;
 //   5. tile ranges as gpu_render.cu:164-177.
 // Each tile's run ends up ordered by (depth bits, entry index), exactly the reference's order, so
 // keys, values and ranges are bit-identical to the reference's for the same projection.
 //
 // Every LSD pass is reduce-then-scan over a fixed number of spans (contiguous runs of 2048-item
-// blocks, one span per CTA, four CTAs per SM): an upsweep counts each span's digits, one CTA per
-// digit scans that digit's counts over the spans, and a downsweep re-reads each block, ranks it
-// with warp match_any, and scatters it through shared memory so global writes are contiguous per
-// digit.
+// blocks, one span per CTA, four CTAs per SM): an upsweep counts each span's digits (in a small
+// frame the preprocess and the expansion count the first depth and tile passes as they write the
+// keys, and those passes have no upsweep), one CTA per digit scans that digit's counts over the
+// spans, and a downsweep re-reads each block, ranks it within each warp (match_any, or ballots on
+// the latency-bound small passes), and scatters it through shared memory so global writes are
+// contiguous per digit.
 // No CTA ever waits on another, so there is no spin loop anywhere in the sort; item counts that
 // are known only on the device (visible entries, pairs) are read from the control block, and the
 // grids are sized for the capacity.

@@ -46,7 +46,7 @@ N_GAUSS = 740_000
 PUBLISHED_GAUSSIANS_PER_S = 741_883 / 2.3e-3
 # dram__bytes_read.sum + dram__bytes_write.sum of one blend launch on a ring view, from one ncu
 # capture (profiles/blend_740k_1280x720.md).
-BLEND_TRAFFIC_BYTES = 35_808_768
+BLEND_TRAFFIC_BYTES = 36_046_848
 
 
 def measured_peaks():

@@ -181,7 +181,10 @@ typedef struct aniso_b200_raw_params {
 } aniso_b200_raw_params;
 
 /* Gradient outputs, DEVICE pointers with the shapes of aniso_b200_raw_params (quats and sh 16-byte
- * aligned). The caller zeroes them; entries of Gaussians culled in the view are left untouched. */
+ * aligned). The caller zeroes them; entries of Gaussians culled in the view are left untouched.
+ * The backward adds to them; with fresh = 1 (they hold only the caller's zeros) the scene's first
+ * view stores its values without reading the zeros back (0 + g, the same bits). The optional
+ * densification statistics (grad2d, visible) are always added to. */
 typedef struct aniso_b200_raw_grads {
     float* means;
     float* log_scales;
@@ -193,6 +196,7 @@ typedef struct aniso_b200_raw_grads {
      * number of views it was visible in, both added to over the views of a backward. */
     float* grad2d;
     float* visible;
+    int32_t fresh;
 } aniso_b200_raw_grads;
 
 int aniso_b200_trainer_create(aniso_b200_trainer** out);

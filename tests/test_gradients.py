@@ -158,3 +158,45 @@ def test_gradients_working_size_vs_fp64_adjoint():
         e = rel(a, b)
         print("%-15s relative error vs FP64 adjoint %.2e" % (name, e))
         assert e <= REL_TOL, (name, e)
+
+
+def test_fresh_gradient_equals_adding_to_zeros(small_case):
+    """The trainer backward into zeroed buffers marked fresh (what the autograd Function passes:
+    the first view stores without reading) gives the same bits as adding into them."""
+    import ctypes
+
+    import torch
+
+    from aniso_b200 import _lib
+    from aniso_b200._lib import check, lib
+    from aniso_b200.autograd import _raw_params
+    from aniso_b200.renderer import RenderOptions, c_camera
+
+    params, cam, target = small_case
+    ts = [torch.tensor(p, dtype=torch.float32, device="cuda").contiguous() for p in params]
+    ts[0][:20, 2] = -5.0  # twenty Gaussians behind the camera: culled, zero gradient
+    raw = _raw_params(*ts)
+    tr = ctypes.c_void_p()
+    check(lib.aniso_b200_trainer_create(ctypes.byref(tr)))
+    try:
+        img = torch.empty(cam.height, cam.width, 3, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        check(lib.aniso_b200_train_forward(tr, ctypes.byref(raw), ctypes.byref(c_camera(cam)),
+                                           ctypes.byref(RenderOptions(sh_degree=1).c()),
+                                           ctypes.c_void_p(img.data_ptr()), ctypes.c_void_p(stream)))
+        gi = (2 * (img - torch.tensor(target, dtype=torch.float32, device="cuda"))).contiguous()
+        results = []
+        for fresh in (0, 1):
+            grads = [torch.zeros_like(t) for t in ts]
+            g = _lib.RawGrads(*[t.data_ptr() for t in grads], None, None, fresh)
+            check(lib.aniso_b200_train_backward(tr, ctypes.c_void_p(gi.data_ptr()), ctypes.byref(g),
+                                                ctypes.c_void_p(stream)))
+            torch.cuda.synchronize()
+            results.append([t.cpu().numpy() for t in grads])
+    finally:
+        lib.aniso_b200_trainer_destroy(tr)
+    for a, b, name in zip(results[0], results[1], GROUPS):
+        np.testing.assert_array_equal(a, b, err_msg=name)
+    assert not results[1][0][:20].any()              # culled: zero
+    assert not results[1][4][:, 4:].any()            # degree-1 render: coefficients 4.. have none
+    assert results[1][4][:, :4].any()
