@@ -138,7 +138,8 @@ typedef struct aniso_b200_batch_options {
     int32_t tile_h;      /*   the image is the same for every shape */
     int32_t blend_batch; /* splats staged per blend round: < 256 the smaller, >= 256 the larger set */
     int32_t use_graph;   /* 1: record the launch sequence once as a CUDA graph and replay it */
-    int32_t radix_bits;  /* digit width of the sort's LSD passes: 8 (the default for 0) or 9 */
+    int32_t radix_bits;  /* widest digit of the sort's tile passes: 8 (the default for 0) or 9, which
+                          * takes 9-bit digits where they save a pass (depth passes are always 8-bit) */
 } aniso_b200_batch_options;
 
 /* A batch of n_views views; view k shows scene scenes[view_scene[k]]. The views of one scene must
