@@ -2,7 +2,7 @@
 
 For a batch (its scenes and its cameras), times every candidate launch shape -- tile shape
 (8x8, 16x16, 16x32), blend batch (128, 256 splats staged per round), widest radix digit of the
-tile sort (8 or 9 bits; 9 saves a pass when the batch's tiles need 17-18 or 25-27 key bits) --
+tile sort (8 or 9 bits; 9 saves a pass when the batch's tiles need 9, 17-18 or 25-27 key bits) --
 with the batch's own CUDA graph, keeps the fastest, and caches the choice in a JSON file keyed by
 the GPU name and a signature of the workload (Gaussian counts, view count, resolutions). Every candidate renders the
 same image (the tile shape only changes how pixels are grouped, the digit width how many passes the
