@@ -353,3 +353,21 @@ def test_unchained_launches_render_the_same_bytes(ab, tmp_path):
     assert out.returncode == 0, out.stdout + out.stderr
     np.testing.assert_array_equal(np.load(tmp_path / "img.npy"), chained)
     assert chained.any()
+
+
+def test_large_host_render_equals_device_render(ab, torch_cuda):
+    """Large frames (odd tile-row counts, a ragged last row) rendered into host memory through the
+    GpuRenderer::render path equal the same frame rendered into device memory, frame after frame."""
+    torch = torch_cuda
+    g, sh, deg = kat.random_cloud(60000, seed=14)
+    r = ab.GpuRenderer(g, sh, deg)
+    for w, h in ((1280, 720), (1000, 1000), (1920, 1080)):
+        cam = kat.gpu_test_camera(w, h)
+        first = r.render(cam)  # also grows the pair capacity for the device render below
+        out = torch.empty(h, w, 3, dtype=torch.uint8, device="cuda")
+        r.render_device(cam, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        r.sync()
+        dev = out.cpu().numpy()
+        np.testing.assert_array_equal(first, dev, err_msg="%dx%d" % (w, h))
+        np.testing.assert_array_equal(r.render(cam), dev, err_msg="%dx%d, again" % (w, h))
+        assert dev.any()
