@@ -30,17 +30,19 @@ class RenderOptions:
         return _lib.Options(int(self.sh_degree), float(self.splat_scale))
 
 
+_CAM_LAYOUT = np.dtype([("v", np.float64, 16), ("wh", np.int32, 2)])
+assert _CAM_LAYOUT.itemsize == ctypes.sizeof(_lib.Camera)
+
+
 def c_camera(cam) -> _lib.Camera:
-    c = _lib.Camera()
-    R = np.asarray(cam.R, np.float64).reshape(9)
-    t = np.asarray(cam.t, np.float64).reshape(3)
-    for k in range(9):
-        c.R[k] = float(R[k])
-    for k in range(3):
-        c.t[k] = float(t[k])
-    c.fx, c.fy, c.cx, c.cy = float(cam.fx), float(cam.fy), float(cam.cx), float(cam.cy)
-    c.width, c.height = int(cam.width), int(cam.height)
-    return c
+    """aniso_b200_camera of a camera (R, t, fx, fy, cx, cy, width, height), packed in one copy."""
+    rec = np.empty((), _CAM_LAYOUT)
+    v = rec["v"]
+    v[:9] = np.asarray(cam.R, np.float64).reshape(9)
+    v[9:12] = np.asarray(cam.t, np.float64).reshape(3)
+    v[12:16] = (cam.fx, cam.fy, cam.cx, cam.cy)
+    rec["wh"] = (cam.width, cam.height)
+    return _lib.Camera.from_buffer_copy(rec.tobytes())
 
 
 def _ply_shape(path):
