@@ -57,24 +57,57 @@ __device__ __forceinline__ void blend_px(float p, float L, float r, float g, flo
     }
 }
 
-template <bool kTrain>
-__device__ __forceinline__ void store_px(const ViewInfo& vi, int x, int y, float tfin, float cr, float cg, float cb,
-                                         unsigned last) {
+// The training outputs of one pixel: float colour, final transmittance, one past the last splat.
+__device__ __forceinline__ void store_train_px(const ViewInfo& vi, int x, int y, float tfin, float cr, float cg,
+                                               float cb, unsigned last) {
     const int width = vi.cam.width;
     if (x >= width || y >= vi.cam.height) return;
     const size_t p = static_cast<size_t>(y) * width + x;
-    if (vi.rgb8) {
-        uint8_t* o = vi.rgb8 + p * 3;
-        o[0] = static_cast<uint8_t>(fminf(fmaxf(cr, 0.f), 1.f) * 255.f + 0.5f);
-        o[1] = static_cast<uint8_t>(fminf(fmaxf(cg, 0.f), 1.f) * 255.f + 0.5f);
-        o[2] = static_cast<uint8_t>(fminf(fmaxf(cb, 0.f), 1.f) * 255.f + 0.5f);
-    }
-    if (kTrain) {
-        vi.rgbf[p * 3 + 0] = cr;
-        vi.rgbf[p * 3 + 1] = cg;
-        vi.rgbf[p * 3 + 2] = cb;
-        vi.t_final[p] = tfin;
-        vi.n_contrib[p] = last;
+    vi.rgbf[p * 3 + 0] = cr;
+    vi.rgbf[p * 3 + 1] = cg;
+    vi.rgbf[p * 3 + 2] = cb;
+    vi.t_final[p] = tfin;
+    vi.n_contrib[p] = last;
+}
+
+// One 8-bit channel as render.cpp quantises it: clamp to [0, 1], scale by 255, round half up.
+__device__ __forceinline__ unsigned quantise(float c) {
+    return static_cast<unsigned>(static_cast<uint8_t>(fminf(fmaxf(c, 0.f), 1.f) * 255.f + 0.5f));
+}
+
+// Copies the tile's RGB8 pixels, staged in s_px (TH rows of TW * 3 bytes, 16-byte aligned), to
+// the image as whole row segments: 16-byte stores where the image rows and the segment allow,
+// else 4-byte ones, else single bytes. Wide contiguous stores matter most when `out` is pinned
+// host memory written across PCIe during the blend (each store instruction becomes a few bus
+// writes, where per-pixel bytes would become many partial ones); in device memory they cost no
+// more than per-pixel stores.
+template <int TW, int TH, int kThreads>
+__device__ __forceinline__ void write_tile_rgb8(const unsigned char* s_px, uint8_t* out, int width, int height,
+                                                int ox, int oy) {
+    constexpr int kRow = TW * 3;
+    const int rows = min(TH, height - oy), seg = min(TW, width - ox) * 3;  // both >= 1: the tile starts inside
+    const size_t pitch = static_cast<size_t>(width) * 3;
+    uint8_t* dst = out + static_cast<size_t>(oy) * pitch + static_cast<size_t>(ox) * 3;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(dst) | pitch | static_cast<unsigned>(seg) | kRow;
+    if ((a & 15) == 0) {
+        const int per = seg >> 4;
+        for (int i = threadIdx.x; i < rows * per; i += kThreads) {
+            const int r = i / per, c = i - r * per;
+            *reinterpret_cast<uint4*>(dst + r * pitch + c * 16) =
+                *reinterpret_cast<const uint4*>(s_px + r * kRow + c * 16);
+        }
+    } else if ((a & 3) == 0) {
+        const int per = seg >> 2;
+        for (int i = threadIdx.x; i < rows * per; i += kThreads) {
+            const int r = i / per, c = i - r * per;
+            *reinterpret_cast<unsigned*>(dst + r * pitch + c * 4) =
+                *reinterpret_cast<const unsigned*>(s_px + r * kRow + c * 4);
+        }
+    } else {
+        for (int i = threadIdx.x; i < rows * seg; i += kThreads) {
+            const int r = i / seg, c = i - r * seg;
+            dst[r * pitch + c] = s_px[r * kRow + c];
+        }
     }
 }
 
@@ -90,6 +123,7 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
     __shared__ float4 s_r1[kBatch];
     __shared__ float s_b[kBatch];
     __shared__ unsigned char s_mask[kBatch];
+    __shared__ __align__(16) unsigned char s_px[TH * TW * 3];  // the tile's RGB8, staged for row stores
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned gtile = blockIdx.x;
@@ -163,8 +197,19 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
             }
         }
     }
-    store_px<kTrain>(vi, x0, y, tf0, r0, g0, b0c, last0);
-    store_px<kTrain>(vi, x0 + 1, y, tf1, r1, g1, b1c, last1);
+    if (kTrain) {
+        store_train_px(vi, x0, y, tf0, r0, g0, b0c, last0);
+        store_train_px(vi, x0 + 1, y, tf1, r1, g1, b1c, last1);
+    }
+    if (vi.rgb8) {  // the same for the whole block: one view per tile
+        // The lane's two pixels are 6 bytes at an even pixel column: three 2-byte words.
+        unsigned short* q = reinterpret_cast<unsigned short*>(s_px + ((y - oy) * TW + (x0 - ox)) * 3);
+        q[0] = static_cast<unsigned short>(quantise(r0) | quantise(g0) << 8);
+        q[1] = static_cast<unsigned short>(quantise(b0c) | quantise(r1) << 8);
+        q[2] = static_cast<unsigned short>(quantise(g1) | quantise(b1c) << 8);
+        __syncthreads();
+        write_tile_rgb8<TW, TH, kThreads>(s_px, vi.rgb8, width, height, ox, oy);
+    }
 }
 
 template <int TW, int TH, int kBatch>

@@ -803,6 +803,18 @@ PlanShape scene_shape(const aniso_b200_options* o) {
 }
 
 // A plan of one view of one scene.
+// The address at which the current device writes the host buffer p, when p is page-locked host
+// memory mapped for this device (cudaHostAlloc, torch's pinned tensors, cudaHostRegister with
+// mapping); else NULL (pageable memory, or pinned memory another device mapped).
+uint8_t* mapped_host(void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? static_cast<uint8_t*>(a.devicePointer) : nullptr;
+}
+
 int single_plan(aniso_b200_scene* s, const aniso_b200_camera* camera, const aniso_b200_options* options,
                 Plan<SceneView>& P) {
     if (options && options->sh_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
@@ -970,14 +982,21 @@ int aniso_b200_render(aniso_b200_scene* s, const aniso_b200_camera* camera, cons
     Plan<SceneView> P;
     AB_TRY(single_plan(s, camera, options, P));
     const size_t bytes = static_cast<size_t>(camera->width) * camera->height * 3;
-    AB_TRY(s->image.reserve(bytes));
-    P.views[0].rgb8 = s->image.p;
+    // Pinned host memory that this device can address is written by the blend itself, across the
+    // bus while the frame is blended, instead of by a copy after it; other memory gets the copy.
+    uint8_t* direct = mapped_host(rgb_host);
+    if (!direct) {
+        AB_TRY(s->image.reserve(bytes));
+        P.views[0].rgb8 = s->image.p;
+    } else {
+        P.views[0].rgb8 = direct;
+    }
     for (int attempt = 0; attempt < 3; ++attempt) {
         const uint64_t k0 = chained_launches();
         AB_TRY(enqueue_plan(s->arena, s->slot(), P, s->stream, stats ? s->ev : nullptr, nullptr, false, false,
                             nullptr));
         s->frame_kernels = static_cast<int32_t>(chained_launches() - k0);
-        AB_CUDA(cudaMemcpyAsync(rgb_host, s->image.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+        if (!direct) AB_CUDA(cudaMemcpyAsync(rgb_host, s->image.p, bytes, cudaMemcpyDeviceToHost, s->stream));
         AB_TRY(read_ctrl(s->arena, s->host_ctrl, s->stream));
         int again = 0;
         AB_TRY(settle(s->arena, *s->host_ctrl, &again, false));

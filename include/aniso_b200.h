@@ -90,7 +90,9 @@ int aniso_b200_scene_destroy(aniso_b200_scene* scene);
 /* GpuRenderer::render(const Camera&, RenderStats*, const RenderOptions&) (gpu_render.h:30,
  * gpu_render.cu:299-375): renders into a HOST buffer of width*height*3 bytes (RGB8, rows top to
  * bottom, image.h:10-17) and returns when it is written. options and stats may be NULL
- * (defaults: degree 3, scale 1). */
+ * (defaults: degree 3, scale 1). A page-locked buffer that the current device can address
+ * (cudaHostAlloc, a pinned torch tensor) is written by the blend kernel directly, across the bus
+ * while the frame blends; any other buffer receives a copy of the finished image. */
 int aniso_b200_render(aniso_b200_scene* scene, const aniso_b200_camera* camera, const aniso_b200_options* options,
                       uint8_t* rgb_host, aniso_b200_stats* stats);
 

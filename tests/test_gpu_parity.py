@@ -371,3 +371,33 @@ def test_large_host_render_equals_device_render(ab, torch_cuda):
         np.testing.assert_array_equal(first, dev, err_msg="%dx%d" % (w, h))
         np.testing.assert_array_equal(r.render(cam), dev, err_msg="%dx%d, again" % (w, h))
         assert dev.any()
+
+
+@pytest.mark.gpu
+def test_pinned_host_render_equals_pageable_render(ab, torch_cuda):
+    """Pinned host buffers are written by the blend itself (16-byte, 4-byte or single-byte row
+    stores, by the alignment of the image rows and the buffer): every byte equals the render into
+    pageable memory (a copy of the finished image) and into device memory, and none is left over
+    from before."""
+    torch = torch_cuda
+    g, sh, deg = kat.random_cloud(60000, seed=15)
+    r = ab.GpuRenderer(g, sh, deg)
+    # 1280: rows of 3840 bytes (16-byte stores); 1284: 3852 (4-byte); 1297: odd (bytes).
+    for w, h in ((1280, 720), (1284, 720), (1297, 731), (64, 48)):
+        cam = kat.gpu_test_camera(w, h)
+        pageable = r.render(cam)
+        out = torch.empty(h, w, 3, dtype=torch.uint8, device="cuda")
+        r.render_device(cam, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        r.sync()
+        np.testing.assert_array_equal(pageable, out.cpu().numpy(), err_msg="%dx%d device" % (w, h))
+        n = w * h * 3
+        keep = torch.full((n + 16,), 0xAB, dtype=torch.uint8).pin_memory()
+        assert keep.is_pinned()
+        pinned = keep.numpy()
+        for off in (0, 1, 4):  # buffer starts 16-, 1- and 4-byte aligned
+            view = pinned[off:off + n].reshape(h, w, 3)
+            view[...] = 0xAB
+            got = r.render(cam, out=view)
+            assert got is view
+            np.testing.assert_array_equal(view, pageable, err_msg="%dx%d pinned +%d" % (w, h, off))
+        assert pageable.any()
