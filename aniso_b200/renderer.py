@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes
 import dataclasses
 import os
+import struct
 
 import numpy as np
 
@@ -30,19 +31,19 @@ class RenderOptions:
         return _lib.Options(int(self.sh_degree), float(self.splat_scale))
 
 
-_CAM_LAYOUT = np.dtype([("v", np.float64, 16), ("wh", np.int32, 2)])
-assert _CAM_LAYOUT.itemsize == ctypes.sizeof(_lib.Camera)
+# The default options, packed once (the library only reads them).
+_DEFAULT_OPTIONS = RenderOptions().c()
+
+_CAM_LAYOUT = struct.Struct("16d2i")  # R (row-major), t, fx, fy, cx, cy as double; width, height
+assert _CAM_LAYOUT.size == ctypes.sizeof(_lib.Camera)
 
 
 def c_camera(cam) -> _lib.Camera:
     """aniso_b200_camera of a camera (R, t, fx, fy, cx, cy, width, height), packed in one copy."""
-    rec = np.empty((), _CAM_LAYOUT)
-    v = rec["v"]
-    v[:9] = np.asarray(cam.R, np.float64).reshape(9)
-    v[9:12] = np.asarray(cam.t, np.float64).reshape(3)
-    v[12:16] = (cam.fx, cam.fy, cam.cx, cam.cy)
-    rec["wh"] = (cam.width, cam.height)
-    return _lib.Camera.from_buffer_copy(rec.tobytes())
+    r = np.asarray(cam.R, np.float64).reshape(9).tolist()
+    t = np.asarray(cam.t, np.float64).reshape(3).tolist()
+    return _lib.Camera.from_buffer_copy(_CAM_LAYOUT.pack(*r, *t, cam.fx, cam.fy, cam.cx, cam.cy, cam.width,
+                                                          cam.height))
 
 
 def _ply_shape(path):
@@ -61,9 +62,10 @@ def _ply_shape(path):
     return n, deg
 
 
-def _ptr(a: np.ndarray):
+def _ptr(a: np.ndarray) -> int:
+    """Address of a C-contiguous array's data, for a c_void_p argument (the caller keeps `a` alive)."""
     assert a.flags["C_CONTIGUOUS"]
-    return a.ctypes.data_as(ctypes.c_void_p)
+    return a.ctypes.data
 
 
 def _stats_dict(s: _lib.Stats) -> dict:
@@ -129,14 +131,14 @@ class GpuRenderer:
     def render(self, camera, stats: dict | None = None, options: RenderOptions | None = None,
                out: np.ndarray | None = None) -> np.ndarray:
         """RGB8 image (H, W, 3) in host memory; fills `stats` like RenderStats if given."""
-        o = (options or RenderOptions()).c()
+        o = options.c() if options is not None else _DEFAULT_OPTIONS
         c = c_camera(camera)
         if out is None:
             out = np.empty((camera.height, camera.width, 3), np.uint8)
         assert out.shape == (camera.height, camera.width, 3) and out.dtype == np.uint8
-        st = _lib.Stats()
+        st = _lib.Stats() if stats is not None else None
         check(lib.aniso_b200_render(self._h, ctypes.byref(c), ctypes.byref(o), _ptr(out),
-                                    ctypes.byref(st) if stats is not None else None))
+                                    ctypes.byref(st) if st is not None else None))
         if stats is not None:
             stats.update(_stats_dict(st))
         return out

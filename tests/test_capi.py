@@ -89,3 +89,20 @@ def test_shim_and_dropin_executables_built_where_reference_present():
     if not cuda_available():
         out = subprocess.run([ref_test], capture_output=True, text=True, timeout=60)
         assert out.returncode == 0 and "skipped" in out.stdout
+
+
+def test_camera_packing_matches_the_struct_fields():
+    """The one-copy camera packing fills aniso_b200_camera exactly as setting its fields does."""
+    from aniso_b200 import _lib
+    from aniso_b200.renderer import c_camera
+    from aniso_b200.scenes import Camera
+
+    rng = np.random.default_rng(3)
+    cam = Camera(R=rng.normal(size=(3, 3)), t=rng.normal(size=3), fx=1.1e3, fy=987.5, cx=640.25, cy=359.75,
+                 width=1297, height=731)
+    ref = _lib.Camera()
+    ref.R[:] = [float(x) for x in cam.R.reshape(9)]
+    ref.t[:] = [float(x) for x in cam.t]
+    ref.fx, ref.fy, ref.cx, ref.cy = cam.fx, cam.fy, cam.cx, cam.cy
+    ref.width, ref.height = cam.width, cam.height
+    assert bytes(c_camera(cam)) == bytes(ref)
