@@ -146,14 +146,6 @@ struct Arena {
     }
 };
 
-// Clears the frame's tile ranges (a tile without pairs keeps [0, 0)). Enqueued ahead of the
-// frame's kernel chain, so that no memset sits between two chained kernels.
-int clear_ranges(Arena& A, unsigned tiles, cudaStream_t st) {
-    AB_TRY(A.ranges.reserve(tiles));
-    AB_CUDA(cudaMemsetAsync(A.ranges.p, 0, static_cast<size_t>(tiles) * sizeof(uint2), st));
-    return 0;
-}
-
 // Largest pass (in items, host capacity) whose digits the kernels that write its keys count, in
 // place of an upsweep launch. Below it a pass is latency-bound and one atomic add per key costs less
 // than a counting kernel; above it the counting kernel's streaming read is the cheaper of the two.
@@ -189,7 +181,7 @@ PassCounts first_pass_counts(Arena& A, unsigned entries, unsigned* zero_words) {
 
 // Depth passes over `entries` depth keys (the first compacts the visible ones), pair scan and
 // expansion, tile passes over `tiles` global tiles, and ranges (cleared beforehand by
-// clear_ranges). *final_buf = the pair buffer that holds the sorted pairs. keep_rank: also record
+// frame_begin). *final_buf = the pair buffer that holds the sorted pairs. keep_rank: also record
 // each visible entry's depth-sorted position (the adjoint reads it). first_counted: the depth
 // keys' producer accumulated the first depth pass's digit counts (first_pass_counts). In a small
 // frame the expansion likewise counts the first tile pass, the last depth pass's span scan clearing
@@ -469,11 +461,11 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     const BatchScene<Src>* scenes = nullptr;
     BatchTables tables;
     AB_TRY(slot.fill(P, st, &views, &scenes, tables));
-    AB_TRY(clear_ranges(A, static_cast<unsigned>(P.tiles), st));
+    AB_TRY(A.ranges.reserve(static_cast<size_t>(P.tiles)));
     if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
     unsigned zero_words = 0;
     const PassCounts first = first_pass_counts(A, static_cast<unsigned>(P.entries), &zero_words);
-    launch_frame_begin(A.ctrl.p, first.counts, zero_words, st);
+    launch_frame_begin(A.ctrl.p, first.counts, zero_words, A.ranges.p, static_cast<unsigned>(P.tiles), st);
     launch_preprocess_any(scenes, P, views, A, dbg, first, st);
     if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
     int fin = 0;
@@ -490,12 +482,30 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     return 0;
 }
 
-// Reads the control block of the last frame on `st` (waits for it). The frame's flags are then
-// consumed: they are cleared on the device, so that the next frame_begin does not fold them into
-// the sticky flags as if no one had seen them.
+// The address at which the current device writes the host buffer p, when p is page-locked host
+// memory mapped for this device (cudaHostAlloc, torch's pinned tensors, cudaHostRegister with
+// mapping); else NULL (pageable memory, or pinned memory another device mapped).
+uint8_t* mapped_host(void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? static_cast<uint8_t*>(a.devicePointer) : nullptr;
+}
+
+// Reads the control block of the last frame on `st` (waits for it) into `host` (page-locked). The
+// frame's flags are then consumed: they are cleared on the device, so that the next frame_begin
+// does not fold them into the sticky flags as if no one had seen them. Where the device maps
+// `host`, one chained kernel does both; else a copy and a memset.
 int read_ctrl(const Arena& A, Ctrl* host, cudaStream_t st) {
-    AB_CUDA(cudaMemcpyAsync(host, A.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
-    AB_CUDA(cudaMemsetAsync(&A.ctrl.p->flags, 0, sizeof(unsigned), st));
+    if (Ctrl* mapped = reinterpret_cast<Ctrl*>(mapped_host(host))) {
+        launch_publish_ctrl(A.ctrl.p, mapped, st);
+        AB_CUDA(cudaGetLastError());
+    } else {
+        AB_CUDA(cudaMemcpyAsync(host, A.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+        AB_CUDA(cudaMemsetAsync(&A.ctrl.p->flags, 0, sizeof(unsigned), st));
+    }
     AB_CUDA(cudaStreamSynchronize(st));
     return 0;
 }
@@ -803,18 +813,6 @@ PlanShape scene_shape(const aniso_b200_options* o) {
 }
 
 // A plan of one view of one scene.
-// The address at which the current device writes the host buffer p, when p is page-locked host
-// memory mapped for this device (cudaHostAlloc, torch's pinned tensors, cudaHostRegister with
-// mapping); else NULL (pageable memory, or pinned memory another device mapped).
-uint8_t* mapped_host(void* p) {
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    return a.type == cudaMemoryTypeHost ? static_cast<uint8_t*>(a.devicePointer) : nullptr;
-}
-
 int single_plan(aniso_b200_scene* s, const aniso_b200_camera* camera, const aniso_b200_options* options,
                 Plan<SceneView>& P) {
     if (options && options->sh_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
@@ -1191,8 +1189,8 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     cudaStream_t st = nullptr;
     const BatchTables tables{dtab.p, dtab.p + 1, dtab.p + 2, 1u};
     const unsigned T = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
-    AB_TRY(clear_ranges(A, T, st));
-    launch_frame_begin(A.ctrl.p, st);
+    AB_TRY(A.ranges.reserve(T));
+    launch_frame_begin(A.ctrl.p, nullptr, 0u, A.ranges.p, T, st);
     launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.depth_key.p, A.rect16.p, st);
     int fin = 0;
     AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, kRadixBits, false, st, &fin));

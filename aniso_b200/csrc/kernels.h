@@ -21,9 +21,14 @@ struct DebugProjection {
 };
 
 // Clears the frame's control block (counts and flags; the flags are folded into the sticky ones),
-// and `zero_words` words at `zero` (the first LSD pass's digit counts, which the preprocess adds to).
+// `zero_words` words at `zero` (the first LSD pass's digit counts, which the preprocess adds to)
+// and the first `tiles` tile ranges (to [0, 0), which a tile without pairs keeps).
 void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
-void launch_frame_begin(Ctrl* ctrl, unsigned* zero, unsigned zero_words, cudaStream_t stream);
+// Writes the control block to `host_mapped` (the device's address of page-locked host memory) and
+// clears the block's flags.
+void launch_publish_ctrl(Ctrl* ctrl, Ctrl* host_mapped, cudaStream_t stream);
+void launch_frame_begin(Ctrl* ctrl, unsigned* zero, unsigned zero_words, uint2* ranges, unsigned tiles,
+                        cudaStream_t stream);
 
 // Projection of every (view, Gaussian) entry of a batch; `blocks` = sum over scenes of
 // ceil(n / preprocess_gaussians_per_block()) (scene s starts at block scenes[s].block_base). counts.counts set: each visible

@@ -48,8 +48,11 @@ constexpr int kExpandChunk = kThreads * kExpandItems;  // pairs per expansion CT
 static_assert(kBlockItems == kSortBlockItems, "an LSD block is kSortBlockItems items");
 static_assert(kExpandChunk == kSortBlockItems, "an expansion CTA writes exactly one LSD block of pairs");
 
-// Clears the control block and `zero_words` words at `zero` (the first pass's digit counts).
-__global__ void frame_begin_kernel(Ctrl* ctrl, unsigned* __restrict__ zero, unsigned zero_words) {
+// Clears the control block, `zero_words` words at `zero` (the first pass's digit counts) and
+// `ranges` tile ranges (a tile without pairs keeps [0, 0)). Clearing the ranges here rather than
+// with a memset ahead of the frame keeps one more operation off the frame's critical path.
+__global__ void frame_begin_kernel(Ctrl* ctrl, unsigned* __restrict__ zero, unsigned zero_words,
+                                   uint2* __restrict__ range, unsigned ranges) {
     chain_entry();
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctrl->sticky_flags |= ctrl->flags;
@@ -58,7 +61,19 @@ __global__ void frame_begin_kernel(Ctrl* ctrl, unsigned* __restrict__ zero, unsi
         ctrl->vis_count = 0;
         ctrl->flags = 0;
     }
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < zero_words; i += gridDim.x * blockDim.x) zero[i] = 0;
+    const unsigned stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
+    for (unsigned i = first; i < zero_words; i += stride) zero[i] = 0;
+    for (unsigned i = first; i < ranges; i += stride) range[i] = make_uint2(0u, 0u);
+}
+
+// Copies the control block into `host` (page-locked host memory this device maps) and clears its
+// flags, so that the next frame_begin does not fold flags the host has already read into the
+// sticky ones. One chained launch where a device-to-host copy and a memset would be two
+// operations after the frame's last kernel.
+__global__ void publish_ctrl_kernel(Ctrl* ctrl, Ctrl* host) {
+    chain_entry();
+    *host = *ctrl;
+    ctrl->flags = 0;
 }
 
 // Items of this frame's pass; false when the frame overflowed (nothing after duplication runs).
@@ -591,13 +606,20 @@ unsigned spans_for(uint64_t max_items) {
 
 }  // namespace
 
-void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream) {
-    launch_chained(frame_begin_kernel, dim3(1), dim3(1), stream, ctrl, static_cast<unsigned*>(nullptr), 0u);
+void launch_publish_ctrl(Ctrl* ctrl, Ctrl* host, cudaStream_t stream) {
+    launch_chained(publish_ctrl_kernel, dim3(1), dim3(1), stream, ctrl, host);
 }
 
-void launch_frame_begin(Ctrl* ctrl, unsigned* zero, unsigned zero_words, cudaStream_t stream) {
-    const unsigned blocks = std::max(1u, std::min((zero_words + kThreads * 4 - 1) / (kThreads * 4), 148u));
-    launch_chained(frame_begin_kernel, dim3(blocks), dim3(kThreads), stream, ctrl, zero, zero_words);
+void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream) {
+    launch_chained(frame_begin_kernel, dim3(1), dim3(1), stream, ctrl, static_cast<unsigned*>(nullptr), 0u,
+                   static_cast<uint2*>(nullptr), 0u);
+}
+
+void launch_frame_begin(Ctrl* ctrl, unsigned* zero, unsigned zero_words, uint2* ranges, unsigned tiles,
+                        cudaStream_t stream) {
+    const unsigned most = std::max(zero_words, tiles);
+    const unsigned blocks = std::max(1u, std::min((most + kThreads * 4 - 1) / (kThreads * 4), 148u));
+    launch_chained(frame_begin_kernel, dim3(blocks), dim3(kThreads), stream, ctrl, zero, zero_words, ranges, tiles);
 }
 
 size_t sort_scratch_words() { return static_cast<size_t>(1 << kMaxRadixBits) * (kMaxSpans + 1); }
