@@ -377,9 +377,22 @@ struct Plan {
 
 // Device copy of a plan's tables, filled from a pinned staging blob by one async copy on the
 // render stream. A slot is reused only after the frame that read it has run (its event).
+// The address at which the current device writes the host buffer p, when p is page-locked host
+// memory mapped for this device (cudaHostAlloc, torch's pinned tensors, cudaHostRegister with
+// mapping); else NULL (pageable memory, or pinned memory another device mapped).
+uint8_t* mapped_host(void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? static_cast<uint8_t*>(a.devicePointer) : nullptr;
+}
+
 struct Slot {
     DevBuf<unsigned char> dev;
     unsigned char* pinned = nullptr;
+    const unsigned char* pinned_dev = nullptr;  // the device's address of `pinned`, NULL if unmapped
     size_t cap = 0;
     cudaEvent_t done = nullptr;
     bool pending = false;
@@ -401,7 +414,9 @@ struct Slot {
         if (bytes > cap) {
             if (pinned) cudaFreeHost(pinned);
             pinned = nullptr;
+            pinned_dev = nullptr;
             AB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&pinned), bytes));
+            pinned_dev = mapped_host(pinned);
             AB_TRY(dev.reserve(bytes));
             cap = bytes;
         }
@@ -416,12 +431,18 @@ struct Slot {
         std::memcpy(t + 2 * V, P.tiles_x.data(), V * sizeof(unsigned));
         return 0;
     }
-    // Stages the blob and enqueues its upload on `st`; returns the device views, scenes, tables.
+    // Stages the blob and enqueues its upload on `st` (a chained kernel reading the mapped staging
+    // buffer, else a copy); returns the device views, scenes, tables.
     template <class Src>
     int fill(const Plan<Src>& P, cudaStream_t st, const ViewInfo** views, const BatchScene<Src>** scenes,
              BatchTables& tables) {
         AB_TRY(stage(P));
-        AB_CUDA(cudaMemcpyAsync(dev.p, pinned, P.blob_bytes(), cudaMemcpyHostToDevice, st));
+        const size_t bytes = P.blob_bytes();
+        if (pinned_dev && bytes % 4 == 0)
+            launch_upload(reinterpret_cast<const unsigned*>(pinned_dev), reinterpret_cast<unsigned*>(dev.p),
+                          static_cast<unsigned>(bytes / 4), st);
+        else
+            AB_CUDA(cudaMemcpyAsync(dev.p, pinned, bytes, cudaMemcpyHostToDevice, st));
         const size_t V = P.views.size(), S = P.scenes.size();
         unsigned char* d = dev.p;
         *views = reinterpret_cast<const ViewInfo*>(d);
@@ -480,18 +501,6 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     if (mark_slot) AB_TRY(slot.mark(st));
     if (final_buf) *final_buf = fin;
     return 0;
-}
-
-// The address at which the current device writes the host buffer p, when p is page-locked host
-// memory mapped for this device (cudaHostAlloc, torch's pinned tensors, cudaHostRegister with
-// mapping); else NULL (pageable memory, or pinned memory another device mapped).
-uint8_t* mapped_host(void* p) {
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    return a.type == cudaMemoryTypeHost ? static_cast<uint8_t*>(a.devicePointer) : nullptr;
 }
 
 // Reads the control block of the last frame on `st` (waits for it) into `host` (page-locked). The

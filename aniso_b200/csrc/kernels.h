@@ -24,6 +24,9 @@ struct DebugProjection {
 // `zero_words` words at `zero` (the first LSD pass's digit counts, which the preprocess adds to)
 // and the first `tiles` tile ranges (to [0, 0), which a tile without pairs keeps).
 void launch_frame_begin(Ctrl* ctrl, cudaStream_t stream);
+// Copies `words` 32-bit words from `src_mapped` (the device's address of page-locked host memory)
+// to `dst` in device memory.
+void launch_upload(const unsigned* src_mapped, unsigned* dst, unsigned words, cudaStream_t stream);
 // Writes the control block to `host_mapped` (the device's address of page-locked host memory) and
 // clears the block's flags.
 void launch_publish_ctrl(Ctrl* ctrl, Ctrl* host_mapped, cudaStream_t stream);

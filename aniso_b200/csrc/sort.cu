@@ -66,6 +66,16 @@ __global__ void frame_begin_kernel(Ctrl* ctrl, unsigned* __restrict__ zero, unsi
     for (unsigned i = first; i < ranges; i += stride) range[i] = make_uint2(0u, 0u);
 }
 
+// Copies `words` 32-bit words of a frame's tables from page-locked host memory (read through the
+// device's mapping, uncached, so that a staging buffer rewritten between launches or graph replays
+// is read afresh) into device memory: the frame's first chained kernel, where a host-to-device copy
+// would be one more non-kernel operation between two frames' kernels.
+__global__ void upload_kernel(const unsigned* __restrict__ src, unsigned* __restrict__ dst, unsigned words) {
+    chain_entry();
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < words) dst[i] = __ldcv(src + i);
+}
+
 // Copies the control block into `host` (page-locked host memory this device maps) and clears its
 // flags, so that the next frame_begin does not fold flags the host has already read into the
 // sticky ones. One chained launch where a device-to-host copy and a memset would be two
@@ -605,6 +615,11 @@ unsigned spans_for(uint64_t max_items) {
 }
 
 }  // namespace
+
+void launch_upload(const unsigned* src_mapped, unsigned* dst, unsigned words, cudaStream_t stream) {
+    const unsigned blocks = std::max(1u, (words + kThreads - 1) / kThreads);
+    launch_chained(upload_kernel, dim3(blocks), dim3(kThreads), stream, src_mapped, dst, words);
+}
 
 void launch_publish_ctrl(Ctrl* ctrl, Ctrl* host, cudaStream_t stream) {
     launch_chained(publish_ctrl_kernel, dim3(1), dim3(1), stream, ctrl, host);
