@@ -10,7 +10,8 @@ A step renders the 16 views once. Metric: Gaussians/s forward = 16 * N / step ti
 `value` is device-timed (CUDA events on the render stream, scene resident in HBM, images
 written to device memory). `e2e` renders the same views through the public C ABI call
 aniso_b200_render (the drop-in for GpuRenderer::render) into pinned host memory, so each view's
-device-to-host image copy is inside the timed region. Under torchrun each rank renders its own
+camera upload and the image's trip to the host (written across PCIe by the blend kernel itself,
+since the buffer is page-locked) are inside the timed region. Under torchrun each rank renders its own
 replica's 16 views (weak scaling, no collective); time is the max over ranks.
 
 Three more workloads of the same metric family ride along on rank 0 (skip with --no-extra):
@@ -561,7 +562,7 @@ def main():
             "accuracy": acc,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": V * 136,
                     "d2h_bytes_per_step": V * (H * W * 3 + 64),
-                    "path": "aniso_b200_render (GpuRenderer::render drop-in), pinned host output"},
+                    "path": "aniso_b200_render (GpuRenderer::render drop-in), pinned host output written by the blend kernel"},
             "gpu_launches": launches_per_step * args.steps,
             "kernels_per_frame": launches_per_step / V,
             "timed_images_match_host_api": same,
