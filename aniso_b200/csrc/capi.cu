@@ -1,10 +1,11 @@
 // The C ABI (include/aniso_b200.h): scenes, batches, the differentiable path.
 //
 // Everything renders through one plan: V views of S scenes. A frame is a fixed, host-sync-free
-// sequence of launches on one stream (capturable in a CUDA graph): upload of the plan's view
-// table, clearing of the tile ranges, then a chain of kernels launched with programmatic stream
-// serialisation: frame_begin, preprocess, 4 depth LSD passes, pair scan, pair expansion, 1-4 tile
-// LSD passes, tile ranges, blend. Data-dependent sizes (visible entries, pairs) stay on the
+// sequence of kernels on one stream (capturable in a CUDA graph), launched with programmatic
+// stream serialisation: upload of the plan's view table, frame_begin (control block, first digit
+// counts, tile ranges), preprocess, 4 depth LSD passes, pair scan, pair expansion, 1-4 tile LSD
+// passes, tile ranges, blend. After a synchronous frame one more kernel hands the control block
+// to the host. Data-dependent sizes (visible entries, pairs) stay on the
 // device; grids are sized for capacity and surplus blocks exit at once. The reference instead reads
 // the pair count back mid-frame (gpu_render.cu:329) to size its buffers; here a frame whose pairs
 // exceed the capacity sets an overflow flag instead of writing them, and the host grows the
@@ -375,8 +376,6 @@ struct Plan {
     }
 };
 
-// Device copy of a plan's tables, filled from a pinned staging blob by one async copy on the
-// render stream. A slot is reused only after the frame that read it has run (its event).
 // The address at which the current device writes the host buffer p, when p is page-locked host
 // memory mapped for this device (cudaHostAlloc, torch's pinned tensors, cudaHostRegister with
 // mapping); else NULL (pageable memory, or pinned memory another device mapped).
@@ -389,6 +388,11 @@ uint8_t* mapped_host(void* p) {
     return a.type == cudaMemoryTypeHost ? static_cast<uint8_t*>(a.devicePointer) : nullptr;
 }
 
+// Device copy of a plan's tables, filled from a pinned staging blob on the render stream (by the
+// frame's first kernel through the blob's device mapping, else by a copy). A slot is restaged only
+// after the frame that read it has run (its event). The blob's size depends only on the numbers of
+// views and scenes, which a recorded graph's geometry fixes, so restaging a graph's slot never
+// moves the blob the recorded upload reads.
 struct Slot {
     DevBuf<unsigned char> dev;
     unsigned char* pinned = nullptr;
