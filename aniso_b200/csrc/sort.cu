@@ -62,8 +62,9 @@ __global__ void frame_begin_kernel(Ctrl* ctrl, unsigned* __restrict__ zero, unsi
         ctrl->flags = 0;
     }
     const unsigned stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
-    for (unsigned i = first; i < zero_words; i += stride) zero[i] = 0;
-    for (unsigned i = first; i < ranges; i += stride) range[i] = make_uint2(0u, 0u);
+    for (unsigned i = first; i < zero_words; i += stride) zero[i] = 0;  // at most 512 x 592 words
+    // 64-bit index: a tile count within one stride of 2^32 must not wrap the loop.
+    for (unsigned long long i = first; i < ranges; i += stride) range[i] = make_uint2(0u, 0u);
 }
 
 // Copies `words` 32-bit words of a frame's tables from page-locked host memory (read through the
