@@ -1,7 +1,8 @@
 """aniso_b200: a B200 (sm_100a) tile-based Gaussian-splat rasterizer behind the C ABI of
 include/aniso_b200.h, a drop-in for the reference's aniso::GpuRenderer.
 
-Importing the package loads libaniso_b200.so and fails if it is missing; there is no CPU path.
+The library libaniso_b200.so is loaded by the first call that needs it, which fails if it is
+missing; there is no CPU path.
 """
 from . import scenes  # noqa: F401  (pure numpy, no library needed)
 from ._lib import AnisoError, LIB_PATH  # noqa: F401

@@ -1,7 +1,8 @@
 """ctypes binding of the C ABI in include/aniso_b200.h (libaniso_b200.so, built in-tree).
 
-There is no fallback: if the library is missing, importing the package fails with the command
-that builds it.
+The library is loaded on first use (the first call through `lib`, or `load()`), so that importing
+the package -- for its pure-numpy scene generator, say -- maps no GPU code. There is no fallback:
+if the library is missing, that first use raises ImportError with the command that builds it.
 """
 from __future__ import annotations
 
@@ -143,7 +144,27 @@ def _load():
     return lib
 
 
-lib = _load()
+class _LazyLibrary:
+    """Stands in for the ctypes library until its first attribute lookup, which loads it."""
+
+    def __init__(self):
+        self._lib = None
+
+    def load(self):
+        if self._lib is None:
+            self._lib = _load()
+        return self._lib
+
+    def __getattr__(self, name):
+        return getattr(self.load(), name)
+
+
+lib = _LazyLibrary()
+
+
+def load():
+    """Loads libaniso_b200.so now (raises ImportError if it is missing) and returns it."""
+    return lib.load()
 
 
 def last_error() -> str:

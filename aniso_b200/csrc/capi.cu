@@ -524,7 +524,9 @@ int read_ctrl(const Arena& A, Ctrl* host, cudaStream_t st) {
 }
 
 // After a synchronised frame: grows the pair buffers on overflow (*again = 1: render it again).
-// With all_frames, also looks at the frames before the last one (the sticky fields).
+// With all_frames, also looks at the frames before the last one (the sticky fields). The caller
+// has waited for every frame that used the buffers (read_ctrl after the owner's last frame), so
+// they are released without waiting for the rest of the device.
 int settle(Arena& A, const Ctrl& h, int* again, bool all_frames) {
     *again = 0;
     const unsigned flags = h.flags | (all_frames ? h.sticky_flags : 0u);
@@ -532,7 +534,6 @@ int settle(Arena& A, const Ctrl& h, int* again, bool all_frames) {
     if (flags & kFlagOverflow) {
         const uint64_t need = pairs + pairs / 4 + 1024;
         if (need > kMaxPairs) return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 splat-tile pairs");
-        AB_CUDA(cudaDeviceSynchronize());
         AB_TRY(A.grow_pairs(static_cast<unsigned>(need)));
         *again = 1;
     }
@@ -547,6 +548,48 @@ int clear_sticky(Arena& A, cudaStream_t st) {
 }
 
 constexpr int kSlots = 8;
+
+// The order of one object's frames (a scene's, a batch's or a trainer's, which share its work
+// buffers) over the caller streams they are enqueued on, and the wait for them. Frames on one
+// stream are ordered by the stream; when the caller switches streams, the new stream first waits
+// (an event) for the last frame on the old one, so the object's frames form one chain. Waiting for
+// the object then means waiting for the end of that chain -- never for the rest of the device, so
+// objects rendering on different streams do not serialise each other's syncs.
+struct StreamChain {
+    cudaStream_t last = nullptr;
+    bool any = false;
+    cudaEvent_t ev = nullptr;
+    StreamChain() = default;
+    StreamChain(const StreamChain&) = delete;
+    StreamChain& operator=(const StreamChain&) = delete;
+    ~StreamChain() {
+        if (ev) cudaEventDestroy(ev);
+    }
+    // Makes `st` wait for the chain's last frame if that went to another stream.
+    int join(cudaStream_t st) {
+        if (!any || st == last) return 0;
+        if (!ev) AB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        AB_CUDA(cudaEventRecord(ev, last));
+        AB_CUDA(cudaStreamWaitEvent(st, ev, 0));
+        return 0;
+    }
+    // A frame was enqueued on `st` (after join(st)).
+    void extend(cudaStream_t st) {
+        last = st;
+        any = true;
+    }
+    // Blocks the host until the chain's last frame has run (for destructors; errors ignored).
+    void wait_host() {
+        if (!any) return;
+        if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        if (cudaEventRecord(ev, last) == cudaSuccess) cudaEventSynchronize(ev);
+        cudaGetLastError();
+        any = false;
+    }
+};
 
 }  // namespace
 
@@ -586,6 +629,7 @@ struct aniso_b200_scene {
     std::vector<cudaEvent_t> prof_ev;
     size_t prof_frames = 0;
     int32_t frame_kernels = 0;  // kernels the last frame launched
+    StreamChain chain;          // the streams the scene's frames went to
 
     SceneView view() const {
         SceneView v;
@@ -599,7 +643,8 @@ struct aniso_b200_scene {
     }
     Slot& slot() { return slots[next_slot++ % kSlots]; }
     ~aniso_b200_scene() {
-        cudaDeviceSynchronize();
+        chain.wait_host();
+        if (stream) cudaStreamSynchronize(stream);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : prof_ev) cudaEventDestroy(e);
@@ -1002,6 +1047,8 @@ int aniso_b200_render(aniso_b200_scene* s, const aniso_b200_camera* camera, cons
     } else {
         P.views[0].rgb8 = direct;
     }
+    AB_TRY(s->chain.join(s->stream));  // after any frame the caller enqueued on another stream
+    s->chain.extend(s->stream);
     for (int attempt = 0; attempt < 3; ++attempt) {
         const uint64_t k0 = chained_launches();
         AB_TRY(enqueue_plan(s->arena, s->slot(), P, s->stream, stats ? s->ev : nullptr, nullptr, false, false,
@@ -1044,9 +1091,11 @@ int aniso_b200_render_device(aniso_b200_scene* s, const aniso_b200_camera* camer
         ev = &s->prof_ev[4 * s->prof_frames++];
     }
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    AB_TRY(s->chain.join(st));
     const uint64_t k0 = chained_launches();
     const int rc = enqueue_plan(s->arena, s->slot(), P, st, ev, nullptr, false, false, nullptr);
     s->frame_kernels = static_cast<int32_t>(chained_launches() - k0);
+    s->chain.extend(st);
     return rc;
 }
 
@@ -1085,7 +1134,9 @@ int aniso_b200_profile_read(aniso_b200_scene* s, double* project_ms, double* sor
 
 int aniso_b200_sync(aniso_b200_scene* s, aniso_b200_stats* stats) {
     if (!s) return fail(ANISO_B200_ERR_ARGUMENT, "scene is NULL");
-    AB_CUDA(cudaDeviceSynchronize());
+    // The control-block read goes on the scene's own stream after its last frame, and waits for it.
+    AB_TRY(s->chain.join(s->stream));
+    s->chain.extend(s->stream);
     AB_TRY(read_ctrl(s->arena, s->host_ctrl, s->stream));
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
@@ -1129,6 +1180,8 @@ int aniso_b200_debug_projection(aniso_b200_scene* s, const aniso_b200_camera* ca
     const BatchScene<SceneView>* scenes = nullptr;
     BatchTables tables;
     Slot& slot = s->slot();
+    AB_TRY(s->chain.join(s->stream));
+    s->chain.extend(s->stream);
     AB_TRY(slot.fill(P, s->stream, &views, &scenes, tables));
     launch_frame_begin(A.ctrl.p, s->stream);
     launch_preprocess_any(scenes, P, views, A, &dbg, PassCounts{}, s->stream);
@@ -1151,6 +1204,8 @@ int aniso_b200_debug_sorted(aniso_b200_scene* s, const aniso_b200_camera* camera
     Plan<SceneView> P;
     AB_TRY(single_plan(s, camera, options, P));
     int fin = 0;
+    AB_TRY(s->chain.join(s->stream));
+    s->chain.extend(s->stream);
     for (int attempt = 0; attempt < 3; ++attempt) {
         AB_TRY(enqueue_plan(s->arena, s->slot(), P, s->stream, nullptr, nullptr, true, false, &fin));
         AB_TRY(read_ctrl(s->arena, s->host_ctrl, s->stream));
@@ -1208,7 +1263,7 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     int fin = 0;
     AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, kRadixBits, false, st, &fin));
     AB_CUDA(cudaGetLastError());
-    AB_CUDA(cudaDeviceSynchronize());
+    AB_CUDA(cudaStreamSynchronize(st));
     Ctrl h;
     AB_CUDA(cudaMemcpy(&h, A.ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost));
     if (h.pair_total != Pn) return fail(ANISO_B200_ERR_CUDA, "device pair count disagrees with the host");
@@ -1235,8 +1290,10 @@ struct aniso_b200_batch {
     cudaGraphExec_t graph = nullptr;
     cudaStream_t capture_stream = nullptr;
     Ctrl* host_ctrl = nullptr;
+    StreamChain chain;  // the streams the batch's frames went to
     ~aniso_b200_batch() {
-        cudaDeviceSynchronize();
+        chain.wait_host();
+        if (capture_stream) cudaStreamSynchronize(capture_stream);
         if (graph) cudaGraphExecDestroy(graph);
         if (capture_stream) cudaStreamDestroy(capture_stream);
         if (host_ctrl) cudaFreeHost(host_ctrl);
@@ -1291,17 +1348,21 @@ int aniso_b200_batch_render(aniso_b200_batch* b, const aniso_b200_camera* camera
         P.views[k].rgb8 = rgb_device[k];
     }
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (b->arena.n < static_cast<int64_t>(P.entries) && b->graph) {
-        AB_CUDA(cudaDeviceSynchronize());
-        cudaGraphExecDestroy(b->graph);  // buffers are about to move: record again
-        b->graph = nullptr;
+    if (b->arena.n < static_cast<int64_t>(P.entries)) {
+        b->chain.wait_host();  // the buffers are about to move: the batch's frames must be done
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);  // record again
+            b->graph = nullptr;
+        }
     }
     AB_TRY(b->arena.ensure(static_cast<int64_t>(std::max<uint64_t>(P.entries, 1))));
+    AB_TRY(b->chain.join(st));
+    b->chain.extend(st);
     if (!b->use_graph)
         return enqueue_plan(b->arena, b->slots[b->next_slot++ % kSlots], P, st, nullptr, nullptr, false, false,
                             nullptr);
     if (b->graph && !P.same_geometry(b->graph_plan)) {
-        AB_CUDA(cudaDeviceSynchronize());
+        b->chain.wait_host();
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
@@ -1334,7 +1395,8 @@ int aniso_b200_batch_render(aniso_b200_batch* b, const aniso_b200_camera* camera
 
 int aniso_b200_batch_sync(aniso_b200_batch* b, aniso_b200_stats* stats) {
     if (!b) return fail(ANISO_B200_ERR_ARGUMENT, "batch is NULL");
-    AB_CUDA(cudaDeviceSynchronize());
+    AB_TRY(b->chain.join(b->capture_stream));  // the control-block read follows the batch's last frame
+    b->chain.extend(b->capture_stream);
     AB_TRY(read_ctrl(b->arena, b->host_ctrl, b->capture_stream));
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
@@ -1372,9 +1434,10 @@ struct aniso_b200_trainer {
     bool has_forward = false;
     Plan<RawParams> plan;
     int fin = 0;
+    StreamChain chain;  // the streams the trainer's forwards and backwards went to
     Slot& slot() { return slots[next_slot++ % kSlots]; }
     ~aniso_b200_trainer() {
-        cudaDeviceSynchronize();
+        chain.wait_host();
         if (host_ctrl) cudaFreeHost(host_ctrl);
     }
 };
@@ -1427,6 +1490,8 @@ int train_forward(aniso_b200_trainer* t, const aniso_b200_raw_params* params, in
     }
     Arena& A = t->arena;
     AB_TRY(A.ensure(static_cast<int64_t>(std::max<uint64_t>(P.entries, 1))));
+    AB_TRY(t->chain.join(st));  // after the trainer's last backward, wherever it went
+    t->chain.extend(st);
     for (int attempt = 0; attempt < 3; ++attempt) {
         int fin = 0;
         AB_TRY(enqueue_plan(A, t->slot(), P, st, nullptr, nullptr, false, true, &fin));
@@ -1467,6 +1532,8 @@ int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const
     const BatchScene<RawParams>* scenes = nullptr;
     BackwardIn in;
     Slot& slot = t->slot();
+    AB_TRY(t->chain.join(st));
+    t->chain.extend(st);
     AB_TRY(slot.fill(P, st, &views, &scenes, in.tables));
     in.ranges = A.ranges.p;
     in.vals = A.pair_val[t->fin].p;

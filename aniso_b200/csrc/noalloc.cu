@@ -12,7 +12,8 @@
 // One g_scratch per device: two calls on one device whose work overlaps in time (different streams
 // or host threads without ordering) race on it. The first call on a device resolves the array's
 // address (cudaGetSymbolAddress, which may load this module), so make it before any stream
-// capture begins.
+// capture begins. The address is kept for the life of the process: after cudaDeviceReset it
+// belongs to a destroyed context, so the entry point must not be used on that device again.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -269,11 +269,12 @@ __device__ __forceinline__ void project_entry(const Src& src, int64_t i, const f
     const float log2_opacity = lg2_approx(pg.w);
     float tau = (log2_opacity + 7.99435343685885793f) * (0.69314718055994530942f * 1.01f) + 0.02f;
     if (isnan(tau)) tau = 3.0e38f;
-    // Colour along the unit direction from the camera centre (gpu_render.cu:137-139), normalised by
-    // one reciprocal square root (the colour is compared to a tolerance, not bit for bit).
+    // Colour along the unit direction from the camera centre, normalised with an IEEE square root
+    // and three IEEE divisions as gpu_render.cu:137-139 does, so the colour is bit-identical to the
+    // reference kernel's too (a few instructions per visible entry).
     float3 d = make_float3(pg.x - cam.eye[0], pg.y - cam.eye[1], pg.z - cam.eye[2]);
-    const float il = rsqrt_approx(d.x * d.x + d.y * d.y + d.z * d.z);
-    const float3 rgb = sh_color_upto<D>(cam.shDegree, src.sh + i * src.sh_planes, d.x * il, d.y * il, d.z * il);
+    const float len = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+    const float3 rgb = sh_color_upto<D>(cam.shDegree, src.sh + i * src.sh_planes, d.x / len, d.y / len, d.z / len);
 
     const unsigned bx = axis_bounds(p.u, p.a, tau, p.radius, cam.width);
     const unsigned by = axis_bounds(p.v, p.c, tau, p.radius, cam.height);

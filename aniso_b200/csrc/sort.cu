@@ -730,7 +730,8 @@ void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect
                    buf.rect_sorted, buf.span_sum);
     launch_chained(pair_offsets_kernel, dim3(spans), dim3(kThreads), stream, buf.rect_sorted, ctrl, spans, capacity,
                    buf.span_sum, buf.offs, buf.chunk_start);
-    const unsigned expand_blocks = (capacity + kExpandChunk - 1) / kExpandChunk;
+    // At least one CTA: with capacity 0 (a count-only call) the frame overflows and the CTA leaves.
+    const unsigned expand_blocks = std::max(1u, (capacity + kExpandChunk - 1) / kExpandChunk);
     launch_chained(expand_kernel, dim3(expand_blocks), dim3(kThreads), stream, sorted_idx, buf.rect_sorted, buf.offs,
                    buf.chunk_start, ctrl, capacity, tables, pair_key, pair_val, first);
 }

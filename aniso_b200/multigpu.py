@@ -1,7 +1,7 @@
 """Several GPUs: one process per GPU, views (and scenes) as the independent units.
 
 Rendering shards with no collective: the scene is replicated on every GPU and each rank renders its
-share of the views (partition_views balances the shares by estimated cost, pixels x Gaussians).
+share of the views (partition_views balances the shares by estimated cost: pixels plus Gaussians).
 Training on one scene seen from views spread over the ranks has exactly one exchange step: each
 rank's gradient buffers are summed with a single all_reduce (allreduce_gradients). Scenes that are
 trained independently (one scene per rank) need no collective at all.
@@ -13,7 +13,8 @@ from __future__ import annotations
 
 
 def view_cost(width: int, height: int, gaussians: int) -> int:
-    """Estimated work of one view: its pixels times the Gaussians projected for it."""
+    """Estimated work of one view: its pixels plus the Gaussians projected for it (the blend's
+    work grows with the pixels, the projection's with the scene's Gaussians, and the two add)."""
     return int(width) * int(height) + int(gaussians)
 
 

@@ -42,11 +42,11 @@ WORKLOAD = "740k-Gaussian SH3 synthetic scene, 16 ring views 1280x720 (forward)"
 METRIC = "Gaussians/s fwd"
 UNIT = "Gaussians/s"
 N_GAUSS = 740_000
-# the reference's published GPU forward on the 0.74M-Gaussian *train* scene at
-# 1280 wide, 2.3 ms/frame on an RTX 5090 (README.md:28) = 741,883 / 2.3 ms.
+# The reference's published GPU forward on its 0.74M-Gaussian *train* scene at 1280 wide:
+# 2.3 ms/frame on an RTX 5090 (README.md:28) = 741,883 / 2.3 ms.
 PUBLISHED_GAUSSIANS_PER_S = 741_883 / 2.3e-3
 # dram__bytes_read.sum + dram__bytes_write.sum of one blend launch on a ring view, from one ncu
-# capture (profiles/blend_740k_1280x720.md).
+# capture of the bench command (the ncu summary of the blend kernel on this workload).
 BLEND_TRAFFIC_BYTES = 36_046_848
 
 
@@ -135,14 +135,17 @@ def reference_arm(args, rank):
 
     gauss, sh, cams = load_workload()
     if oracle.ReferenceCPU.available():
-        impl, kind = oracle.ReferenceCPU(), "reference"
+        # The scene is built once, as the reference CLI does; each timed step is aniso::render.
+        scene, kind = oracle.ReferenceCPU().scene(gauss, sh, 3), "reference"
+        render = scene.render
     else:
-        impl, kind = oracle.Restatement(), "port"
+        port, kind = oracle.Restatement(), "port"
+        render = lambda cam: port.render(gauss, sh, 3, cam)
     for k in range(args.warmup):
-        impl.render(gauss, sh, 3, cams[k % len(cams)])
+        render(cams[k % len(cams)])
     t = time.perf_counter()
     for k in range(args.steps):
-        impl.render(gauss, sh, 3, cams[k % len(cams)])
+        render(cams[k % len(cams)])
     dt = time.perf_counter() - t
     value = args.steps * N_GAUSS / dt
     cores = os.cpu_count() if kind == "reference" else 1
@@ -153,13 +156,27 @@ def reference_arm(args, rank):
             "config": {"workload": WORKLOAD + "; one ring view per step", "gaussians": N_GAUSS},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                              "sample": "%d views of the 16 (one per step), reference render.cpp with "
-                                       "std::thread::hardware_concurrency() threads" % args.steps},
+                                       "std::thread::hardware_concurrency() threads; the scene built once "
+                                       "outside the timed loop" % args.steps},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     try:
         line["reference_gpu"] = reference_gpu_leg(gauss, sh, cams)
     except Exception as e:  # no GPU in this arm's environment: the CPU figure stands alone
         line["reference_gpu"] = {"unavailable": str(e).splitlines()[0][:200]}
+    # This repository's shared libraries mapped by this process: only the reference builds under
+    # oracle/ belong here, never the library under test.
+    line["repo_libraries_loaded"] = repo_libraries_loaded()
     print(json.dumps(line), flush=True)
+
+
+def repo_libraries_loaded():
+    """Shared objects under this repository that the current process has mapped (Linux)."""
+    try:
+        with open("/proc/self/maps") as f:
+            paths = {l.split()[-1] for l in f if l.rstrip().endswith(".so") or ".so." in l}
+    except OSError:
+        return None
+    return sorted(os.path.relpath(p, ROOT) for p in paths if p.startswith(ROOT + os.sep))
 
 
 def cpu_baseline_leg(gauss, sh, cams, images):
@@ -167,23 +184,25 @@ def cpu_baseline_leg(gauss, sh, cams, images):
     import oracle
 
     if oracle.ReferenceCPU.available():
-        impl, kind, cores = oracle.ReferenceCPU(), "reference", os.cpu_count()
+        scene, kind, cores = oracle.ReferenceCPU().scene(gauss, sh, 3), "reference", os.cpu_count()
+        render = scene.render
     else:
-        impl, kind, cores = oracle.Restatement(), "port", 1
+        port, kind, cores = oracle.Restatement(), "port", 1
+        render = lambda cam: port.render(gauss, sh, 3, cam)
     views = [0, 8]
-    impl.render(gauss, sh, 3, cams[views[0]])  # warm-up
+    render(cams[views[0]])  # warm-up
     worst_abs, worst_psnr = 0, float("inf")
     t = time.perf_counter()
-    refs = [impl.render(gauss, sh, 3, cams[v])[0] for v in views]
+    refs = [render(cams[v])[0] for v in views]
     dt = time.perf_counter() - t
     for v, ref in zip(views, refs):
         d = np.abs(images[v].astype(np.int32) - ref.astype(np.int32))
         worst_abs = max(worst_abs, int(d.max()))
         worst_psnr = min(worst_psnr, oracle.psnr(images[v], ref))
     base = {"value": len(views) * N_GAUSS / dt, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": "ring views 0 and 8 of the 16, 1 warm-up, %s" % ("reference render.cpp -O3, "
-                                                                     "hardware_concurrency threads" if kind == "reference"
-                                                                     else "C restatement, 1 thread")}
+            "sample": "ring views 0 and 8 of the 16, 1 warm-up, %s" % ("reference render.cpp -O3 (scene built "
+                                                                     "once), hardware_concurrency threads"
+                                                                     if kind == "reference" else "C restatement, 1 thread")}
     return base, {"max_abs_255": worst_abs, "psnr_db": worst_psnr, "views": views, "vs": "CPU renderer"}
 
 
@@ -547,7 +566,7 @@ def main():
                        "l2": "inputs larger than L2: scene %.0f MB (> 126 MB) re-read from HBM every view"
                              % (N_GAUSS * 240 / 1e6),
                        "parallelism": "replicas (views independent; no collective)" if world > 1 else "1 GPU",
-                       "vs_baseline_source": "BASELINE.md: 2.3 ms/frame, 0.74M train scene, RTX 5090"},
+                       "vs_baseline_source": "reference README.md:28: 2.3 ms/frame, 0.74M train scene, RTX 5090"},
             "stages_ms_per_frame": {k: prof[k] / frames for k in ("project_ms", "sort_ms", "blend_ms")},
             "pairs_per_frame": pairs_per_step / V,
             "roofline": {"kernel": "blend", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -290,9 +290,12 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
  *   left untouched, ranges are all zero, and *pairs (device) still receives the total.
  * A rectangle outside the tile grid refuses the call on the device: *pairs = UINT64_MAX.
  * Alignment: rect and tiles 16 bytes, ranges and pairs 8 bytes (cudaMalloc'd memory is).
+ * capacity 0 is a count-only call: *pairs receives the total and no pair is written.
  * The static buffers are shared: calls on one device must not overlap in time (issue them on one
  * stream, or wait for the previous one). The first call on a device looks the buffers up
- * (cudaGetSymbolAddress), so make it before any stream capture starts. */
+ * (cudaGetSymbolAddress) and keeps the address for the life of the process, so make it before any
+ * stream capture starts, and do not use the entry point on a device after cudaDeviceReset (the
+ * kept address then belongs to the destroyed context). */
 #define ANISO_B200_NOALLOC_MAX_GAUSSIANS 65536
 #define ANISO_B200_NOALLOC_MAX_PAIRS 1048576
 int aniso_b200_sort_projection_noalloc(int64_t n, const uint32_t* tiles_touched, const uint32_t* rect,

@@ -171,6 +171,10 @@ class ReferenceCPU:
         L.ref_cpu_load_ply.argtypes = [ctypes.c_char_p, ctypes.POINTER(_I64), ctypes.POINTER(_I), _P, _P]
         L.ref_cpu_load_colmap.argtypes = [ctypes.c_char_p, ctypes.POINTER(_I), _P]
         L.ref_cpu_camera_centre.argtypes = [_P, _P]
+        L.ref_cpu_scene_create.argtypes = [_P, _P, _I64, _I]
+        L.ref_cpu_scene_create.restype = _P
+        L.ref_cpu_scene_destroy.argtypes = [_P]
+        L.ref_cpu_scene_render.argtypes = [_P, _P, _I, _I, _I, _F, _P, _P]
 
     @staticmethod
     def available(path: str = REF_CPU_SO) -> bool:
@@ -189,6 +193,10 @@ class ReferenceCPU:
                                             cam.width, cam.height, sh_degree, splat_scale, _ptr(img), _ptr(stats)))
         return img, {"visible": int(stats[0]), "tile_pairs": int(stats[1]), "project_ms": stats[2],
                      "sort_ms": stats[3], "blend_ms": stats[4]}
+
+    def scene(self, gauss, sh, scene_degree):
+        """An aniso::Scene built once (as the reference CLI builds it) for repeated renders."""
+        return ReferenceCPUScene(self, gauss, sh, scene_degree)
 
     def make_splats(self, gauss, sh, scene_degree, cam, sh_degree=3, splat_scale=1.0):
         gauss, sh = _f32(gauss), _f32(sh)
@@ -229,6 +237,34 @@ class ReferenceCPU:
         out = np.empty(3, np.float32)
         self.lib.ref_cpu_camera_centre(_ptr(c), _ptr(out))
         return out
+
+
+class ReferenceCPUScene:
+    """A scene held by the reference CPU library: render() times aniso::render alone."""
+
+    def __init__(self, ref: ReferenceCPU, gauss, sh, scene_degree):
+        self.ref = ref
+        gauss, sh = _f32(gauss), _f32(sh)
+        self.handle = ref.lib.ref_cpu_scene_create(_ptr(gauss), _ptr(sh), gauss.shape[0], scene_degree)
+        if not self.handle:
+            raise RuntimeError(ref.lib.ref_cpu_last_error().decode())
+
+    def render(self, cam, sh_degree=3, splat_scale=1.0, out=None):
+        img = out if out is not None else np.zeros((cam.height, cam.width, 3), np.uint8)
+        stats = np.zeros(5, np.float64)
+        c = _cam(cam)
+        self.ref._check(self.ref.lib.ref_cpu_scene_render(self.handle, _ptr(c), cam.width, cam.height, sh_degree,
+                                                          splat_scale, _ptr(img), _ptr(stats)))
+        return img, {"visible": int(stats[0]), "tile_pairs": int(stats[1]), "project_ms": stats[2],
+                     "sort_ms": stats[3], "blend_ms": stats[4]}
+
+    def close(self):
+        if self.handle:
+            self.ref.lib.ref_cpu_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
 
 
 class ReferenceGPU:

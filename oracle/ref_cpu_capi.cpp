@@ -87,6 +87,46 @@ int ref_cpu_render(const float* gauss, const float* sh, int64_t n, int scene_deg
     }
 }
 
+// A scene built once, as the reference CLI builds it (main.cpp loads the PLY once and renders each
+// view from the same Scene), so that a timed loop of ref_cpu_scene_render calls measures
+// aniso::render alone (render.cpp:140-223), not the Scene construction.
+void* ref_cpu_scene_create(const float* gauss, const float* sh, int64_t n, int scene_degree) {
+    try {
+        return new aniso::Scene(makeScene(gauss, sh, n, scene_degree));
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
+void ref_cpu_scene_destroy(void* scene) { delete static_cast<aniso::Scene*>(scene); }
+
+// aniso::render of a scene made by ref_cpu_scene_create; stats as ref_cpu_render.
+int ref_cpu_scene_render(const void* scene, const double* cam, int w, int h, int sh_degree, float splat_scale,
+                         uint8_t* out_rgb, double* stats) {
+    try {
+        const aniso::Scene& s = *static_cast<const aniso::Scene*>(scene);
+        const aniso::Camera c = makeCamera(cam, w, h);
+        aniso::RenderOptions o;
+        o.shDegree = sh_degree;
+        o.splatScale = splat_scale;
+        aniso::RenderStats st;
+        const aniso::Image img = aniso::render(s, c, &st, o);
+        std::memcpy(out_rgb, img.rgb.data(), img.rgb.size());
+        if (stats) {
+            stats[0] = static_cast<double>(st.visible);
+            stats[1] = static_cast<double>(st.tilePairs);
+            stats[2] = st.projectMs;
+            stats[3] = st.sortMs;
+            stats[4] = st.blendMs;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 // makeSplat (render.cpp:39-104) for every Gaussian. out: n x 10 floats
 // (u, v, conicA, conicB, conicC, opacity, depth, r, g, b); radius: n ints; alive: n bytes.
 int ref_cpu_make_splats(const float* gauss, const float* sh, int64_t n, int scene_degree, const double* cam, int w,

@@ -32,6 +32,9 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] in ("reference", "port") and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert "reference_gpu" in d  # timed on a GPU box, else the reason it is not
+    # the arm runs the reference alone: the library under test is never mapped in its process
+    assert d["repo_libraries_loaded"] is not None
+    assert not [p for p in d["repo_libraries_loaded"] if p.startswith("aniso_b200")], d["repo_libraries_loaded"]
 
 
 def test_reference_arm_other_ranks_exit_without_work():

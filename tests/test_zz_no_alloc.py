@@ -95,6 +95,18 @@ def test_pairs_beyond_capacity_are_not_written(env):
     assert not ranges.any()
 
 
+def test_capacity_zero_counts_only(env):
+    """capacity 0 is a count-only call: it succeeds, reports the pair total and writes no pair."""
+    torch, ab, _lib = env
+    proj, tx, ty = projection(ab, 4000, 192, 128, seed=6)
+    ref = ab.sort_projection(proj["tiles_touched"], proj["rect"], proj["depth"], tx, ty)
+    for _ in range(2):
+        tiles, values, ranges, pairs = call(torch, _lib, proj, tx, ty, 0, torch.cuda.Stream())
+        assert pairs == len(ref[1]) > 0
+        assert (tiles == np.uint32(0xFFFFFFF9)).all() and (values == np.uint32(0xFFFFFFF9)).all()
+        assert not ranges.any()
+
+
 def test_refuses_oversize_and_bad_rectangles(env):
     torch, ab, _lib = env
     P = ctypes.c_void_p
