@@ -66,6 +66,17 @@ class Restatement:
         L.orc_train_backward_f64.argtypes = [_I64, _P, _P, _P, _P, _P, _I, _P, _I, _I, _I, ctypes.c_double, _P,
                                              _P, _P, _P, _P, _P]
         L.orc_train_backward_f64.restype = _I
+        L.orc_big_create.argtypes = [_I64, _P, _P, _P, _P, _P, _I, _P, _I, _I, _I, ctypes.c_double]
+        L.orc_big_create.restype = _P
+        L.orc_big_destroy.argtypes = [_P]
+        L.orc_big_counts.argtypes = [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]
+        L.orc_big_image.argtypes = [_P, _I, _I, _I, _I, _P]
+        L.orc_big_image.restype = _I
+        L.orc_big_adjoint.argtypes = [_P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P]
+        L.orc_big_adjoint.restype = _I
+        L.orc_big_fd.argtypes = [_P, _P, _I64, _I, _I, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(_I), ctypes.POINTER(_I64)]
+        L.orc_big_fd.restype = _I
 
     def activate(self, raw):
         n = raw.n
@@ -154,6 +165,61 @@ class Restatement:
                                              _ptr(gi), *[_ptr(g) for g in grads])
         assert rc == 0, rc
         return grads
+
+    def big_frame(self, params, cam, sh_degree=3, splat_scale=1.0):
+        """The FP64 training render of a scene of any size, for local queries (BigFrame)."""
+        return BigFrame(self, params, cam, sh_degree, splat_scale)
+
+
+class BigFrame:
+    """FP64 training render (orc_big_*) held for local queries: window images, window adjoints and
+    single-parameter central differences of the whole-image L2 loss."""
+
+    GROUPS = ("means", "log_scales", "quats", "opacity_logits", "sh")
+
+    def __init__(self, R: Restatement, params, cam, sh_degree=3, splat_scale=1.0):
+        self.R, self.cam = R, cam
+        self.params = Restatement._f64(params)  # kept alive: the frame reads them
+        means, ls, q, lg, sh = self.params
+        c = _cam(cam)
+        self.h = R.lib.orc_big_create(means.shape[0], _ptr(means), _ptr(ls), _ptr(q), _ptr(lg), _ptr(sh),
+                                      sh.shape[1], _ptr(c), cam.width, cam.height, sh_degree, splat_scale)
+        if not self.h:
+            raise MemoryError("orc_big_create failed")
+
+    def counts(self):
+        v, p = _I64(0), _I64(0)
+        self.R.lib.orc_big_counts(self.h, ctypes.byref(v), ctypes.byref(p))
+        return v.value, p.value
+
+    def image(self, x0, y0, w, h):
+        out = np.zeros((h, w, 3), np.float64)
+        assert self.R.lib.orc_big_image(self.h, x0, y0, w, h, _ptr(out)) == 0
+        return out
+
+    def adjoint(self, x0, y0, grad):
+        grad = np.ascontiguousarray(grad, np.float64)
+        h, w = grad.shape[:2]
+        grads = [np.zeros_like(a) for a in self.params]
+        assert self.R.lib.orc_big_adjoint(self.h, x0, y0, w, h, _ptr(grad), *[_ptr(g) for g in grads]) == 0
+        return grads
+
+    def fd(self, target, i, group, comp, step):
+        """(central difference, smooth, pixels evaluated) of the whole-image L2 loss vs target."""
+        target = np.ascontiguousarray(target, np.float32)
+        assert target.shape == (self.cam.height, self.cam.width, 3)
+        d, sm, px = ctypes.c_double(0), _I(0), _I64(0)
+        assert self.R.lib.orc_big_fd(self.h, _ptr(target), int(i), int(group), int(comp), float(step), ctypes.byref(d),
+                                     ctypes.byref(sm), ctypes.byref(px)) == 0
+        return d.value, bool(sm.value), px.value
+
+    def close(self):
+        if self.h:
+            self.R.lib.orc_big_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 class ReferenceCPU:

@@ -602,6 +602,98 @@ int orc_train_forward_f64(int64_t n, const double* means, const double* log_scal
     return 0;
 }
 
+/* The adjoint of one Gaussian's projection and colour (splat64) given the gradients of its
+ * splat g[9] = d/d(u, v, A, B, C, o, r, g, b): writes its 59 raw-parameter gradients. */
+static void gauss_adjoint64(const orc_cam64* cam_, const orc_sp64* s, int64_t i, const double* g,
+                            const double* sh, int K, int D, double* g_means, double* g_log_scales,
+                            double* g_quats, double* g_logits, double* g_sh) {
+    const orc_cam64 cam = *cam_;
+    const int count = (D + 1) * (D + 1);
+    /* colour and SH */
+    double b[16], bx[16], by[16], bz[16];
+    sh_basis64(s->dir[0], s->dir[1], s->dir[2], D, b, bx, by, bz);
+    double gdir[3] = {0, 0, 0};
+    for (int ch = 0; ch < 3; ++ch) {
+        const double gcol = s->pre[ch] > 0 ? g[6 + ch] : 0;
+        for (int q = 0; q < count; ++q) {
+            const double shv = sh[((size_t)i * K + q) * 3 + ch];
+            g_sh[((size_t)i * K + q) * 3 + ch] = b[q] * gcol;
+            gdir[0] += shv * bx[q] * gcol;
+            gdir[1] += shv * by[q] * gcol;
+            gdir[2] += shv * bz[q] * gcol;
+        }
+    }
+    const double dd = s->dir[0] * gdir[0] + s->dir[1] * gdir[1] + s->dir[2] * gdir[2];
+    double gm[3];
+    for (int q = 0; q < 3; ++q) gm[q] = (gdir[q] - s->dir[q] * dd) / s->len;
+    g_logits[i] = g[5] * s->o * (1 - s->o);
+    /* conic -> 2D covariance */
+    const double a = s->a, bb = s->b, c = s->c, det = s->det, id2 = 1.0 / (det * det);
+    const double gA = g[2], gB = g[3], gC = g[4];
+    const double ga = (-c * c * gA + bb * c * gB - bb * bb * gC) * id2;
+    const double gb = (2 * bb * c * gA - (det + 2 * bb * bb) * gB + 2 * a * bb * gC) * id2;
+    const double gc2 = (-bb * bb * gA + a * bb * gB - a * a * gC) * id2;
+    const double* T = s->T;
+    const double* S = s->S;
+    double ST[6];
+    for (int r = 0; r < 2; ++r)
+        for (int q = 0; q < 3; ++q) ST[3 * r + q] = S[3 * q] * T[3 * r] + S[3 * q + 1] * T[3 * r + 1] + S[3 * q + 2] * T[3 * r + 2];
+    double gS[9], gT[6], gJ[6];
+    for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 3; ++q)
+            gS[3 * r + q] = ga * T[r] * T[q] + gb * T[r] * T[3 + q] + gc2 * T[3 + r] * T[3 + q];
+    for (int q = 0; q < 3; ++q) {
+        gT[q] = 2 * ga * ST[q] + gb * ST[3 + q];
+        gT[3 + q] = gb * ST[q] + 2 * gc2 * ST[3 + q];
+    }
+    const double* W = cam.R;
+    for (int r = 0; r < 2; ++r)
+        for (int kk = 0; kk < 3; ++kk) gJ[3 * r + kk] = gT[3 * r] * W[3 * kk] + gT[3 * r + 1] * W[3 * kk + 1] + gT[3 * r + 2] * W[3 * kk + 2];
+    const double px = s->pc[0], py = s->pc[1], pz = s->pc[2], iz = 1 / pz, iz2 = iz * iz, iz3 = iz2 * iz;
+    const double limX = 1.3 * 0.5 * cam.w / cam.fx, limY = 1.3 * 0.5 * cam.h / cam.fy;
+    double rx = px / pz, ry = py / pz;
+    rx = rx < -limX ? -limX : (rx > limX ? limX : rx);
+    ry = ry < -limY ? -limY : (ry > limY ? limY : ry);
+    const double tx = rx * pz, ty = ry * pz;
+    double gpx = g[0] * cam.fx * iz, gpy = g[1] * cam.fy * iz;
+    double gpz = -(g[0] * cam.fx * px + g[1] * cam.fy * py) * iz2 - (gJ[0] * cam.fx + gJ[4] * cam.fy) * iz2;
+    if (!s->clx) { gpx += gJ[2] * (-cam.fx * iz2); gpz += gJ[2] * (2 * cam.fx * tx * iz3); }
+    else gpz += gJ[2] * (cam.fx * rx * iz2);
+    if (!s->cly) { gpy += gJ[5] * (-cam.fy * iz2); gpz += gJ[5] * (2 * cam.fy * ty * iz3); }
+    else gpz += gJ[5] * (cam.fy * ry * iz2);
+    for (int q = 0; q < 3; ++q) gm[q] += W[q] * gpx + W[3 + q] * gpy + W[6 + q] * gpz;
+    for (int q = 0; q < 3; ++q) g_means[3 * i + q] = gm[q];
+    /* S = M M^T, M = R(q) diag(s) */
+    const double* M = s->M;
+    const double* Rq = s->Rq;
+    double gM[9], gR[9];
+    for (int r = 0; r < 3; ++r)
+        for (int kk = 0; kk < 3; ++kk) {
+            double v = 0;
+            for (int q = 0; q < 3; ++q) v += (gS[3 * r + q] + gS[3 * q + r]) * M[3 * q + kk];
+            gM[3 * r + kk] = v;
+        }
+    for (int kk = 0; kk < 3; ++kk) {
+        double gsv = 0;
+        for (int r = 0; r < 3; ++r) {
+            gR[3 * r + kk] = gM[3 * r + kk] * s->s[kk];
+            gsv += gM[3 * r + kk] * Rq[3 * r + kk];
+        }
+        g_log_scales[3 * i + kk] = gsv * s->s[kk];
+    }
+    const double qw = s->qn[0], qx = s->qn[1], qy = s->qn[2], qz = s->qn[3];
+    const double gqw = 2 * (-qz * gR[1] + qy * gR[2] + qz * gR[3] - qx * gR[5] - qy * gR[6] + qx * gR[7]);
+    const double gqx = 2 * (qy * gR[1] + qz * gR[2] + qy * gR[3] - 2 * qx * gR[4] - qw * gR[5] + qz * gR[6] + qw * gR[7] - 2 * qx * gR[8]);
+    const double gqy = 2 * (-2 * qy * gR[0] + qx * gR[1] + qw * gR[2] + qx * gR[3] + qz * gR[5] - qw * gR[6] + qz * gR[7] - 2 * qy * gR[8]);
+    const double gqz = 2 * (-2 * qz * gR[0] - qw * gR[1] + qx * gR[2] + qw * gR[3] - 2 * qz * gR[4] + qy * gR[5] + qx * gR[6] + qy * gR[7]);
+    const double dq = qw * gqw + qx * gqx + qy * gqy + qz * gqz;
+    const double il = s->qlen > 0 ? 1 / s->qlen : 0;
+    g_quats[4 * i] = (gqw - qw * dq) * il;
+    g_quats[4 * i + 1] = (gqx - qx * dq) * il;
+    g_quats[4 * i + 2] = (gqy - qy * dq) * il;
+    g_quats[4 * i + 3] = (gqz - qz * dq) * il;
+}
+
 int orc_train_backward_f64(int64_t n, const double* means, const double* log_scales, const double* quats,
                            const double* logits, const double* sh, int K, const double* camd, int w, int h,
                            int sh_degree, double splat_scale, const double* grad_img, double* g_means,
@@ -645,98 +737,327 @@ int orc_train_backward_f64(int64_t n, const double* means, const double* log_sca
                 g[1] += dpow * (s->C * dy + s->B * dx);
             }
         }
-    const int count = (D + 1) * (D + 1);
     for (size_t k = 0; k < f.visible; ++k) {
         const uint32_t i = f.order[k];
-        const orc_sp64* s = &f.sp[i];
-        const double* g = g2 + (size_t)i * 9;
-        /* colour and SH */
-        double b[16], bx[16], by[16], bz[16];
-        sh_basis64(s->dir[0], s->dir[1], s->dir[2], D, b, bx, by, bz);
-        double gdir[3] = {0, 0, 0};
-        for (int ch = 0; ch < 3; ++ch) {
-            const double gcol = s->pre[ch] > 0 ? g[6 + ch] : 0;
-            for (int q = 0; q < count; ++q) {
-                const double shv = sh[((size_t)i * K + q) * 3 + ch];
-                g_sh[((size_t)i * K + q) * 3 + ch] = b[q] * gcol;
-                gdir[0] += shv * bx[q] * gcol;
-                gdir[1] += shv * by[q] * gcol;
-                gdir[2] += shv * bz[q] * gcol;
-            }
-        }
-        const double dd = s->dir[0] * gdir[0] + s->dir[1] * gdir[1] + s->dir[2] * gdir[2];
-        double gm[3];
-        for (int q = 0; q < 3; ++q) gm[q] = (gdir[q] - s->dir[q] * dd) / s->len;
-        g_logits[i] = g[5] * s->o * (1 - s->o);
-        /* conic -> 2D covariance */
-        const double a = s->a, bb = s->b, c = s->c, det = s->det, id2 = 1.0 / (det * det);
-        const double gA = g[2], gB = g[3], gC = g[4];
-        const double ga = (-c * c * gA + bb * c * gB - bb * bb * gC) * id2;
-        const double gb = (2 * bb * c * gA - (det + 2 * bb * bb) * gB + 2 * a * bb * gC) * id2;
-        const double gc2 = (-bb * bb * gA + a * bb * gB - a * a * gC) * id2;
-        const double* T = s->T;
-        const double* S = s->S;
-        double ST[6];
-        for (int r = 0; r < 2; ++r)
-            for (int q = 0; q < 3; ++q) ST[3 * r + q] = S[3 * q] * T[3 * r] + S[3 * q + 1] * T[3 * r + 1] + S[3 * q + 2] * T[3 * r + 2];
-        double gS[9], gT[6], gJ[6];
-        for (int r = 0; r < 3; ++r)
-            for (int q = 0; q < 3; ++q)
-                gS[3 * r + q] = ga * T[r] * T[q] + gb * T[r] * T[3 + q] + gc2 * T[3 + r] * T[3 + q];
-        for (int q = 0; q < 3; ++q) {
-            gT[q] = 2 * ga * ST[q] + gb * ST[3 + q];
-            gT[3 + q] = gb * ST[q] + 2 * gc2 * ST[3 + q];
-        }
-        const double* W = cam.R;
-        for (int r = 0; r < 2; ++r)
-            for (int kk = 0; kk < 3; ++kk) gJ[3 * r + kk] = gT[3 * r] * W[3 * kk] + gT[3 * r + 1] * W[3 * kk + 1] + gT[3 * r + 2] * W[3 * kk + 2];
-        const double px = s->pc[0], py = s->pc[1], pz = s->pc[2], iz = 1 / pz, iz2 = iz * iz, iz3 = iz2 * iz;
-        const double limX = 1.3 * 0.5 * cam.w / cam.fx, limY = 1.3 * 0.5 * cam.h / cam.fy;
-        double rx = px / pz, ry = py / pz;
-        rx = rx < -limX ? -limX : (rx > limX ? limX : rx);
-        ry = ry < -limY ? -limY : (ry > limY ? limY : ry);
-        const double tx = rx * pz, ty = ry * pz;
-        double gpx = g[0] * cam.fx * iz, gpy = g[1] * cam.fy * iz;
-        double gpz = -(g[0] * cam.fx * px + g[1] * cam.fy * py) * iz2 - (gJ[0] * cam.fx + gJ[4] * cam.fy) * iz2;
-        if (!s->clx) { gpx += gJ[2] * (-cam.fx * iz2); gpz += gJ[2] * (2 * cam.fx * tx * iz3); }
-        else gpz += gJ[2] * (cam.fx * rx * iz2);
-        if (!s->cly) { gpy += gJ[5] * (-cam.fy * iz2); gpz += gJ[5] * (2 * cam.fy * ty * iz3); }
-        else gpz += gJ[5] * (cam.fy * ry * iz2);
-        for (int q = 0; q < 3; ++q) gm[q] += W[q] * gpx + W[3 + q] * gpy + W[6 + q] * gpz;
-        for (int q = 0; q < 3; ++q) g_means[3 * i + q] = gm[q];
-        /* S = M M^T, M = R(q) diag(s) */
-        const double* M = s->M;
-        const double* Rq = s->Rq;
-        double gM[9], gR[9];
-        for (int r = 0; r < 3; ++r)
-            for (int kk = 0; kk < 3; ++kk) {
-                double v = 0;
-                for (int q = 0; q < 3; ++q) v += (gS[3 * r + q] + gS[3 * q + r]) * M[3 * q + kk];
-                gM[3 * r + kk] = v;
-            }
-        for (int kk = 0; kk < 3; ++kk) {
-            double gsv = 0;
-            for (int r = 0; r < 3; ++r) {
-                gR[3 * r + kk] = gM[3 * r + kk] * s->s[kk];
-                gsv += gM[3 * r + kk] * Rq[3 * r + kk];
-            }
-            g_log_scales[3 * i + kk] = gsv * s->s[kk];
-        }
-        const double qw = s->qn[0], qx = s->qn[1], qy = s->qn[2], qz = s->qn[3];
-        const double gqw = 2 * (-qz * gR[1] + qy * gR[2] + qz * gR[3] - qx * gR[5] - qy * gR[6] + qx * gR[7]);
-        const double gqx = 2 * (qy * gR[1] + qz * gR[2] + qy * gR[3] - 2 * qx * gR[4] - qw * gR[5] + qz * gR[6] + qw * gR[7] - 2 * qx * gR[8]);
-        const double gqy = 2 * (-2 * qy * gR[0] + qx * gR[1] + qw * gR[2] + qx * gR[3] + qz * gR[5] - qw * gR[6] + qz * gR[7] - 2 * qy * gR[8]);
-        const double gqz = 2 * (-2 * qz * gR[0] - qw * gR[1] + qx * gR[2] + qw * gR[3] - 2 * qz * gR[4] + qy * gR[5] + qx * gR[6] + qy * gR[7]);
-        const double dq = qw * gqw + qx * gqx + qy * gqy + qz * gqz;
-        const double il = s->qlen > 0 ? 1 / s->qlen : 0;
-        g_quats[4 * i] = (gqw - qw * dq) * il;
-        g_quats[4 * i + 1] = (gqx - qx * dq) * il;
-        g_quats[4 * i + 2] = (gqy - qy * dq) * il;
-        g_quats[4 * i + 3] = (gqz - qz * dq) * il;
+        gauss_adjoint64(&cam, &f.sp[i], i, g2 + (size_t)i * 9, sh, K, D, g_means, g_log_scales, g_quats,
+                        g_logits, g_sh);
     }
     free(g2);
     free(cl);
     free(f.sp);
     free(f.order);
+    return 0;
+}
+
+/* ==== FP64 training render at full size: local queries for the gradient checks ===================
+ *
+ * The function of orc_train_forward_f64 / orc_train_backward_f64 (the same splat64, blending and
+ * thresholds) on scenes of millions of Gaussians, where every pixel against every splat is out of
+ * reach: the visible splats are kept in (depth, index) order with one list per 8x8 tile, the
+ * binning of render.cpp:159-190, and each query touches only the pixels it needs.
+ *   orc_big_create / orc_big_destroy   the frame: projection, depth order, tile lists
+ *   orc_big_image                      the FP64 colour of a pixel window
+ *   orc_big_adjoint                    the adjoint of a loss on a pixel window (dL/dcolour given
+ *                                      there): the raw-parameter gradients of every Gaussian
+ *   orc_big_fd                         the central difference, in one raw parameter, of the
+ *                                      whole-image L2 loss against a target, evaluated on the
+ *                                      pixels its Gaussian can reach (no other pixel changes), and
+ *                                      whether the renderer takes the same branches at +h and -h
+ *                                      (alpha cut, 0.99 clamp, early termination, depth order,
+ *                                      tile rectangle, SH clamp, Jacobian clip): if not, the loss
+ *                                      is not smooth on [-h, h] and the difference measures a jump.
+ * Parameters are the caller's float64 arrays (orc_train_forward_f64's layout), which must outlive
+ * the frame. */
+
+typedef struct {
+    double u, v, A, B, C, o, rgb[3];
+    float depth32;
+    uint32_t idx;
+    int x0, y0, x1, y1;
+} orc_bl64;
+
+typedef struct {
+    orc_cam64 cam;
+    int D, K;
+    double splat_scale;
+    int64_t n;
+    const double *means, *log_scales, *quats, *logits, *sh;
+    orc_bl64* rec;          /* visible splats in (depth32, index) order */
+    size_t visible;
+    int tx8, ty8;
+    uint64_t* tile_start;   /* tx8 * ty8 + 1 */
+    uint32_t* tile_list;    /* positions in rec, ascending within each tile (= depth order) */
+} orc_big64;
+
+static void to_bl64(const orc_sp64* s, int64_t i, orc_bl64* r) {
+    r->u = s->u; r->v = s->v; r->A = s->A; r->B = s->B; r->C = s->C; r->o = s->o;
+    for (int c = 0; c < 3; ++c) r->rgb[c] = s->rgb[c];
+    r->depth32 = s->depth32;
+    r->idx = (uint32_t)i;
+    r->x0 = s->x0; r->y0 = s->y0; r->x1 = s->x1; r->y1 = s->y1;
+}
+
+static int cmp_bl64(const void* a, const void* b) {
+    const orc_bl64* p = (const orc_bl64*)a;
+    const orc_bl64* q = (const orc_bl64*)b;
+    if (p->depth32 < q->depth32) return -1;
+    if (p->depth32 > q->depth32) return 1;
+    return p->idx < q->idx ? -1 : (p->idx > q->idx);
+}
+
+void orc_big_destroy(void* h) {
+    orc_big64* f = (orc_big64*)h;
+    if (!f) return;
+    free(f->rec);
+    free(f->tile_start);
+    free(f->tile_list);
+    free(f);
+}
+
+void* orc_big_create(int64_t n, const double* means, const double* log_scales, const double* quats,
+                     const double* logits, const double* sh, int K, const double* camd, int w, int h, int sh_degree,
+                     double splat_scale) {
+    orc_big64* f = (orc_big64*)calloc(1, sizeof *f);
+    if (!f) return NULL;
+    f->cam = cam64(camd, w, h);
+    f->D = sh_degree > 3 ? 3 : sh_degree;
+    f->K = K;
+    f->splat_scale = splat_scale;
+    f->n = n;
+    f->means = means; f->log_scales = log_scales; f->quats = quats; f->logits = logits; f->sh = sh;
+    if ((f->D + 1) * (f->D + 1) > K) { free(f); return NULL; }
+    f->rec = (orc_bl64*)malloc((n ? (size_t)n : 1) * sizeof(orc_bl64));
+    f->tx8 = (w + 7) / 8;
+    f->ty8 = (h + 7) / 8;
+    const size_t T = (size_t)f->tx8 * f->ty8;
+    f->tile_start = (uint64_t*)calloc(T + 1, sizeof(uint64_t));
+    if (!f->rec || !f->tile_start) { orc_big_destroy(f); return NULL; }
+    orc_sp64 s;
+    for (int64_t i = 0; i < n; ++i) {
+        splat64(&f->cam, means, log_scales, quats, logits, sh, K, f->D, splat_scale, i, &s);
+        if (s.alive) to_bl64(&s, i, &f->rec[f->visible++]);
+    }
+    qsort(f->rec, f->visible, sizeof(orc_bl64), cmp_bl64);
+    for (size_t k = 0; k < f->visible; ++k) {
+        const orc_bl64* r = &f->rec[k];
+        for (int ty = r->y0; ty <= r->y1; ++ty)
+            for (int tx = r->x0; tx <= r->x1; ++tx) ++f->tile_start[(size_t)ty * f->tx8 + tx + 1];
+    }
+    for (size_t t = 0; t < T; ++t) f->tile_start[t + 1] += f->tile_start[t];
+    f->tile_list = (uint32_t*)malloc((f->tile_start[T] ? f->tile_start[T] : 1) * sizeof(uint32_t));
+    uint64_t* fill = (uint64_t*)malloc((T ? T : 1) * sizeof(uint64_t));
+    if (!f->tile_list || !fill) { free(fill); orc_big_destroy(f); return NULL; }
+    memcpy(fill, f->tile_start, T * sizeof(uint64_t));
+    for (size_t k = 0; k < f->visible; ++k) {
+        const orc_bl64* r = &f->rec[k];
+        for (int ty = r->y0; ty <= r->y1; ++ty)
+            for (int tx = r->x0; tx <= r->x1; ++tx) f->tile_list[fill[(size_t)ty * f->tx8 + tx]++] = (uint32_t)k;
+    }
+    free(fill);
+    return f;
+}
+
+/* Counts of the frame: visible splats and (splat, 8x8 tile) pairs. */
+void orc_big_counts(const void* h, int64_t* visible, int64_t* pairs) {
+    const orc_big64* f = (const orc_big64*)h;
+    *visible = (int64_t)f->visible;
+    *pairs = (int64_t)f->tile_start[(size_t)f->tx8 * f->ty8];
+}
+
+static uint64_t mix64(uint64_t x) {
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdull; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull; x ^= x >> 33;
+    return x;
+}
+
+static int key_less64(float da, uint32_t ia, float db, uint32_t ib) { return da < db || (da == db && ia < ib); }
+
+/* One contributor of a pixel, for the adjoint: rec position (or -1 for the variant), alpha, T before,
+ * e^power, offsets, clamped. */
+typedef struct { int64_t pos; double alpha, T, ep, dx, dy; int clamped; } orc_bc64;
+
+/* Pixel (x, y) front to back (pixel64's rules). Gaussian `skip` (if >= 0) is left out and `var`
+ * (if not NULL) takes part in its place at its own (depth, index) position. col: colour; sig: a
+ * hash of the branches taken (applied contributors with their clamp state, the terminating
+ * splat); out (may be NULL): the applied contributors. Returns their count. */
+static size_t big_pixel(const orc_big64* f, int x, int y, int64_t skip, const orc_bl64* var, double* col,
+                        uint64_t* sig, orc_bc64* out) {
+    const double px = x + 0.5, py = y + 0.5;
+    const int tx = x / 8, ty = y / 8;
+    const size_t t = (size_t)ty * f->tx8 + tx;
+    uint64_t q = f->tile_start[t];
+    const uint64_t qe = f->tile_start[t + 1];
+    int var_in = var && tx >= var->x0 && tx <= var->x1 && ty >= var->y0 && ty <= var->y1;
+    double T = 1.0;
+    uint64_t hsh = 0x9e3779b97f4a7c15ull;
+    size_t m = 0;
+    col[0] = col[1] = col[2] = 0;
+    for (;;) {
+        const orc_bl64* c = NULL;
+        while (q < qe) {
+            c = &f->rec[f->tile_list[q]];
+            if ((int64_t)c->idx == skip) { ++q; c = NULL; continue; }
+            break;
+        }
+        const orc_bl64* s;
+        int64_t pos;
+        if (var_in && (!c || key_less64(var->depth32, var->idx, c->depth32, c->idx))) {
+            s = var; pos = -1; var_in = 0;
+        } else if (c) {
+            s = c; pos = (int64_t)f->tile_list[q]; ++q;
+        } else {
+            break;
+        }
+        const double dx = px - s->u, dy = py - s->v;
+        const double power = -0.5 * (s->A * dx * dx + s->C * dy * dy) - s->B * dx * dy;
+        if (power > 0) continue;
+        const double ep = exp(power);
+        const double e = s->o * ep;
+        const double alpha = e < 0.99 ? e : 0.99;
+        if (alpha < 1.0 / 255.0) continue;
+        const double nt = T * (1 - alpha);
+        if (nt < 1e-4) {
+            hsh = mix64(hsh ^ (0x8000000000000000ull | s->idx));
+            break;
+        }
+        for (int ch = 0; ch < 3; ++ch) col[ch] += s->rgb[ch] * alpha * T;
+        hsh = mix64(hsh ^ ((uint64_t)s->idx << 1 | (uint64_t)!(e < 0.99)));
+        if (out) {
+            out[m].pos = pos; out[m].alpha = alpha; out[m].T = T; out[m].ep = ep;
+            out[m].dx = dx; out[m].dy = dy; out[m].clamped = !(e < 0.99);
+        }
+        ++m;
+        T = nt;
+    }
+    if (sig) *sig += mix64(hsh ^ ((uint64_t)y << 32 | (uint32_t)x));
+    return m;
+}
+
+/* FP64 colour of the window [x0, x0 + ww) x [y0, y0 + wh): out ww * wh * 3 doubles. */
+int orc_big_image(const void* h, int x0, int y0, int ww, int wh, double* out) {
+    const orc_big64* f = (const orc_big64*)h;
+    if (x0 < 0 || y0 < 0 || ww < 0 || wh < 0 || x0 + ww > f->cam.w || y0 + wh > f->cam.h) return 1;
+    for (int y = 0; y < wh; ++y)
+        for (int x = 0; x < ww; ++x) big_pixel(f, x0 + x, y0 + y, -1, NULL, out + ((size_t)y * ww + x) * 3, NULL, NULL);
+    return 0;
+}
+
+/* The adjoint of a loss whose gradient with respect to the colour is grad (ww * wh * 3 doubles) on the
+ * window and zero elsewhere: adds nothing, writes the raw-parameter gradients of every Gaussian that
+ * contributes to a window pixel (the others are left as the caller set them, normally zero). */
+int orc_big_adjoint(const void* h, int x0, int y0, int ww, int wh, const double* grad, double* g_means,
+                    double* g_log_scales, double* g_quats, double* g_logits, double* g_sh) {
+    const orc_big64* f = (const orc_big64*)h;
+    if (x0 < 0 || y0 < 0 || ww < 0 || wh < 0 || x0 + ww > f->cam.w || y0 + wh > f->cam.h) return 1;
+    double* g2 = (double*)calloc((f->visible ? f->visible : 1) * 9, sizeof(double));
+    unsigned char* touched = (unsigned char*)calloc(f->visible ? f->visible : 1, 1);
+    orc_bc64* cl = (orc_bc64*)malloc((f->visible ? f->visible : 1) * sizeof(orc_bc64));
+    if (!g2 || !touched || !cl) { free(g2); free(touched); free(cl); return 2; }
+    for (int y = 0; y < wh; ++y)
+        for (int x = 0; x < ww; ++x) {
+            double col[3];
+            const size_t m = big_pixel(f, x0 + x, y0 + y, -1, NULL, col, NULL, cl);
+            const double* gc = grad + ((size_t)y * ww + x) * 3;
+            double acc[3] = {0, 0, 0};
+            for (size_t q = m; q-- > 0;) {
+                const orc_bc64* c = &cl[q];
+                const orc_bl64* s = &f->rec[c->pos];
+                double* g = g2 + (size_t)c->pos * 9;
+                touched[c->pos] = 1;
+                const double wgt = c->alpha * c->T;
+                double dalpha = 0;
+                for (int ch = 0; ch < 3; ++ch) {
+                    g[6 + ch] += gc[ch] * wgt;
+                    dalpha += gc[ch] * (s->rgb[ch] * c->T - acc[ch] / (1 - c->alpha));
+                    acc[ch] += s->rgb[ch] * wgt;
+                }
+                if (c->clamped) continue;
+                g[5] += dalpha * c->ep;
+                const double dpow = dalpha * c->alpha;
+                const double dx = c->dx, dy = c->dy;
+                g[2] += dpow * (-0.5 * dx * dx);
+                g[3] += dpow * (-dx * dy);
+                g[4] += dpow * (-0.5 * dy * dy);
+                g[0] += dpow * (s->A * dx + s->B * dy);
+                g[1] += dpow * (s->C * dy + s->B * dx);
+            }
+        }
+    orc_sp64 s;
+    for (size_t k = 0; k < f->visible; ++k) {
+        if (!touched[k]) continue;
+        const int64_t i = f->rec[k].idx;
+        splat64(&f->cam, f->means, f->log_scales, f->quats, f->logits, f->sh, f->K, f->D, f->splat_scale, i, &s);
+        gauss_adjoint64(&f->cam, &s, i, g2 + k * 9, f->sh, f->K, f->D, g_means, g_log_scales, g_quats, g_logits,
+                        g_sh);
+    }
+    free(g2);
+    free(touched);
+    free(cl);
+    return 0;
+}
+
+/* The splat of Gaussian i with raw parameter (group, comp) moved by delta; group 0 means (3),
+ * 1 log-scales (3), 2 quaternion (4), 3 opacity logit (1), 4 SH (K x 3). */
+static void moved_splat(const orc_big64* f, int64_t i, int group, int comp, double delta, orc_sp64* s) {
+    double m[3], ls[3], q[4], lg[1];
+    double shv[75];
+    const int K3 = f->K * 3;
+    for (int k = 0; k < 3; ++k) { m[k] = f->means[3 * i + k]; ls[k] = f->log_scales[3 * i + k]; }
+    for (int k = 0; k < 4; ++k) q[k] = f->quats[4 * i + k];
+    lg[0] = f->logits[i];
+    for (int k = 0; k < K3 && k < 75; ++k) shv[k] = f->sh[(size_t)i * K3 + k];
+    double* p = group == 0 ? m : group == 1 ? ls : group == 2 ? q : group == 3 ? lg : shv;
+    p[comp] += delta;
+    splat64(&f->cam, m, ls, q, lg, shv, f->K, f->D, f->splat_scale, 0, s);
+}
+
+/* Central difference of L = sum over all pixels and channels of (colour - target)^2 (target: the
+ * full w x h x 3 image, float32) in raw parameter (group, comp) of Gaussian i, step h:
+ * *fd = (L(+h) - L(-h)) / 2h, evaluated on the tiles either moved splat touches. *smooth = 1 when
+ * both evaluations take the same branches (then L is smooth on [-h, h] up to a branch flipping and
+ * flipping back inside it); *pixels = the pixels evaluated. Returns nonzero on bad arguments. */
+int orc_big_fd(const void* hnd, const float* target, int64_t i, int group, int comp, double step, double* fd,
+               int* smooth, int64_t* pixels) {
+    const orc_big64* f = (const orc_big64*)hnd;
+    const int sizes[5] = {3, 3, 4, 1, f->K * 3};
+    if (i < 0 || i >= f->n || group < 0 || group > 4 || comp < 0 || comp >= sizes[group] || f->K * 3 > 75) return 1;
+    orc_sp64 sp, sm;
+    moved_splat(f, i, group, comp, step, &sp);
+    moved_splat(f, i, group, comp, -step, &sm);
+    orc_bl64 bp, bm;
+    if (sp.alive) to_bl64(&sp, i, &bp);
+    if (sm.alive) to_bl64(&sm, i, &bm);
+    int same = sp.alive == sm.alive;
+    if (same && sp.alive) {
+        same = sp.x0 == sm.x0 && sp.y0 == sm.y0 && sp.x1 == sm.x1 && sp.y1 == sm.y1 && sp.clx == sm.clx &&
+               sp.cly == sm.cly;
+        for (int c = 0; c < 3; ++c) same = same && ((sp.pre[c] > 0) == (sm.pre[c] > 0));
+    }
+    /* the tiles either moved splat touches (outside them both evaluations leave Gaussian i out) */
+    int tx0 = f->tx8, ty0 = f->ty8, tx1 = -1, ty1 = -1;
+    const orc_sp64* both[2] = {&sp, &sm};
+    for (int k = 0; k < 2; ++k)
+        if (both[k]->alive) {
+            if (both[k]->x0 < tx0) tx0 = both[k]->x0;
+            if (both[k]->y0 < ty0) ty0 = both[k]->y0;
+            if (both[k]->x1 > tx1) tx1 = both[k]->x1;
+            if (both[k]->y1 > ty1) ty1 = both[k]->y1;
+        }
+    double diff = 0;
+    uint64_t sig_p = 0, sig_m = 0;
+    int64_t count = 0;
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx)
+            for (int y = ty * 8; y < ty * 8 + 8 && y < f->cam.h; ++y)
+                for (int x = tx * 8; x < tx * 8 + 8 && x < f->cam.w; ++x) {
+                    double cp[3], cm[3];
+                    big_pixel(f, x, y, i, sp.alive ? &bp : NULL, cp, &sig_p, NULL);
+                    big_pixel(f, x, y, i, sm.alive ? &bm : NULL, cm, &sig_m, NULL);
+                    const float* t = target + ((size_t)y * f->cam.w + x) * 3;
+                    for (int c = 0; c < 3; ++c) diff += (cp[c] - cm[c]) * (cp[c] + cm[c] - 2.0 * (double)t[c]);
+                    ++count;
+                }
+    *fd = diff / (2 * step);
+    *smooth = same && sig_p == sig_m;
+    *pixels = count;
     return 0;
 }
