@@ -106,6 +106,11 @@ struct Arena {
     DevBuf<Ctrl> ctrl;
     DevBuf<unsigned> sort_scratch;          // per-span digit counts of the pass in flight
     DevBuf<unsigned long long> span_sum;    // pairs per span of the pair-offset scan
+    // The persistent sort (one CTA per SM, `ctas` of them; 0 = the multi-kernel sort runs): two
+    // CTA-major count matrices and the entry holding each CTA's first expansion pair.
+    unsigned ctas = 0;
+    DevBuf<unsigned> pcounts;
+    DevBuf<unsigned> chunk_first;
 
     int init(int64_t count, unsigned cap) {
         n = count;
@@ -119,7 +124,12 @@ struct Arena {
         }
         AB_TRY(ctrl.reserve(1, true));
         AB_TRY(sort_scratch.reserve(2 * sort_scratch_words()));  // two count matrices and the totals
-        AB_TRY(span_sum.reserve(sort_span_sums()));
+        ctas = persistent_sort_ctas();
+        AB_TRY(span_sum.reserve(std::max<size_t>(sort_span_sums(), ctas)));
+        if (ctas) {
+            AB_TRY(pcounts.reserve(2 * persistent_sort_count_words(ctas)));
+            AB_TRY(chunk_first.reserve(ctas + 1));
+        }
         AB_TRY(offs.reserve(nn));
         AB_TRY(rank.reserve(nn));
         AB_TRY(rect_sorted.reserve(nn));
@@ -171,13 +181,49 @@ int tile_pass_widths(unsigned tiles, int max_bits, int widths[4]) {
 unsigned* count_matrix(Arena& A, int q) { return A.sort_scratch.p + (q & 1) * sort_count_words(); }
 
 // The digit counts of the first depth pass when the preprocess accumulates them (the frame is
-// small enough), else {NULL}. *zero_words: the cells frame_begin must clear for it.
+// small enough), else {NULL}. *zero_words: the cells frame_begin must clear for it. The persistent
+// sort chunks the pass over its CTAs and keeps the matrix CTA-major; the multi-kernel sort over
+// its spans, digit-major.
 PassCounts first_pass_counts(Arena& A, unsigned entries, unsigned* zero_words) {
     *zero_words = 0;
     if (entries == 0 || entries > kProducerCountMax) return PassCounts{};
+    if (A.ctas) {
+        *zero_words = A.ctas << kDepthBits;
+        return PassCounts{A.pcounts.p, A.ctas, 0u, (1u << kDepthBits) - 1, 1u, 1u << kDepthBits};
+    }
     const unsigned spans = sort_spans(entries);
     *zero_words = spans << kDepthBits;
-    return PassCounts{count_matrix(A, 0), spans, 0u, (1u << kDepthBits) - 1};
+    return PassCounts{count_matrix(A, 0), spans, 0u, (1u << kDepthBits) - 1, spans, 1u};
+}
+
+// Steps 2-4 of a frame as one cooperative launch (sort_persistent.cu); *final_buf as enqueue_sort.
+int enqueue_sort_persistent(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank,
+                            int bits, bool first_counted, cudaStream_t st, int* final_buf) {
+    SortFrameArgs a{};
+    a.depth_key = A.depth_key.p;
+    a.rect16 = A.rect16.p;
+    for (int k = 0; k < 2; ++k) {
+        a.vis_key[k] = A.vis_key[k].p;
+        a.vis_idx[k] = A.vis_idx[k].p;
+        a.pair_key[k] = A.pair_key[k].p;
+        a.pair_val[k] = A.pair_val[k].p;
+        a.counts[k] = A.pcounts.p + k * persistent_sort_count_words(A.ctas);
+    }
+    a.offs = A.offs.p;
+    a.rank = keep_rank ? A.rank.p : nullptr;
+    a.rect_sorted = A.rect_sorted.p;
+    a.chunk_first = A.chunk_first.p;
+    a.span_sum = A.span_sum.p;
+    a.ranges = A.ranges.p;
+    a.ctrl = A.ctrl.p;
+    a.tables = tables;
+    a.entries = entries;
+    a.pair_cap = A.pair_cap;
+    a.tile_passes = tile_pass_widths(tiles, bits, a.tile_bits);
+    a.first_counted = first_counted ? 1 : 0;
+    AB_CUDA(launch_sort_frame(a, A.ctas, st));
+    *final_buf = a.tile_passes & 1;
+    return 0;
 }
 
 // Depth passes over `entries` depth keys (the first compacts the visible ones), pair scan and
@@ -189,9 +235,12 @@ PassCounts first_pass_counts(Arena& A, unsigned entries, unsigned* zero_words) {
 // that count matrix first; every other pass has its own upsweep. (Counting in the downsweeps too
 // was measured slower: keys written next to each other often share the next digit, the high depth
 // digits taking few values, so one atomic per key contends -- 0.177 ms against 0.139 ms for the
-// sort of the 740k / 1280x720 frame.)
+// sort of the 740k / 1280x720 frame.) Where the persistent sort can run (A.ctas), it replaces this
+// whole sequence with one launch and the same outputs.
 int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank, int bits,
                  bool first_counted, cudaStream_t st, int* final_buf) {
+    if (A.ctas)
+        return enqueue_sort_persistent(A, entries, tiles, tables, keep_rank, bits, first_counted, st, final_buf);
     Ctrl* ctrl = A.ctrl.p;
     const unsigned cap = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
     unsigned* totals = A.sort_scratch.p + 2 * sort_count_words();
@@ -200,8 +249,9 @@ int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& 
     const bool expand_counts = A.pair_cap <= kProducerCountMax;
     const unsigned tile_spans = sort_spans(A.pair_cap);
     const PassCounts first_tile =
-        expand_counts ? PassCounts{count_matrix(A, kDepthPasses), tile_spans, 0u, (1u << tile_bits[0]) - 1}
-                      : PassCounts{};
+        expand_counts
+            ? PassCounts{count_matrix(A, kDepthPasses), tile_spans, 0u, (1u << tile_bits[0]) - 1, tile_spans, 1u}
+            : PassCounts{};
 
     for (int p = 0; p < kDepthPasses; ++p) {
         const int src = (p + 1) & 1, dst = p & 1;  // pass 0 reads depth_key and writes buffer 0
@@ -531,6 +581,8 @@ int settle(Arena& A, const Ctrl& h, int* again, bool all_frames) {
     *again = 0;
     const unsigned flags = h.flags | (all_frames ? h.sticky_flags : 0u);
     const uint64_t pairs = all_frames ? std::max(h.pair_total, h.max_pair_total) : h.pair_total;
+    if (flags & kFlagWaitTimeout)  // the persistent sort's bounded grid-barrier wait gave up
+        return fail(ANISO_B200_ERR_DEVICE_WAIT, "a sort grid barrier wait gave up: the frame was not rendered");
     if (flags & kFlagOverflow) {
         const uint64_t need = pairs + pairs / 4 + 1024;
         if (need > kMaxPairs) return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 splat-tile pairs");

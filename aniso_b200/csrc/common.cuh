@@ -128,7 +128,7 @@ struct Ctrl {
     unsigned int vis_count;             // visible entries
     unsigned int flags;                 // kFlag* bits, read back by the host after the frame
     unsigned int sticky_flags;          // OR of the flags of earlier frames since the host last read it
-    unsigned int pad;
+    unsigned int sort_barrier;          // arrivals at the persistent sort's grid barriers (cleared per frame)
     unsigned long long max_pair_total;  // largest pair_total of earlier frames since then
 };
 
@@ -137,7 +137,8 @@ struct Ctrl {
 constexpr unsigned kCulledKey = 0xFFFFFFFFu;
 
 enum : unsigned {
-    kFlagOverflow = 1u,  // pairs exceeded the pair capacity: nothing after duplication ran
+    kFlagOverflow = 1u,     // pairs exceeded the pair capacity: nothing after duplication ran
+    kFlagWaitTimeout = 2u,  // a bounded grid-barrier wait gave up (never expected): the frame is void
 };
 
 // ---- digit counts of an LSD pass, accumulated by the kernel that writes the pass's keys ---------
@@ -145,10 +146,11 @@ enum : unsigned {
 // CTA each; span b holds blocks [T b / spans, T (b + 1) / spans) of the T = ceil(items / block)).
 // It needs, per (digit, span), the number of items. Instead of a counting kernel that re-reads
 // the keys, the kernel that writes them adds each key to its cell as it goes:
-//   counts[digit(key) * spans + span(position)] += 1,
+//   counts[digit(key) * digit_stride + span(position) * span_stride] += 1,
 // with span(position) = ((position / kSortBlockItems + 1) * spans - 1) / T (the span whose block
-// range holds the position). The cells must be zero beforehand; integer adds make the totals
-// independent of their order.
+// range holds the position). The multi-kernel sort keeps the matrix digit-major (digit_stride =
+// spans, span_stride = 1), the persistent sort span-major (1, radix). The cells must be zero
+// beforehand; integer adds make the totals independent of their order.
 constexpr unsigned kSortBlockItems = 2048;
 
 struct PassCounts {
@@ -156,6 +158,8 @@ struct PassCounts {
     unsigned spans;
     unsigned shift;
     unsigned mask;     // radix - 1
+    unsigned digit_stride;
+    unsigned span_stride;
 };
 
 __device__ __forceinline__ unsigned span_of(unsigned position, unsigned spans, unsigned blocks) {
@@ -163,7 +167,9 @@ __device__ __forceinline__ unsigned span_of(unsigned position, unsigned spans, u
 }
 
 __device__ __forceinline__ void count_key(const PassCounts& pc, unsigned blocks, unsigned position, unsigned key) {
-    atomicAdd(&pc.counts[((key >> pc.shift) & pc.mask) * pc.spans + span_of(position, pc.spans, blocks)], 1u);
+    atomicAdd(&pc.counts[((key >> pc.shift) & pc.mask) * pc.digit_stride +
+                         span_of(position, pc.spans, blocks) * pc.span_stride],
+              1u);
 }
 
 // ---- programmatic dependent launch --------------------------------------------------------------

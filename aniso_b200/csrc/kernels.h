@@ -104,6 +104,39 @@ void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capac
 void launch_projection_keys(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
                             unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream);
 
+// ---- the persistent sort: steps 2-4 of a frame (depth passes, pair scan and expansion, tile
+// passes, tile ranges) as ONE cooperative launch of one 1024-thread CTA per SM, its phases
+// separated by grid barriers whose waits are bounded (sort_persistent.cu). Same outputs as the
+// multi-kernel sequence above, bit for bit.
+struct SortFrameArgs {
+    const unsigned* depth_key;            // [entries] depth bits, kCulledKey when culled
+    const unsigned long long* rect16;     // [entries] tile rectangles of visible entries
+    unsigned* vis_key[2];                 // [entries] ping-pong depth passes
+    unsigned* vis_idx[2];
+    unsigned* pair_key[2];                // [pair_cap] ping-pong tile passes
+    unsigned* pair_val[2];
+    unsigned* offs;                       // [entries] pair offset of each depth-sorted entry
+    unsigned* rank;                       // [entries] depth-sorted position of each entry, or NULL
+    unsigned long long* rect_sorted;      // [entries]
+    unsigned* chunk_first;                // [ctas + 1] entry holding each expansion chunk's first pair
+    unsigned long long* span_sum;         // [ctas] pairs of each CTA's share of the sorted entries
+    unsigned* counts[2];                  // two count matrices of ctas x 512 words (CTA-major)
+    uint2* ranges;                        // [tiles], cleared beforehand
+    Ctrl* ctrl;
+    BatchTables tables;
+    unsigned entries;
+    unsigned pair_cap;
+    int tile_passes;
+    int tile_bits[4];
+    int first_counted;                    // counts[0] holds depth pass 0's digit counts already
+};
+// CTAs of the persistent sort on the current device (one per SM), 0 if it cannot run there (no
+// cooperative launch, or not one CTA per SM resident); ANISO_B200_SORT=multi in the environment
+// also gives 0 (the multi-kernel sequence then runs).
+unsigned persistent_sort_ctas();
+size_t persistent_sort_count_words(unsigned ctas);  // words of one count matrix
+cudaError_t launch_sort_frame(const SortFrameArgs& args, unsigned ctas, cudaStream_t stream);
+
 // Blends every tile of a batch (blockIdx = global tile); outputs go to each view's ViewInfo.
 // train: also the float colour, final transmittance and last contributor per pixel.
 bool blend_shape_supported(int tile_w, int tile_h);

@@ -197,11 +197,20 @@ __device__ __forceinline__ bool project(const float4 pg, const Cov3& cov, const 
     const float c = TS[1][0] * T[1][0] + TS[1][1] * T[1][1] + TS[1][2] * T[1][2] + 0.3f;
     const float det = a * c - b * b;
     if (det <= 0) return false;
+    // A projection that is not finite (a NaN or infinite position, scale or rotation, or an
+    // overflow on the way) or a radius of a billion pixels or more is culled. The reference leaves
+    // these cases to undefined float-to-int conversions (render.cpp:84-89, gpu_render.cu:126-132),
+    // which on x86-64 leave such a splat with no tile; culling them gives that image everywhere.
+    // Finite, representable projections are unaffected (bit for bit).
+    if (!(isfinite(a) && isfinite(b) && isfinite(c) && isfinite(det))) return false;
 
     const float mid = 0.5f * (a + c);
     const float lambda = mid + sqrtf(fmaxf(0.1f, mid * mid - det));
-    const int radius = (int)ceilf(3.0f * sqrtf(lambda));
+    const float r3 = 3.0f * sqrtf(lambda);
+    if (!(r3 < 1.0e9f)) return false;
+    const int radius = (int)ceilf(r3);
     const float u = cam.fx * px / pz + cam.cx, v = cam.fy * py / pz + cam.cy;
+    if (!(isfinite(u) && isfinite(v))) return false;
     if (u + radius < 0 || v + radius < 0 || u - radius >= cam.width || v - radius >= cam.height) return false;
 
     const int x0 = max(0, (int)(u - radius) / tile_w), y0 = max(0, (int)(v - radius) / tile_h);

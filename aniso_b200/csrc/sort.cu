@@ -60,6 +60,7 @@ __global__ void frame_begin_kernel(Ctrl* ctrl, unsigned* __restrict__ zero, unsi
         ctrl->pair_total = 0;
         ctrl->vis_count = 0;
         ctrl->flags = 0;
+        ctrl->sort_barrier = 0;
     }
     const unsigned stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
     for (unsigned i = first; i < zero_words; i += stride) zero[i] = 0;  // at most 512 x 592 words
@@ -546,7 +547,7 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(const unsigned* __rest
     __syncthreads();
     const unsigned span = span_of(base, first.spans, (P + kSortBlockItems - 1) / kSortBlockItems);
     for (unsigned d = tid; d <= first.mask; d += kThreads)
-        if (s_hist[d]) atomicAdd(&first.counts[d * first.spans + span], s_hist[d]);
+        if (s_hist[d]) atomicAdd(&first.counts[d * first.digit_stride + span * first.span_stride], s_hist[d]);
 }
 
 // ranges[tile] = [first, last + 1) over the sorted tile keys; four keys per thread and step.

@@ -315,10 +315,87 @@ def fwd_bwd_leg(torch, steps: int):
         torch.cuda.synchronize()
     ms_f = e0.elapsed_time(e1) / steps
     finite = all(bool(torch.isfinite(p.grad).all()) for p in ps)
+    # What the checker needs (outside any timed region): the last step's gradients and the image
+    # and target they came from.
+    with torch.no_grad():
+        image = rasterize(*ps, cam)
+    check = {"raw": raw, "cam": cam, "grads": [p.grad.cpu().numpy().astype(np.float64) for p in ps],
+             "image": image.cpu().numpy().astype(np.float64), "target": target.cpu().numpy()}
+    del ps, target, image
+    torch.cuda.empty_cache()
+
+    # The plain forward (RGB8, the GpuRenderer::render path) of the same 2.2M scene and view.
+    from aniso_b200 import GpuRenderer
+
+    r = GpuRenderer.from_raw(raw)
+    first = r.render(cam)  # sizes the pair buffers
+    out = torch.empty(cam.height, cam.width, 3, dtype=torch.uint8, device="cuda")
+    plain_stream = torch.cuda.Stream()
+    for _ in range(3):
+        r.render_device(cam, out.data_ptr(), plain_stream.cuda_stream)
+    r.sync()
+    e0.record(plain_stream)
+    for _ in range(steps):
+        r.render_device(cam, out.data_ptr(), plain_stream.cuda_stream)
+    e1.record(plain_stream)
+    r.sync()
+    ms_plain = e0.elapsed_time(e1) / steps
+    pinned = torch.empty(cam.height, cam.width, 3, dtype=torch.uint8).pin_memory().numpy()
+    for _ in range(3):
+        r.render(cam, out=pinned)
+    t = time.perf_counter()
+    for _ in range(steps):
+        r.render(cam, out=pinned)
+    ms_plain_e2e = 1000 * (time.perf_counter() - t) / steps
+    check["rgb8"] = first
+    check["rgb8_same_as_device"] = bool(np.array_equal(out.cpu().numpy(), first))
+    del r
     return {"workload": "2.2M-Gaussian SH3 scene (30x8x30 box), 1280x720, L2 loss vs the perturbed-scene target, "
                         "grads of all 59 raw parameters through torch.autograd.Function",
             "ms_per_view_fwd_bwd": ms, "ms_per_view_fwd_train": ms_f, "gaussians": raw.n,
-            "grads_finite": finite, "target_ms": 3.0}
+            "grads_finite": finite, "target_ms": 3.0,
+            "plain_forward": {"ms_per_frame": ms_plain, "ms_per_frame_e2e": ms_plain_e2e,
+                              "gaussians_per_s": raw.n / (ms_plain / 1000.0), "target_ms": 1.0,
+                              "path": "aniso_b200_render_device (device-timed); e2e: aniso_b200_render into "
+                                      "pinned host memory"}}, check
+
+
+def accuracy_checks(check):
+    """The checker, on the CPU after the timed legs (the FP64 oracle and the reference CPU
+    renderer): the 2.2M plain forward against render.cpp, and the 2.2M gradients against FP64
+    central differences on 256 sampled parameters and against the FP64 adjoint of every gradient."""
+    import oracle
+    from oracle import gradcheck
+
+    out = {}
+    raw, cam = check["raw"], check["cam"]
+    gauss, sh = oracle.Restatement().activate(raw)
+    if oracle.ReferenceCPU.available():
+        cpu = oracle.ReferenceCPU().scene(gauss, sh, 3).render(cam)[0]
+        vs = "reference render.cpp"
+    else:
+        cpu = oracle.Restatement().render(gauss, sh, 3, cam)[0]
+        vs = "C restatement of render.cpp"
+    d = np.abs(check["rgb8"].astype(np.int32) - cpu.astype(np.int32))
+    out["plain_forward_accuracy"] = {"max_abs_255": int(d.max()), "psnr_db": oracle.psnr(check["rgb8"], cpu),
+                                     "vs": vs, "device_equals_host_render": check["rgb8_same_as_device"]}
+    params = [p.astype(np.float64) for p in gradcheck.raw_param_arrays(raw)]
+    big = oracle.Restatement().big_frame(params, cam)
+    grads = check["grads"]
+    live = np.nonzero(np.abs(grads[0]).sum(1) > 0)[0]
+    fd = gradcheck.fd_check(big, check["target"], grads, live, samples=256, step=1e-4)
+    adj = gradcheck.window_check(big, 0, 0, 2 * (check["image"] - check["target"]), grads)
+    ref_img = big.image(0, 0, cam.width, cam.height)
+    out["grad_rel_err"] = {
+        "vs_fp64_fd": {k: fd[k] for k in gradcheck.GROUPS},
+        "fd_totals": fd["_totals"],
+        "vs_fp64_adjoint": adj,
+        "forward_max_abs_vs_fp64": float(np.abs(check["image"] - ref_img).max()),
+        "bar": 1e-3,
+        "rel": "||g_gpu - g_ref||_2 / ||g_ref||_2 per group; FD draws whose +h and -h renders take "
+               "different branches (alpha cut, clamp, termination, order, rectangle) are redrawn"}
+    big.close()
+    return out
 
 
 def reference_gpu_leg(gauss, sh, cams, rounds: int = 2):
@@ -436,7 +513,8 @@ def main():
     torch.cuda.set_device(local)
     if args.only:
         if rank == 0:
-            leg = {"batched": batched_leg, "fwd_bwd": fwd_bwd_leg, "train_batch": train_batch_leg}[args.only]
+            leg = {"batched": batched_leg, "fwd_bwd": lambda t, s: fwd_bwd_leg(t, s)[0],
+                   "train_batch": train_batch_leg}[args.only]
             print(json.dumps({"leg": args.only, **leg(torch, args.steps)}), flush=True)
         return
     dist = None
@@ -552,8 +630,9 @@ def main():
         extra = {}
         if not args.no_extra:
             extra["batched"] = batched_leg(torch, max(3, min(args.steps, 10)))
-            extra["fwd_bwd"] = fwd_bwd_leg(torch, max(3, min(args.steps, 10)))
+            extra["fwd_bwd"], check = fwd_bwd_leg(torch, max(3, min(args.steps, 10)))
             extra["train_batch"] = train_batch_leg(torch, 2)
+            extra["fwd_bwd"].update(accuracy_checks(check))
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "ms_per_frame": ms_step / V,
