@@ -6,4 +6,5 @@ missing; there is no CPU path.
 """
 from . import scenes  # noqa: F401  (pure numpy, no library needed)
 from ._lib import AnisoError, LIB_PATH  # noqa: F401
-from .renderer import BatchOptions, BatchRenderer, GpuRenderer, RenderOptions, keys_of, sort_projection  # noqa: F401
+from .renderer import (BatchOptions, BatchRenderer, GpuRenderer, RenderOptions, colmap_load, keys_of,  # noqa: F401
+                       sort_projection)

@@ -50,6 +50,7 @@ EXPORTS = [
     "aniso_b200_sort_projection_noalloc",
     "aniso_b200_scene_load_ply",
     "aniso_b200_adam_step",
+    "aniso_b200_colmap_load",
 ]
 
 
@@ -57,6 +58,10 @@ class Camera(ctypes.Structure):
     _fields_ = [("R", ctypes.c_double * 9), ("t", ctypes.c_double * 3), ("fx", ctypes.c_double),
                 ("fy", ctypes.c_double), ("cx", ctypes.c_double), ("cy", ctypes.c_double),
                 ("width", ctypes.c_int32), ("height", ctypes.c_int32)]
+
+
+class ColmapCamera(ctypes.Structure):
+    _fields_ = [("camera", Camera), ("image_name", ctypes.c_char * 256)]
 
 
 class Options(ctypes.Structure):
@@ -134,6 +139,7 @@ def _load():
         "aniso_b200_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(I64)],
         "aniso_b200_frame_kernels": [P, ctypes.POINTER(ctypes.c_int32)],
+        "aniso_b200_colmap_load": [ctypes.c_char_p, ctypes.POINTER(ColmapCamera), I32, ctypes.POINTER(I32)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

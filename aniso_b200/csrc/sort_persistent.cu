@@ -415,6 +415,7 @@ __device__ void expand_phase(const SortFrameArgs& a, const unsigned* sorted_idx,
     unsigned plo, phi;
     chunk_of(P, plo, phi);
     unsigned j_start = plo < phi ? __ldcg(a.chunk_first + blockIdx.x) : 0u;
+    if (j_start >= V) j_start = V > 0 ? V - 1 : 0u;  // never taken (every chunk start is marked); keeps reads in bounds
     __syncthreads();
     unsigned* pk = a.pair_key[0];
     unsigned* pv = a.pair_val[0];

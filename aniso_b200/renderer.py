@@ -226,6 +226,24 @@ def keys_of(tiles: np.ndarray, values: np.ndarray, depth: np.ndarray) -> np.ndar
     return (tiles.astype(np.uint64) << np.uint64(32)) | bits[values].astype(np.uint64)
 
 
+def colmap_load(folder) -> list:
+    """aniso::loadColmapCameras through the C ABI (aniso_b200_colmap_load): the binary model when
+    cameras.bin exists, else the text one; scenes.Camera objects sorted by image name."""
+    from .scenes import Camera
+
+    path = os.fsencode(folder)
+    count = ctypes.c_int32(0)
+    check(lib.aniso_b200_colmap_load(path, None, 0, ctypes.byref(count)))
+    arr = (_lib.ColmapCamera * max(count.value, 1))()
+    check(lib.aniso_b200_colmap_load(path, arr, count.value, ctypes.byref(count)))
+    out = []
+    for k in range(count.value):
+        c = arr[k].camera
+        out.append(Camera(c.width, c.height, c.fx, c.fy, c.cx, c.cy, np.array(c.R[:], np.float64).reshape(3, 3),
+                          np.array(c.t[:], np.float64), arr[k].image_name.decode()))
+    return out
+
+
 @dataclasses.dataclass
 class BatchOptions:
     """aniso_b200_batch_options: colour options plus the launch shape (tile, blend batch, graph,

@@ -126,6 +126,20 @@ int aniso_b200_frame_kernels(aniso_b200_scene* scene, int32_t* kernels);
 /* Copies the last error message (NUL-terminated, truncated to len) and returns its full length. */
 size_t aniso_b200_last_error(char* buf, size_t len);
 
+/* One camera of a COLMAP sparse model: aniso::Camera (camera.h:16-26), image name included. */
+typedef struct aniso_b200_colmap_camera {
+    aniso_b200_camera camera;
+    char image_name[256];  /* NUL-terminated */
+} aniso_b200_colmap_camera;
+
+/* aniso::loadColmapCameras (camera.h:51, camera.cpp:105-140) with COLMAP's text format added:
+ * reads `folder`'s cameras.bin + images.bin when cameras.bin exists (the reference's format, its
+ * rules and messages), else cameras.txt + images.txt. PINHOLE and SIMPLE_PINHOLE only (a model
+ * with lens distortion is refused, camera.cpp:82-85); each image's quaternion normalised in double
+ * into R; cameras sorted by image name. Host code only (no device needed). Two calls: with out ==
+ * NULL only *count is set; then capacity >= *count entries of out are filled. */
+int aniso_b200_colmap_load(const char* folder, aniso_b200_colmap_camera* out, int32_t capacity, int32_t* count);
+
 /* ---- batches (no counterpart in the reference, whose multi-view caller renders views one by one
  * with two host syncs each, main.cpp:233-244): many views of several scenes rendered by one fixed
  * launch sequence. Every Gaussian is read once and projected for all views of its scene; one
