@@ -208,16 +208,8 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_backward_kernel(BackwardIn 
             s_r0[slot] = r.r0;
             s_r1[slot] = r.r1;
             s_b[slot] = r.r2.x;
-            const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
-            const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
-            unsigned cols = 0, m = 0;
-#pragma unroll
-            for (int c = 0; c < kWarpsX; ++c)
-                if (overlaps(xlo, xhi, ox + 8 * c, ox + 8 * c + 7)) cols |= 1u << c;
-#pragma unroll
-            for (int rr = 0; rr < TH / 8; ++rr)
-                if (overlaps(ylo, yhi, oy + 8 * rr, oy + 8 * rr + 7)) m |= cols << (kWarpsX * rr);
-            s_mask[slot] = static_cast<unsigned char>(m);
+            // The forward's masks (the same function), so the adjoint walks exactly its splats.
+            s_mask[slot] = static_cast<unsigned char>(splat_block_mask<TW, TH>(r, ox, oy));
             s_hit[slot] = 0;
             const unsigned j = in.rank[g];
             const unsigned long long rc = in.rect_sorted[j];

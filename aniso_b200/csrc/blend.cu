@@ -111,8 +111,13 @@ __device__ __forceinline__ void write_tile_rgb8(const unsigned char* s_px, uint8
     }
 }
 
+// Resident CTAs per SM the blend is compiled for: as many as 40 registers a thread allow (the walk
+// is issue-bound and wants the warps; the block-mask test of the staging would otherwise raise the
+// whole kernel's register count), at most 32.
+constexpr int blend_min_ctas(int threads) { return 65536 / (42 * threads) < 32 ? 65536 / (42 * threads) : 32; }
+
 template <int TW, int TH, int kBatch, bool kTrain>
-__global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restrict__ ranges,
+__global__ void __launch_bounds__(TW * TH / 2, blend_min_ctas(TW * TH / 2)) blend_kernel(const uint2* __restrict__ ranges,
                                                             const unsigned* __restrict__ vals,
                                                             const SplatRecord* __restrict__ rec, const Ctrl* ctrl,
                                                             const ViewInfo* __restrict__ views, BatchTables tables) {
@@ -156,15 +161,7 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
                 s_r0[slot] = r.r0;
                 s_r1[slot] = r.r1;
                 s_b[slot] = r.r2.x;
-                const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
-                const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
-                unsigned cols = 0;
-#pragma unroll
-                for (int c = 0; c < kWarpsX; ++c)
-                    if (overlaps(xlo, xhi, ox + 8 * c, ox + 8 * c + 7)) cols |= 1u << c;
-#pragma unroll
-                for (int rr = 0; rr < TH / 8; ++rr)
-                    if (overlaps(ylo, yhi, oy + 8 * rr, oy + 8 * rr + 7)) m |= cols << (kWarpsX * rr);
+                m = splat_block_mask<TW, TH>(r, ox, oy);
             }
             s_mask[slot] = static_cast<unsigned char>(m);
         }

@@ -299,4 +299,60 @@ __device__ __forceinline__ unsigned pack_i16x2(int lo, int hi) {
 __device__ __forceinline__ int unpack_lo(unsigned v) { return static_cast<int>(static_cast<short>(v & 0xFFFFu)); }
 __device__ __forceinline__ int unpack_hi(unsigned v) { return static_cast<int>(static_cast<short>(v >> 16)); }
 
+// The largest base-2 exponent A2 dx^2 + B2 dx dy + C2 dy^2 (a concave form: A2, C2 < 0) over the
+// pixel-centre rectangle [X0, X1] x [Y0, Y1] of offsets from the splat centre. At the centre if the
+// rectangle holds it (0), else on an edge, where the form is a 1-D concave quadratic whose vertex
+// (dy = kx X on an edge X = const, dx = ky Y on an edge Y = const) is clamped into the edge.
+__device__ __forceinline__ float form_max(float A, float B, float C, float kx, float ky, float X0, float X1,
+                                          float Y0, float Y1) {
+    if (X0 <= 0.f && X1 >= 0.f && Y0 <= 0.f && Y1 >= 0.f) return 0.f;
+    const auto q = [&](float x, float y) { return fmaf(fmaf(A, x, B * y), x, C * y * y); };
+    const float ya = fminf(fmaxf(kx * X0, Y0), Y1), yb = fminf(fmaxf(kx * X1, Y0), Y1);
+    const float xa = fminf(fmaxf(ky * Y0, X0), X1), xb = fminf(fmaxf(ky * Y1, X0), X1);
+    return fmaxf(fmaxf(q(X0, ya), q(X1, yb)), fmaxf(q(xa, Y0), q(xb, Y1)));
+}
+
+// The 8x8 pixel blocks of a TW x TH tile at pixel (ox, oy) in which a splat can pass the alpha test,
+// bit rr * (TW / 8) + c for block (c, rr). A block is kept when it overlaps the splat's pixel bounds
+// (its 8x8-tile rectangle of the CPU renderer cut by the bounding box of the ellipse where alpha can
+// reach 1/255) AND, over the pixel centres the two share, the splat's exponent can still reach the
+// cut: L + max(form) >= log2(1/255), widened by 0.02 plus a term relative to the size of the form's
+// terms (in log2 units), which covers the rounding of this test and of the blend's own evaluation,
+// so a dropped block is one where no pixel can pass -- the image does not change, only the warp
+// steps that could not apply anything are skipped. The forward and adjoint blends use the same
+// masks, so the adjoint replays exactly the forward's walk.
+template <int TW, int TH>
+__device__ __forceinline__ unsigned splat_block_mask(const SplatRecord& r, int ox, int oy) {
+    constexpr int kWX = TW / 8, kWY = TH / 8;
+    constexpr float kCut = -7.99435343685885793f;  // log2(1/255)
+    const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
+    const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
+    const float u = r.r0.x, v = r.r0.y, A = r.r0.z, B = r.r0.w, C = r.r1.x, L = r.r1.y;
+    // A degenerate form (a coefficient that is 0 or not finite) keeps every overlapping block.
+    const bool exact = A < 0.f && C < 0.f && isfinite(A + B + C + L);
+    const float kx = exact ? __fdividef(-B, 2.f * C) : 0.f, ky = exact ? __fdividef(-B, 2.f * A) : 0.f;
+    unsigned m = 0;
+#pragma unroll
+    for (int rr = 0; rr < kWY; ++rr) {
+        const int y0 = max(ylo, oy + 8 * rr), y1 = min(yhi, oy + 8 * rr + 7);
+        if (y0 > y1) continue;
+        const float Y0 = static_cast<float>(y0) + 0.5f - v, Y1 = static_cast<float>(y1) + 0.5f - v;
+#pragma unroll
+        for (int c = 0; c < kWX; ++c) {
+            const int x0 = max(xlo, ox + 8 * c), x1 = min(xhi, ox + 8 * c + 7);
+            if (x0 > x1) continue;
+            bool keep = true;
+            if (exact) {
+                const float X0 = static_cast<float>(x0) + 0.5f - u, X1 = static_cast<float>(x1) + 0.5f - u;
+                const float best = form_max(A, B, C, kx, ky, X0, X1, Y0, Y1);
+                const float mx = fmaxf(fabsf(X0), fabsf(X1)), my = fmaxf(fabsf(Y0), fabsf(Y1));
+                const float size = fabsf(A) * mx * mx + fabsf(B) * mx * my + fabsf(C) * my * my;
+                keep = L + best + 0.02f + 1e-5f * size >= kCut;
+            }
+            if (keep) m |= 1u << (rr * kWX + c);
+        }
+    }
+    return m;
+}
+
 }  // namespace ab2
