@@ -194,13 +194,19 @@ class RasterizeBatchFunction(torch.autograd.Function):
 
 
 def rasterize_batch(scenes, cameras, view_scene, sh_degree: int = 3, splat_scale: float = 1.0,
-                    tile: tuple[int, int] = (16, 16), blend_batch: int = 256):
+                    tile: tuple[int, int] = (16, 16), blend_batch: int = 256, use_graph: bool = True,
+                    options: BatchOptions | None = None):
     """Differentiable render of many views of several scenes in one forward/backward.
 
     scenes: a list of (means, log_scales, quats, opacity_logits, sh) tuples; view k shows scene
     view_scene[k] (the views of a scene consecutive). Returns one (H, W, 3) image per view. The
     gradient of a scene is the sum over its views, added in view order (deterministic).
+    options: a launch shape (autotune.tune_train's choice) instead of sh_degree .. use_graph. With
+    use_graph, the forward's and the backward's launch sequences are recorded as CUDA graphs on
+    the first step of a shape and replayed on the next ones (the parameter, image and gradient
+    tensors may move between steps; a new shape or size records again).
     """
     flat = [t for s in scenes for t in s]
-    opts = BatchOptions(sh_degree, splat_scale, tuple(tile), blend_batch, False)
+    opts = options if options is not None else BatchOptions(sh_degree, splat_scale, tuple(tile), blend_batch,
+                                                            use_graph)
     return RasterizeBatchFunction.apply((list(cameras), [int(v) for v in view_scene], opts), *flat)

@@ -119,4 +119,71 @@ def tune(scenes, view_scene, cameras, sh_degree: int = 3, splat_scale: float = 1
                         int(best["radix_bits"]))
 
 
-__all__ = ["tune", "time_batch", "signature", "TILES", "BLEND_BATCHES", "RADIX_BITS", "CACHE_PATH"]
+def tune_train(scenes, cameras, view_scene, sh_degree: int = 3, splat_scale: float = 1.0, use_graph: bool = True,
+               cache_path: str | None = CACHE_PATH, force: bool = False, report: list | None = None,
+               iters: int = 3) -> BatchOptions:
+    """The fastest launch shape for a training step of this batch: one batched forward
+    (rasterize_batch) and its backward against fixed random upstream gradients, per candidate
+    shape, timed with CUDA events; the candidates must agree on every image and gradient bit for
+    bit (the blend order and the adjoint's sums do not depend on the shape). scenes: the
+    (means, log_scales, quats, opacity_logits, sh) tensors of each scene."""
+    import torch
+
+    from .autograd import rasterize_batch
+
+    class _N:  # the signature wants Gaussian counts
+        def __init__(self, n):
+            self.n = n
+
+    gpu = torch.cuda.get_device_name()
+    key = "train|%s|%s" % (gpu, signature([_N(s[0].shape[0]) for s in scenes], view_scene, cameras, sh_degree,
+                                          splat_scale))
+    cache = _load_cache(cache_path) if cache_path else {}
+    if not force and key in cache:
+        c = cache[key]
+        return BatchOptions(sh_degree, splat_scale, tuple(c["tile"]), int(c["blend_batch"]), use_graph,
+                            int(c.get("radix_bits", 8)))
+    gen = torch.Generator(device="cuda").manual_seed(4)
+    ups = [torch.randn((c.height, c.width, 3), device="cuda", generator=gen) for c in cameras]
+    leaves = [[t.detach().requires_grad_(True) for t in s] for s in scenes]
+
+    def step(opt):
+        for group in leaves:
+            for t in group:
+                t.grad = None
+        imgs = rasterize_batch(leaves, cameras, view_scene, options=opt)
+        torch.autograd.backward(imgs, ups)
+        return imgs
+
+    results, probe = [], None
+    for tile in TILES:
+        for bb in BLEND_BATCHES:
+            for bits in RADIX_BITS:
+                opt = BatchOptions(sh_degree, splat_scale, tile, bb, use_graph, bits)
+                imgs = step(opt)  # also records the graphs and sizes the buffers
+                got = [i.detach().clone() for i in imgs] + [t.grad.clone() for g in leaves for t in g]
+                if probe is None:
+                    probe = got
+                elif not all(torch.equal(a, b) for a, b in zip(got, probe)):
+                    raise RuntimeError("launch shapes disagree (tile %s, batch %d, %d-bit digits)" % (tile, bb, bits))
+                step(opt)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                for _ in range(iters):
+                    step(opt)
+                e1.record()
+                torch.cuda.synchronize()
+                results.append({"tile": list(tile), "blend_batch": bb, "radix_bits": bits,
+                                "ms": e0.elapsed_time(e1) / iters})
+    best = min(results, key=lambda r: r["ms"])
+    if report is not None:
+        report.extend(results)
+    if cache_path:
+        cache[key] = dict(best, candidates=results)
+        _store_cache(cache_path, cache)
+    return BatchOptions(sh_degree, splat_scale, tuple(best["tile"]), int(best["blend_batch"]), use_graph,
+                        int(best["radix_bits"]))
+
+
+__all__ = ["tune", "tune_train", "time_batch", "signature", "TILES", "BLEND_BATCHES", "RADIX_BITS", "CACHE_PATH"]

@@ -348,15 +348,40 @@ __global__ void __launch_bounds__(256) visible_list_kernel(int64_t n, unsigned e
         if (vis[k]) list[at++] = static_cast<unsigned>(i0 + k * 256);
 }
 
+// The view's camera, its scene's raw tensors and gradient buffers come from the frame's device
+// tables (copied into shared memory by each CTA), not from kernel arguments, so a recorded CUDA graph
+// of the backward stays valid when the parameters, gradients or cameras move between replays.
+template <typename T>
+__device__ __forceinline__ void copy_words(T& dst, const T& src) {
+    static_assert(sizeof(T) % 4 == 0, "copied as 32-bit words");
+    if (threadIdx.x < sizeof(T) / 4)
+        reinterpret_cast<unsigned*>(&dst)[threadIdx.x] = reinterpret_cast<const unsigned*>(&src)[threadIdx.x];
+}
+
 template <int D, bool kFresh>
-__global__ void __launch_bounds__(128) gauss_backward_kernel(RawParams raw, CamParams cam, unsigned entry_base,
+__global__ void __launch_bounds__(128) gauss_backward_kernel(const BatchScene<RawParams>* __restrict__ scenes,
+                                                             unsigned scene, const ViewInfo* __restrict__ views,
+                                                             unsigned view, const RawGrads* __restrict__ grads_table,
                                                              const Ctrl* ctrl, const unsigned* __restrict__ list,
                                                              const unsigned* __restrict__ list_count,
                                                              const unsigned* __restrict__ rank,
                                                              const unsigned* __restrict__ offs,
                                                              const unsigned long long* __restrict__ rect_sorted,
-                                                             const float* __restrict__ grad_pair, RawGrads out) {
+                                                             const float* __restrict__ grad_pair) {
     chain_entry();
+    __shared__ CamParams s_cam;
+    __shared__ RawParams s_raw;
+    __shared__ RawGrads s_out;
+    __shared__ unsigned s_entry_base;
+    copy_words(s_cam, views[view].cam);
+    copy_words(s_raw, scenes[scene].src);
+    copy_words(s_out, grads_table[scene]);
+    if (threadIdx.x == 0) s_entry_base = views[view].entry_base;
+    __syncthreads();
+    const CamParams& cam = s_cam;
+    const RawParams raw = s_raw;
+    const RawGrads out = s_out;
+    const unsigned entry_base = s_entry_base;
     const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
     const unsigned count = *list_count;
@@ -616,38 +641,37 @@ namespace {
 // The fresh and the accumulating gradient passes are separate instantiations: a run-time flag
 // inside the kernel made the accumulating one (a batch's later views) slower.
 template <bool kFresh>
-void launch_gauss_backward_t(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
-                             const unsigned* list, const unsigned* list_count, const unsigned* rank,
-                             const unsigned* offs, const unsigned long long* rect_sorted, const float* grad_pair,
-                             const RawGrads& out, dim3 grid, dim3 block, cudaStream_t stream) {
-    switch (cam.shDegree) {
-        case 0: launch_chained(gauss_backward_kernel<0, kFresh>, grid, block, stream, raw, cam, entry_base, ctrl, list,
-                               list_count, rank, offs, rect_sorted, grad_pair, out); break;
-        case 1: launch_chained(gauss_backward_kernel<1, kFresh>, grid, block, stream, raw, cam, entry_base, ctrl, list,
-                               list_count, rank, offs, rect_sorted, grad_pair, out); break;
-        case 2: launch_chained(gauss_backward_kernel<2, kFresh>, grid, block, stream, raw, cam, entry_base, ctrl, list,
-                               list_count, rank, offs, rect_sorted, grad_pair, out); break;
-        default: launch_chained(gauss_backward_kernel<3, kFresh>, grid, block, stream, raw, cam, entry_base, ctrl,
-                                list, list_count, rank, offs, rect_sorted, grad_pair, out); break;
+void launch_gauss_backward_t(const GaussBackwardArgs& a, const Ctrl* ctrl, const unsigned* list,
+                             const unsigned* list_count, const unsigned* rank, const unsigned* offs,
+                             const unsigned long long* rect_sorted, const float* grad_pair, dim3 grid, dim3 block,
+                             cudaStream_t stream) {
+    switch (a.sh_degree) {
+        case 0: launch_chained(gauss_backward_kernel<0, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
+                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
+        case 1: launch_chained(gauss_backward_kernel<1, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
+                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
+        case 2: launch_chained(gauss_backward_kernel<2, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
+                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
+        default: launch_chained(gauss_backward_kernel<3, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
+                                a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
     }
 }
 }  // namespace
 
-void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
-                           const unsigned* depth_key, const unsigned* rank, const unsigned* offs,
-                           const unsigned long long* rect_sorted, const float* grad_pair, unsigned* list,
-                           unsigned* list_count, const RawGrads& out, cudaStream_t stream) {
-    const unsigned lblocks = static_cast<unsigned>((raw.n + 256 * kListItems - 1) / (256 * kListItems));
+void launch_gauss_backward(const GaussBackwardArgs& a, const Ctrl* ctrl, const unsigned* depth_key,
+                           const unsigned* rank, const unsigned* offs, const unsigned long long* rect_sorted,
+                           const float* grad_pair, unsigned* list, unsigned* list_count, cudaStream_t stream) {
+    const unsigned lblocks = static_cast<unsigned>((a.n + 256 * kListItems - 1) / (256 * kListItems));
     if (lblocks == 0) return;
-    launch_chained(visible_list_kernel, dim3(lblocks), dim3(256), stream, raw.n, entry_base, depth_key, list,
+    launch_chained(visible_list_kernel, dim3(lblocks), dim3(256), stream, a.n, a.entry_base, depth_key, list,
                    list_count);
-    const dim3 grid(static_cast<unsigned>((raw.n + 127) / 128)), block(128);
-    if (out.fresh)
-        launch_gauss_backward_t<true>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair,
-                                      out, grid, block, stream);
+    const dim3 grid(static_cast<unsigned>((a.n + 127) / 128)), block(128);
+    if (a.fresh)
+        launch_gauss_backward_t<true>(a, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, grid, block,
+                                      stream);
     else
-        launch_gauss_backward_t<false>(raw, cam, entry_base, ctrl, list, list_count, rank, offs, rect_sorted,
-                                       grad_pair, out, grid, block, stream);
+        launch_gauss_backward_t<false>(a, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, grid, block,
+                                       stream);
 }
 
 }  // namespace ab2

@@ -111,9 +111,17 @@ struct Arena {
     unsigned ctas = 0;
     DevBuf<unsigned> pcounts;
     DevBuf<unsigned> chunk_first;
+    // Counts the (re)allocations of these buffers: a recorded graph is valid while it is unchanged.
+    // Global so that a re-initialised arena never repeats an older arena's value.
+    uint64_t gen = 0;
+    static uint64_t next_gen() {
+        static uint64_t g = 0;
+        return ++g;
+    }
 
     int init(int64_t count, unsigned cap) {
         n = count;
+        gen = next_gen();
         const size_t nn = static_cast<size_t>(std::max<int64_t>(count, 1));
         AB_TRY(rec.reserve(nn));
         AB_TRY(rect16.reserve(nn));
@@ -146,8 +154,14 @@ struct Arena {
         return init(entries, static_cast<unsigned>(std::min<uint64_t>(cap, kMaxPairs)));
     }
 
+    int reserve_ranges(size_t tiles) {
+        if (tiles > ranges.cap || !ranges.p) gen = next_gen();
+        return ranges.reserve(tiles);
+    }
+
     int grow_pairs(unsigned cap) {
         if (cap <= pair_cap && pair_key[0].p) return 0;
+        gen = next_gen();
         for (int k = 0; k < 2; ++k) {
             AB_TRY(pair_key[k].reserve(cap));
             AB_TRY(pair_val[k].reserve(cap));
@@ -326,6 +340,7 @@ int pack_camera(int scene_degree, int rendered_degree, const aniso_b200_camera* 
 struct PlanShape {
     int tile_w = kTile, tile_h = kTile, blend_batch = 128, sh_degree = 3, radix_bits = kRadixBits;
     float splat_scale = 1.0f;
+    bool use_graph = false;
 };
 
 int check_options(const aniso_b200_batch_options* o, PlanShape& shape) {
@@ -336,6 +351,7 @@ int check_options(const aniso_b200_batch_options* o, PlanShape& shape) {
     shape.tile_h = o->tile_h ? o->tile_h : kTile;
     shape.blend_batch = o->blend_batch ? o->blend_batch : 256;
     shape.radix_bits = o->radix_bits ? o->radix_bits : kRadixBits;
+    shape.use_graph = o->use_graph != 0;
     if (shape.sh_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
     if (!radix_bits_supported(shape.radix_bits)) return fail(ANISO_B200_ERR_ARGUMENT, "radix_bits must be 8 or 9");
     if (!blend_shape_supported(shape.tile_w, shape.tile_h))
@@ -350,6 +366,7 @@ struct Plan {
     std::vector<ViewInfo> views;
     std::vector<BatchScene<Src>> scenes;
     std::vector<unsigned> entry_base, tile_base, tiles_x;
+    std::vector<RawGrads> grads;  // the backward's gradient buffers, one per scene (empty otherwise)
     uint64_t entries = 0, tiles = 0;
     unsigned pre_blocks = 0;
 
@@ -408,17 +425,23 @@ struct Plan {
         for (const auto& v : views) d = std::max(d, v.cam.shDegree);
         return d;
     }
-    size_t blob_bytes() const {
-        return views.size() * sizeof(ViewInfo) + scenes.size() * sizeof(BatchScene<Src>) +
-               3 * views.size() * sizeof(unsigned);
+    // Blob layout: views, scenes, the three per-view tables, then (16-byte aligned) the gradients.
+    size_t grads_offset() const {
+        const size_t b = views.size() * sizeof(ViewInfo) + scenes.size() * sizeof(BatchScene<Src>) +
+                         3 * views.size() * sizeof(unsigned);
+        return (b + 15) / 16 * 16;
     }
+    size_t blob_bytes() const { return grads_offset() + grads.size() * sizeof(RawGrads); }
     // Same launch geometry (the only thing a recorded graph fixes besides the slot).
     bool same_geometry(const Plan& o) const {
         if (views.size() != o.views.size() || scenes.size() != o.scenes.size() || entries != o.entries ||
-            tiles != o.tiles)
+            tiles != o.tiles || grads.size() != o.grads.size())
             return false;
+        for (size_t s = 0; s < scenes.size(); ++s)
+            if (scenes[s].src.n != o.scenes[s].src.n) return false;
         for (size_t k = 0; k < views.size(); ++k)
-            if (views[k].cam.width != o.views[k].cam.width || views[k].cam.height != o.views[k].cam.height)
+            if (views[k].cam.width != o.views[k].cam.width || views[k].cam.height != o.views[k].cam.height ||
+                views[k].cam.shDegree != o.views[k].cam.shDegree)
                 return false;
         return shape.tile_w == o.shape.tile_w && shape.tile_h == o.shape.tile_h &&
                shape.blend_batch == o.shape.blend_batch && shape.radix_bits == o.shape.radix_bits &&
@@ -483,7 +506,13 @@ struct Slot {
         std::memcpy(t, P.entry_base.data(), V * sizeof(unsigned));
         std::memcpy(t + V, P.tile_base.data(), V * sizeof(unsigned));
         std::memcpy(t + 2 * V, P.tiles_x.data(), V * sizeof(unsigned));
+        if (!P.grads.empty()) std::memcpy(h + P.grads_offset(), P.grads.data(), P.grads.size() * sizeof(RawGrads));
         return 0;
+    }
+    // The device address of the blob's gradient table (after fill).
+    template <class Src>
+    const RawGrads* grads_dev(const Plan<Src>& P) const {
+        return reinterpret_cast<const RawGrads*>(dev.p + P.grads_offset());
     }
     // Stages the blob and enqueues its upload on `st` (a chained kernel reading the mapped staging
     // buffer, else a copy); returns the device views, scenes, tables.
@@ -536,7 +565,7 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     const BatchScene<Src>* scenes = nullptr;
     BatchTables tables;
     AB_TRY(slot.fill(P, st, &views, &scenes, tables));
-    AB_TRY(A.ranges.reserve(static_cast<size_t>(P.tiles)));
+    AB_TRY(A.reserve_ranges(static_cast<size_t>(P.tiles)));
     if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
     unsigned zero_words = 0;
     const PassCounts first = first_pass_counts(A, static_cast<unsigned>(P.entries), &zero_words);
@@ -1309,7 +1338,7 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     cudaStream_t st = nullptr;
     const BatchTables tables{dtab.p, dtab.p + 1, dtab.p + 2, 1u};
     const unsigned T = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
-    AB_TRY(A.ranges.reserve(T));
+    AB_TRY(A.reserve_ranges(T));
     launch_frame_begin(A.ctrl.p, nullptr, 0u, A.ranges.p, T, st);
     launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.depth_key.p, A.rect16.p, st);
     int fin = 0;
@@ -1423,7 +1452,7 @@ int aniso_b200_batch_render(aniso_b200_batch* b, const aniso_b200_camera* camera
         // pinned blob at every replay, and each replay refreshes that blob first.
         // Every allocation the sequence needs happens first: none may happen while capturing.
         AB_TRY(b->graph_slot.stage(P));
-        AB_TRY(b->arena.ranges.reserve(static_cast<size_t>(P.tiles)));
+        AB_TRY(b->arena.reserve_ranges(static_cast<size_t>(P.tiles)));
         cudaGraph_t g = nullptr;
         AB_CUDA(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
         const int rc = enqueue_plan(b->arena, b->graph_slot, P, b->capture_stream, nullptr, nullptr, false, false,
@@ -1487,9 +1516,28 @@ struct aniso_b200_trainer {
     Plan<RawParams> plan;
     int fin = 0;
     StreamChain chain;  // the streams the trainer's forwards and backwards went to
+    // CUDA graphs of a batch (batch options with use_graph): the forward's and the backward's
+    // launch sequences, each recorded once per launch geometry and replayed after restaging its
+    // slot's tables (cameras, parameter, image and gradient pointers all travel in the tables).
+    cudaStream_t capture_stream = nullptr;
+    Slot graph_slot_f, graph_slot_b;
+    cudaGraphExec_t fwd_graph = nullptr, bwd_graph = nullptr;
+    Plan<RawParams> fwd_plan, bwd_plan;
+    uint64_t fwd_gen = 0, bwd_gen = 0;     // the work buffers' generation each was recorded against
+    int fwd_fin = 0;                       // the pair buffer the recorded forward leaves sorted
+    int bwd_fin = -1;                      // the pair buffer the recorded backward reads
+    std::vector<int> bwd_fresh;            // per view: the fresh flag the backward was recorded with
+    const void* bwd_buffers[3] = {nullptr, nullptr, nullptr};
     Slot& slot() { return slots[next_slot++ % kSlots]; }
+    void drop_graphs() {
+        if (fwd_graph) cudaGraphExecDestroy(fwd_graph);
+        if (bwd_graph) cudaGraphExecDestroy(bwd_graph);
+        fwd_graph = bwd_graph = nullptr;
+    }
     ~aniso_b200_trainer() {
         chain.wait_host();
+        drop_graphs();
+        if (capture_stream) cudaStreamDestroy(capture_stream);
         if (host_ctrl) cudaFreeHost(host_ctrl);
     }
 };
@@ -1512,6 +1560,53 @@ int raw_of(const aniso_b200_raw_params& P, RawParams& raw) {
     raw.n = P.n;
     raw.sh_planes = (P.sh_degree + 1) * (P.sh_degree + 1) * 3 / 4;
     return 0;
+}
+
+// Records `enqueue` on the trainer's private stream as a CUDA graph and instantiates it in *exec.
+template <typename F>
+int record_graph(aniso_b200_trainer* t, cudaGraphExec_t* exec, F&& enqueue) {
+    if (!t->capture_stream) AB_CUDA(cudaStreamCreateWithFlags(&t->capture_stream, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    AB_CUDA(cudaStreamBeginCapture(t->capture_stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue(t->capture_stream);
+    const cudaError_t ce = cudaStreamEndCapture(t->capture_stream, &g);
+    if (rc != 0) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+        *exec = nullptr;
+        return cuda_fail(ie, "cudaGraphInstantiate");
+    }
+    return 0;
+}
+
+// The forward of a batch from its recorded graph: recorded (after every allocation it needs) when
+// the launch geometry or the work buffers changed, else replayed after restaging the graph's slot.
+int train_forward_graph(aniso_b200_trainer* t, const Plan<RawParams>& P, cudaStream_t st, int* fin) {
+    Arena& A = t->arena;
+    AB_TRY(A.reserve_ranges(static_cast<size_t>(P.tiles)));
+    AB_TRY(t->graph_slot_f.stage(P));
+    if (!t->fwd_graph || t->fwd_gen != A.gen || !P.same_geometry(t->fwd_plan)) {
+        if (t->fwd_graph) {
+            t->chain.wait_host();  // no replay of the old graph may still be in flight
+            cudaGraphExecDestroy(t->fwd_graph);
+            t->fwd_graph = nullptr;
+        }
+        int rec_fin = 0;
+        AB_TRY(record_graph(t, &t->fwd_graph, [&](cudaStream_t cs) {
+            return enqueue_plan(A, t->graph_slot_f, P, cs, nullptr, nullptr, false, true, &rec_fin, false);
+        }));
+        t->fwd_plan = P;
+        t->fwd_gen = A.gen;
+        t->fwd_fin = rec_fin;
+    }
+    *fin = t->fwd_fin;
+    AB_CUDA(cudaGraphLaunch(t->fwd_graph, st));
+    return t->graph_slot_f.mark(st);
 }
 
 int train_forward(aniso_b200_trainer* t, const aniso_b200_raw_params* params, int32_t n_scenes,
@@ -1546,7 +1641,11 @@ int train_forward(aniso_b200_trainer* t, const aniso_b200_raw_params* params, in
     t->chain.extend(st);
     for (int attempt = 0; attempt < 3; ++attempt) {
         int fin = 0;
-        AB_TRY(enqueue_plan(A, t->slot(), P, st, nullptr, nullptr, false, true, &fin));
+        if (shape.use_graph) {
+            AB_TRY(train_forward_graph(t, P, st, &fin));
+        } else {
+            AB_TRY(enqueue_plan(A, t->slot(), P, st, nullptr, nullptr, false, true, &fin));
+        }
         AB_TRY(read_ctrl(A, t->host_ctrl, st));
         int again = 0;
         AB_TRY(settle(A, *t->host_ctrl, &again, false));
@@ -1579,42 +1678,79 @@ int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const
     }
     Arena& A = t->arena;
     const Ctrl& h = *t->host_ctrl;
-    AB_TRY(t->grad_pair.reserve(std::max<uint64_t>(h.pair_total, 1) * 9));
-    const ViewInfo* views = nullptr;
-    const BatchScene<RawParams>* scenes = nullptr;
-    BackwardIn in;
-    Slot& slot = t->slot();
-    AB_TRY(t->chain.join(st));
-    t->chain.extend(st);
-    AB_TRY(slot.fill(P, st, &views, &scenes, in.tables));
-    in.ranges = A.ranges.p;
-    in.vals = A.pair_val[t->fin].p;
-    in.rec = A.rec.p;
-    in.ctrl = A.ctrl.p;
-    in.views = views;
-    in.rank = A.rank.p;
-    in.offs = A.offs.p;
-    in.rect_sorted = A.rect_sorted.p;
+    const bool graph = P.shape.use_graph;
+    // The pairs' gradient slots; sized for the pair capacity when a recorded graph replays (the
+    // graph fixes the buffer, whatever the frame's own pair count).
+    AB_TRY(t->grad_pair.reserve(std::max<uint64_t>(graph ? A.pair_cap : h.pair_total, 1) * 9));
     int64_t max_n = 1;
     for (const auto& sc : P.scenes) max_n = std::max<int64_t>(max_n, sc.src.n);
     AB_TRY(t->vis_list.reserve(static_cast<size_t>(max_n)));
     AB_TRY(t->vis_counts.reserve(P.views.size()));
-    AB_CUDA(cudaMemsetAsync(t->vis_counts.p, 0, P.views.size() * sizeof(unsigned), st));
-    launch_blend_backward(in, static_cast<unsigned>(P.tiles), P.shape.tile_w, P.shape.tile_h, t->grad_pair.p, st);
+    // The scenes' gradient buffers travel in the frame's tables; the scene's first view of a fresh
+    // gradient stores without reading the zeros (a separate kernel instantiation).
+    P.grads.assign(P.scenes.size(), RawGrads{});
+    for (size_t s = 0; s < P.scenes.size(); ++s) {
+        const aniso_b200_raw_grads& g = grads[s];
+        P.grads[s] = RawGrads{g.means, g.log_scales, g.quats, g.opacity_logits, g.sh, g.grad2d,
+                              g.grad2d ? g.visible : nullptr, g.fresh != 0 ? 1u : 0u, 0u};
+    }
+    std::vector<int> fresh(P.views.size());
     for (size_t k = 0; k < P.views.size(); ++k) {
         const unsigned s = P.views[k].scene;
-        const aniso_b200_raw_grads& g = grads[s];
-        // The scene's first view of a fresh gradient stores without reading the zeros.
-        const bool first = k == P.scenes[s].view_begin;
-        const RawGrads out{g.means, g.log_scales, g.quats, g.opacity_logits, g.sh, g.grad2d,
-                           g.grad2d ? g.visible : nullptr, g.fresh != 0 && first};
-        launch_gauss_backward(P.scenes[s].src, P.views[k].cam, P.views[k].entry_base, A.ctrl.p, A.depth_key.p,
-                              A.rank.p, A.offs.p, A.rect_sorted.p, t->grad_pair.p, t->vis_list.p, t->vis_counts.p + k,
-                              out, st);
+        fresh[k] = grads[s].fresh != 0 && k == P.scenes[s].view_begin;
     }
-    AB_TRY(slot.mark(st));
-    AB_CUDA(cudaGetLastError());
-    return ANISO_B200_OK;
+    const auto enqueue = [&](Slot& slot, cudaStream_t cs) -> int {
+        const ViewInfo* views = nullptr;
+        const BatchScene<RawParams>* scenes = nullptr;
+        BackwardIn in;
+        AB_TRY(slot.fill(P, cs, &views, &scenes, in.tables));
+        in.ranges = A.ranges.p;
+        in.vals = A.pair_val[t->fin].p;
+        in.rec = A.rec.p;
+        in.ctrl = A.ctrl.p;
+        in.views = views;
+        in.rank = A.rank.p;
+        in.offs = A.offs.p;
+        in.rect_sorted = A.rect_sorted.p;
+        AB_CUDA(cudaMemsetAsync(t->vis_counts.p, 0, P.views.size() * sizeof(unsigned), cs));
+        launch_blend_backward(in, static_cast<unsigned>(P.tiles), P.shape.tile_w, P.shape.tile_h, t->grad_pair.p, cs);
+        for (size_t k = 0; k < P.views.size(); ++k) {
+            const unsigned s = P.views[k].scene;
+            const GaussBackwardArgs ga{scenes, s, views, static_cast<unsigned>(k), slot.grads_dev(P),
+                                       P.scenes[s].src.n, P.views[k].entry_base, P.views[k].cam.shDegree,
+                                       fresh[k] != 0};
+            launch_gauss_backward(ga, A.ctrl.p, A.depth_key.p, A.rank.p, A.offs.p, A.rect_sorted.p, t->grad_pair.p,
+                                  t->vis_list.p, t->vis_counts.p + k, cs);
+        }
+        AB_CUDA(cudaGetLastError());
+        return 0;
+    };
+    AB_TRY(t->chain.join(st));
+    t->chain.extend(st);
+    if (!graph) {
+        Slot& slot = t->slot();
+        AB_TRY(enqueue(slot, st));
+        return slot.mark(st);
+    }
+    AB_TRY(t->graph_slot_b.stage(P));
+    const void* bufs[3] = {t->grad_pair.p, t->vis_list.p, t->vis_counts.p};
+    const bool valid = t->bwd_graph && t->bwd_gen == A.gen && P.same_geometry(t->bwd_plan) && t->bwd_fresh == fresh &&
+                       std::equal(bufs, bufs + 3, t->bwd_buffers) && t->bwd_fin == t->fin;
+    if (!valid) {
+        if (t->bwd_graph) {
+            t->chain.wait_host();  // no replay of the old graph may still be in flight
+            cudaGraphExecDestroy(t->bwd_graph);
+            t->bwd_graph = nullptr;
+        }
+        AB_TRY(record_graph(t, &t->bwd_graph, [&](cudaStream_t cs) { return enqueue(t->graph_slot_b, cs); }));
+        t->bwd_plan = P;
+        t->bwd_gen = A.gen;
+        t->bwd_fresh = fresh;
+        t->bwd_fin = t->fin;
+        std::copy(bufs, bufs + 3, t->bwd_buffers);
+    }
+    AB_CUDA(cudaGraphLaunch(t->bwd_graph, st));
+    return t->graph_slot_b.mark(st);
 }
 
 }  // namespace

@@ -165,17 +165,31 @@ struct RawGrads {
     float* sh;
     float* grad2d;   // optional (NULL): per Gaussian, |dL/d(screen position)| in NDC units, added over views
     float* visible;  // with grad2d: per Gaussian, the number of views it was visible in, added
-    bool fresh;      // the buffers hold zeros (the scene's first view of a fresh gradient): store, do not read
+    unsigned fresh;  // 1: the buffers hold zeros (the scene's first view of a fresh gradient): store, do not read
+    unsigned pad;
 };
 // grad_pair: 9 floats per pair, at the pair's depth-ordered slot.
 void launch_blend_backward(const BackwardIn& in, unsigned tiles, int tile_w, int tile_h, float* grad_pair,
                            cudaStream_t stream);
-// One view: its scene's Gaussians visible in it add their gradients to `out` (with out.fresh,
-// whose entries are zero, without reading them). list (the scene's n words) and *list_count (zero
-// on entry) are work space for the compacted visible list.
-void launch_gauss_backward(const RawParams& raw, const CamParams& cam, unsigned entry_base, const Ctrl* ctrl,
-                           const unsigned* depth_key, const unsigned* rank, const unsigned* offs,
-                           const unsigned long long* rect_sorted, const float* grad_pair, unsigned* list,
-                           unsigned* list_count, const RawGrads& out, cudaStream_t stream);
+// One view of one scene, everything the kernel reads about them in the frame's device tables: the
+// scene's raw tensors (scenes[scene].src), the view's camera and entry base (views[view]), the
+// scene's gradient buffers (grads[scene]). n, entry_base and sh_degree (the view's rendered degree)
+// size and choose the launch; fresh: the scene's first view of a fresh gradient (store, do not read).
+struct GaussBackwardArgs {
+    const BatchScene<RawParams>* scenes;
+    unsigned scene;
+    const ViewInfo* views;
+    unsigned view;
+    const RawGrads* grads;
+    int64_t n;
+    unsigned entry_base;
+    int sh_degree;
+    bool fresh;
+};
+// The view's visible Gaussians add their gradients to the scene's buffers. list (the scene's n
+// words) and *list_count (zero on entry) are work space for the compacted visible list.
+void launch_gauss_backward(const GaussBackwardArgs& args, const Ctrl* ctrl, const unsigned* depth_key,
+                           const unsigned* rank, const unsigned* offs, const unsigned long long* rect_sorted,
+                           const float* grad_pair, unsigned* list, unsigned* list_count, cudaStream_t stream);
 
 }  // namespace ab2

@@ -471,9 +471,14 @@ def train_batch_leg(torch, steps: int):
             for p in group:
                 p.grad = None
 
+    from aniso_b200.autotune import tune_train
+
+    candidates = []
+    best = tune_train(ps, cams, view_scene, cache_path=None, report=candidates, iters=2)
+
     def batched():
         zero()
-        imgs = rasterize_batch(ps, cams, view_scene)
+        imgs = rasterize_batch(ps, cams, view_scene, options=best)
         torch.autograd.backward(imgs, ups)
 
     def per_view():
@@ -502,6 +507,10 @@ def train_batch_leg(torch, steps: int):
             "ms_per_view_batched": out["batched"] / V, "ms_per_view_per_view": out["per_view"] / V,
             "speedup": out["per_view"] / out["batched"], "views": V,
             "gaussians": sum(rw.n for rw in raws),
+            "tuned": {"tile": "%dx%d" % best.tile, "blend_batch": best.blend_batch, "radix_bits": best.radix_bits,
+                      "cuda_graph": bool(best.use_graph)},
+            "candidates_ms_per_step": {"%dx%d/%d/%db" % (c["tile"][0], c["tile"][1], c["blend_batch"],
+                                                         c["radix_bits"]): round(c["ms"], 3) for c in candidates},
             "grads_equal_per_view_sum": same,
             "note": "batched gradients equal the per-view gradients summed in view order bit for bit; "
                     "the per-view adjoint is checked against FP64 in tests/test_gradients.py"}
