@@ -124,9 +124,10 @@ def tune_train(scenes, cameras, view_scene, sh_degree: int = 3, splat_scale: flo
                iters: int = 3) -> BatchOptions:
     """The fastest launch shape for a training step of this batch: one batched forward
     (rasterize_batch) and its backward against fixed random upstream gradients, per candidate
-    shape, timed with CUDA events; the candidates must agree on every image and gradient bit for
-    bit (the blend order and the adjoint's sums do not depend on the shape). scenes: the
-    (means, log_scales, quats, opacity_logits, sh) tensors of each scene."""
+    shape, timed with CUDA events; the candidates must agree on every image bit for bit and on the
+    gradients to rounding (each Gaussian sums one slot per tile it touches, so the tile grid groups
+    the same terms differently). scenes: the (means, log_scales, quats, opacity_logits, sh) tensors
+    of each scene."""
     import torch
 
     from .autograd import rasterize_batch
@@ -161,11 +162,18 @@ def tune_train(scenes, cameras, view_scene, sh_degree: int = 3, splat_scale: flo
             for bits in RADIX_BITS:
                 opt = BatchOptions(sh_degree, splat_scale, tile, bb, use_graph, bits)
                 imgs = step(opt)  # also records the graphs and sizes the buffers
-                got = [i.detach().clone() for i in imgs] + [t.grad.clone() for g in leaves for t in g]
+                got = ([i.detach().clone() for i in imgs], [t.grad.clone() for g in leaves for t in g])
                 if probe is None:
                     probe = got
-                elif not all(torch.equal(a, b) for a, b in zip(got, probe)):
-                    raise RuntimeError("launch shapes disagree (tile %s, batch %d, %d-bit digits)" % (tile, bb, bits))
+                else:
+                    # Images agree bit for bit; the gradients are the same sums grouped by another
+                    # tile grid, so they agree to rounding.
+                    same = all(torch.equal(a, b) for a, b in zip(got[0], probe[0])) and all(
+                        torch.allclose(a, b, rtol=1e-4, atol=1e-5 * float(b.abs().max()) + 1e-30)
+                        for a, b in zip(got[1], probe[1]))
+                    if not same:
+                        raise RuntimeError("launch shapes disagree (tile %s, batch %d, %d-bit digits)"
+                                           % (tile, bb, bits))
                 step(opt)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 torch.cuda.synchronize()

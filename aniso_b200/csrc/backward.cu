@@ -30,8 +30,6 @@ constexpr float kLn2 = 0.69314718055994530942f;
 constexpr float kHalfLog2e = -0.72134752044448170368f;  // A2 = kHalfLog2e * A, C2 likewise
 constexpr float kNegLog2e = -1.44269504088896340736f;   // B2 = kNegLog2e * B
 
-__device__ __forceinline__ bool overlaps(int lo, int hi, int a, int b) { return lo <= b && hi >= a; }
-
 // Sums v[0..8] over the warp; afterwards the even lanes hold one sum each: value index *k (-1 for
 // none). 12 shuffles: each step hands half of the values to the partner lane.
 __device__ __forceinline__ float warp_reduce9(const float v[kG], int lane, int& k) {
@@ -364,6 +362,7 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(const BatchScene<Ra
                                                              unsigned view, const RawGrads* __restrict__ grads_table,
                                                              const Ctrl* ctrl, const unsigned* __restrict__ list,
                                                              const unsigned* __restrict__ list_count,
+                                                             const unsigned* __restrict__ sorted,
                                                              const unsigned* __restrict__ rank,
                                                              const unsigned* __restrict__ offs,
                                                              const unsigned long long* __restrict__ rect_sorted,
@@ -384,16 +383,19 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(const BatchScene<Ra
     const unsigned entry_base = s_entry_base;
     const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
-    const unsigned count = *list_count;
+    // A frame of one view walks its depth-sorted visible list itself: thread t takes the t-th
+    // nearest entry, so the reads of the rectangles, the pair offsets and -- the largest stream --
+    // the pair slots are contiguous across the warp. Otherwise the view's compacted list.
+    const unsigned count = sorted ? ctrl->vis_count : *list_count;
     if (blockIdx.x * blockDim.x >= count) return;
     const int lane = threadIdx.x & 31;
     // Past the end of the list: no Gaussian, but the lane still helps its warp.
     const bool active = t < count;
-    const int64_t i = active ? list[t] : 0;
-    const unsigned e = entry_base + static_cast<unsigned>(i);
+    const unsigned e = active ? (sorted ? sorted[t] : entry_base + list[t]) : entry_base;
+    const int64_t i = e - entry_base;
     unsigned cnt = 0, off = 0;
     if (active) {
-        const unsigned j = rank[e];
+        const unsigned j = sorted ? t : rank[e];
         const unsigned long long rc = rect_sorted[j];
         cnt = ((rc >> 32 & 0xFFFFu) - (rc & 0xFFFFu) + 1) * ((rc >> 48) - (rc >> 16 & 0xFFFFu) + 1);
         off = offs[j];
@@ -647,13 +649,13 @@ void launch_gauss_backward_t(const GaussBackwardArgs& a, const Ctrl* ctrl, const
                              cudaStream_t stream) {
     switch (a.sh_degree) {
         case 0: launch_chained(gauss_backward_kernel<0, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
-                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
+                               a.view, a.grads, ctrl, list, list_count, a.sorted, rank, offs, rect_sorted, grad_pair); break;
         case 1: launch_chained(gauss_backward_kernel<1, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
-                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
+                               a.view, a.grads, ctrl, list, list_count, a.sorted, rank, offs, rect_sorted, grad_pair); break;
         case 2: launch_chained(gauss_backward_kernel<2, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
-                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
+                               a.view, a.grads, ctrl, list, list_count, a.sorted, rank, offs, rect_sorted, grad_pair); break;
         default: launch_chained(gauss_backward_kernel<3, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
-                                a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
+                                a.view, a.grads, ctrl, list, list_count, a.sorted, rank, offs, rect_sorted, grad_pair); break;
     }
 }
 }  // namespace
@@ -663,8 +665,9 @@ void launch_gauss_backward(const GaussBackwardArgs& a, const Ctrl* ctrl, const u
                            const float* grad_pair, unsigned* list, unsigned* list_count, cudaStream_t stream) {
     const unsigned lblocks = static_cast<unsigned>((a.n + 256 * kListItems - 1) / (256 * kListItems));
     if (lblocks == 0) return;
-    launch_chained(visible_list_kernel, dim3(lblocks), dim3(256), stream, a.n, a.entry_base, depth_key, list,
-                   list_count);
+    if (!a.sorted)  // a frame of one view walks the depth-sorted list instead: no compaction
+        launch_chained(visible_list_kernel, dim3(lblocks), dim3(256), stream, a.n, a.entry_base, depth_key, list,
+                       list_count);
     const dim3 grid(static_cast<unsigned>((a.n + 127) / 128)), block(128);
     if (a.fresh)
         launch_gauss_backward_t<true>(a, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, grid, block,

@@ -27,8 +27,6 @@
 namespace ab2 {
 namespace {
 
-__device__ __forceinline__ bool overlaps(int lo, int hi, int a, int b) { return lo <= b && hi >= a; }
-
 // One pixel's step for one splat. p is the base-2 exponent including log2(opacity) L, so
 // alpha = min(0.99, 2^p) and the reference's "power > 0" skip is p > L. The new transmittance is
 // T - alpha T (one instruction fewer than T (1 - alpha); it differs only in rounding).

@@ -668,7 +668,8 @@ struct StreamChain {
         }
         if (cudaEventRecord(ev, last) == cudaSuccess) cudaEventSynchronize(ev);
         cudaGetLastError();
-        any = false;
+        // The chain stays as it is: work enqueued after this wait still goes to `last`, and the
+        // next join must order behind it.
     }
 };
 
@@ -1716,9 +1717,11 @@ int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const
         launch_blend_backward(in, static_cast<unsigned>(P.tiles), P.shape.tile_w, P.shape.tile_h, t->grad_pair.p, cs);
         for (size_t k = 0; k < P.views.size(); ++k) {
             const unsigned s = P.views[k].scene;
+            // One view: every visible entry is this view's, so the sort's depth-ordered list serves
+            // as the work list (coalesced pair-slot reads, no compaction launch).
             const GaussBackwardArgs ga{scenes, s, views, static_cast<unsigned>(k), slot.grads_dev(P),
                                        P.scenes[s].src.n, P.views[k].entry_base, P.views[k].cam.shDegree,
-                                       fresh[k] != 0};
+                                       fresh[k] != 0, P.views.size() == 1 ? A.vis_idx[1].p : nullptr};
             launch_gauss_backward(ga, A.ctrl.p, A.depth_key.p, A.rank.p, A.offs.p, A.rect_sorted.p, t->grad_pair.p,
                                   t->vis_list.p, t->vis_counts.p + k, cs);
         }

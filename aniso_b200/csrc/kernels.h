@@ -185,6 +185,9 @@ struct GaussBackwardArgs {
     unsigned entry_base;
     int sh_degree;
     bool fresh;
+    // A frame of one view: its depth-sorted visible entries (the sort's output), walked in that
+    // order instead of a compacted list; NULL otherwise.
+    const unsigned* sorted;
 };
 // The view's visible Gaussians add their gradients to the scene's buffers. list (the scene's n
 // words) and *list_count (zero on entry) are work space for the compacted visible list.

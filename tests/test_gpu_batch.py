@@ -134,16 +134,21 @@ def test_many_tiles_with_nine_bit_digits(ab, torch, tile):
 
 
 def test_frame_kernel_count(ab):
-    """A small frame: the tables' upload, frame_begin, preprocess (which also counts the first
-    depth pass's digits), the first depth pass (span scan + downsweep), three more of upsweep +
+    """A small frame with the persistent sort (the default): the tables' upload, frame_begin,
+    preprocess (which also counts the first depth pass's digits), the sort (one cooperative launch:
+    depth passes, pair expansion, tile passes, ranges), blend. With ANISO_B200_SORT=multi, the
+    multi-kernel sort instead: the first depth pass (span scan + downsweep), three more of upsweep +
     span scan + downsweep, pair count / offsets / expansion (which counts the first tile pass's
-    digits), the first tile pass (2 kernels), any second one (3), ranges, blend."""
+    digits), the first tile pass (2 kernels), any second one (3), ranges."""
+    import os
+
+    multi = os.environ.get("ANISO_B200_SORT") == "multi"
     g, sh, d = kat.random_cloud(5000, seed=3)
     r = ab.GpuRenderer(g, sh, d)
     r.render(kat.gpu_test_camera(320, 240))  # 300 tiles: 2 tile passes
-    assert r.frame_kernels() == 1 + 1 + 1 + 2 + 3 * 3 + 3 + 2 + 3 + 1 + 1
+    assert r.frame_kernels() == (1 + 1 + 1 + 2 + 3 * 3 + 3 + 2 + 3 + 1 + 1 if multi else 5)
     r.render(kat.gpu_test_camera(64, 48))  # 12 tiles: 1 tile pass
-    assert r.frame_kernels() == 1 + 1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 + 1
+    assert r.frame_kernels() == (1 + 1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 + 1 if multi else 5)
 
 
 def test_large_batch_counts_digits_in_separate_passes(ab, torch):
