@@ -13,6 +13,13 @@
 // after which the frame is marked void (kFlagWaitTimeout | kFlagOverflow: nothing downstream uses
 // it) and every CTA returns -- no wait can hang the device.
 //
+// Measured, it is the slower sort, so it is opt-in (ANISO_B200_SORT=persistent): 0.169 against
+// 0.125 ms per 740k 1280x720 frame. ncu: one 1024-thread CTA per SM (64 registers), half the warp
+// slots active, 35% issue-active, and the top stall is the block barrier: each scatter round is a
+// chain of about nine __syncthreads around a few instructions of work per thread, and a phase
+// cannot end before its slowest CTA, where the multi-kernel sequence overlaps one kernel's tail
+// with the next one's launch.
+//
 // Phases (one CTA = one contiguous chunk of each pass's items: blocks [T c / G, T (c + 1) / G) of
 // kSortBlockItems, the chunking the producers' digit counts use):
 //   depth pass 0 (8-bit, compacting): counts from the preprocess (or a counting phase), then
@@ -23,7 +30,7 @@
 //     | barrier
 //   tile passes: (count | barrier |) scan + scatter | barrier;  tile ranges.
 // "scan" is each CTA reading every CTA's digit counts (a G x R matrix, CTA-major so the reads
-// coalesce) and forming its own per-digit output positions; "scatter" ranks 8192 items per round
+// coalesce) and forming its own per-digit output positions; "scatter" ranks 4096 items per round
 // (warp-level peer masks, cross-warp prefix per digit) and writes them through shared memory so
 // global writes are contiguous per digit. Data another CTA wrote in an earlier phase is read with
 // ld.global.cg (L2), never through the non-coherent path.
@@ -212,7 +219,7 @@ __device__ unsigned scan_phase(const unsigned* counts, ScanSmem& s, KeepSmem& k)
     return all;
 }
 
-// Ranks and scatters this CTA's chunk, 8192 items per round, stably: within a round items keep
+// Ranks and scatters this CTA's chunk, 4096 items per round, stably: within a round items keep
 // their position order per digit (warp peer masks in (item, lane) order, warps in order), rounds
 // in order, CTAs in order through k.run. masked: the input is the depth keys in entry order, culled
 // ones dropped, the entry index as the value.
@@ -595,12 +602,12 @@ __global__ void __launch_bounds__(kT, 1) sort_frame_kernel(SortFrameArgs a) {
     ranges_phase(a.pair_key[a.tile_passes & 1], P, a.ranges);
 }
 
-bool sort_env_multi() {
-    static const bool multi = [] {
+bool sort_env_persistent() {
+    static const bool persistent = [] {
         const char* v = std::getenv("ANISO_B200_SORT");
-        return v && std::strcmp(v, "multi") == 0;
+        return v && std::strcmp(v, "persistent") == 0;
     }();
-    return multi;
+    return persistent;
 }
 
 constexpr int kMaxDevices = 64;
@@ -609,7 +616,7 @@ int g_ctas[kMaxDevices];  // 0: not yet probed; -1: not supported; else the CTA 
 }  // namespace
 
 unsigned persistent_sort_ctas() {
-    if (sort_env_multi()) return 0;
+    if (!sort_env_persistent()) return 0;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();

@@ -134,15 +134,15 @@ def test_many_tiles_with_nine_bit_digits(ab, torch, tile):
 
 
 def test_frame_kernel_count(ab):
-    """A small frame with the persistent sort (the default): the tables' upload, frame_begin,
-    preprocess (which also counts the first depth pass's digits), the sort (one cooperative launch:
-    depth passes, pair expansion, tile passes, ranges), blend. With ANISO_B200_SORT=multi, the
-    multi-kernel sort instead: the first depth pass (span scan + downsweep), three more of upsweep +
-    span scan + downsweep, pair count / offsets / expansion (which counts the first tile pass's
-    digits), the first tile pass (2 kernels), any second one (3), ranges."""
+    """A small frame: the tables' upload, frame_begin, preprocess (which also counts the first
+    depth pass's digits), the multi-kernel sort (the default): the first depth pass (span scan +
+    downsweep), three more of upsweep + span scan + downsweep, pair count / offsets / expansion
+    (which counts the first tile pass's digits), the first tile pass (2 kernels), any second one
+    (3), ranges; blend. With ANISO_B200_SORT=persistent the sort is one cooperative launch
+    instead (depth passes, pair expansion, tile passes, ranges)."""
     import os
 
-    multi = os.environ.get("ANISO_B200_SORT") == "multi"
+    multi = os.environ.get("ANISO_B200_SORT") != "persistent"
     g, sh, d = kat.random_cloud(5000, seed=3)
     r = ab.GpuRenderer(g, sh, d)
     r.render(kat.gpu_test_camera(320, 240))  # 300 tiles: 2 tile passes

@@ -1,6 +1,6 @@
-"""The persistent sort (one cooperative launch with bounded grid barriers, the default where the
-device supports it) and the multi-kernel sort (ANISO_B200_SORT=multi, read once per process, hence
-child processes) give the same bytes: sorted pair lists and tile ranges of single views, images of
+"""The persistent sort (one cooperative launch with bounded grid barriers, selected by
+ANISO_B200_SORT=persistent, read once per process, hence child processes) and the multi-kernel
+sort (the default) give the same bytes: sorted pair lists and tile ranges of single views, images of
 batches of mixed resolutions and tile shapes (8- and 9-bit tile digits), gradients of the
 differentiable path (needs a GPU)."""
 import os
@@ -64,8 +64,8 @@ def run_child(tmp_path, mode):
     path = str(tmp_path / ("%s.npz" % mode))
     code = "ROOT = %r\nOUT = %r\n" % (ROOT, path) + CHILD
     env = dict(os.environ)
-    if mode == "multi":
-        env["ANISO_B200_SORT"] = "multi"
+    if mode == "persistent":
+        env["ANISO_B200_SORT"] = "persistent"
     else:
         env.pop("ANISO_B200_SORT", None)
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
@@ -74,8 +74,8 @@ def run_child(tmp_path, mode):
 
 
 def test_persistent_sort_equals_multi_kernel_sort(tmp_path):
-    a = run_child(tmp_path, "default")
-    b = run_child(tmp_path, "multi")
+    a = run_child(tmp_path, "persistent")
+    b = run_child(tmp_path, "default")
     assert set(a) == set(b)
     for key in sorted(a):
         np.testing.assert_array_equal(a[key], b[key], err_msg=key)
