@@ -362,7 +362,6 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(const BatchScene<Ra
                                                              unsigned view, const RawGrads* __restrict__ grads_table,
                                                              const Ctrl* ctrl, const unsigned* __restrict__ list,
                                                              const unsigned* __restrict__ list_count,
-                                                             const unsigned* __restrict__ sorted,
                                                              const unsigned* __restrict__ rank,
                                                              const unsigned* __restrict__ offs,
                                                              const unsigned long long* __restrict__ rect_sorted,
@@ -383,19 +382,20 @@ __global__ void __launch_bounds__(128) gauss_backward_kernel(const BatchScene<Ra
     const unsigned entry_base = s_entry_base;
     const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
-    // A frame of one view walks its depth-sorted visible list itself: thread t takes the t-th
-    // nearest entry, so the reads of the rectangles, the pair offsets and -- the largest stream --
-    // the pair slots are contiguous across the warp. Otherwise the view's compacted list.
-    const unsigned count = sorted ? ctrl->vis_count : *list_count;
+    // The view's visible entries in entry order (the compacted list), so that a warp's reads of the
+    // raw parameters and its gradient writes fall on neighbouring rows. (Walking the depth-sorted
+    // list instead makes the pair-slot reads contiguous but every parameter row a random gather:
+    // measured 0.22 -> 0.30 ms at 2.2M Gaussians.)
+    const unsigned count = *list_count;
     if (blockIdx.x * blockDim.x >= count) return;
     const int lane = threadIdx.x & 31;
     // Past the end of the list: no Gaussian, but the lane still helps its warp.
     const bool active = t < count;
-    const unsigned e = active ? (sorted ? sorted[t] : entry_base + list[t]) : entry_base;
+    const unsigned e = active ? entry_base + list[t] : entry_base;
     const int64_t i = e - entry_base;
     unsigned cnt = 0, off = 0;
     if (active) {
-        const unsigned j = sorted ? t : rank[e];
+        const unsigned j = rank[e];
         const unsigned long long rc = rect_sorted[j];
         cnt = ((rc >> 32 & 0xFFFFu) - (rc & 0xFFFFu) + 1) * ((rc >> 48) - (rc >> 16 & 0xFFFFu) + 1);
         off = offs[j];
@@ -649,13 +649,13 @@ void launch_gauss_backward_t(const GaussBackwardArgs& a, const Ctrl* ctrl, const
                              cudaStream_t stream) {
     switch (a.sh_degree) {
         case 0: launch_chained(gauss_backward_kernel<0, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
-                               a.view, a.grads, ctrl, list, list_count, a.sorted, rank, offs, rect_sorted, grad_pair); break;
+                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
         case 1: launch_chained(gauss_backward_kernel<1, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
-                               a.view, a.grads, ctrl, list, list_count, a.sorted, rank, offs, rect_sorted, grad_pair); break;
+                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
         case 2: launch_chained(gauss_backward_kernel<2, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
-                               a.view, a.grads, ctrl, list, list_count, a.sorted, rank, offs, rect_sorted, grad_pair); break;
+                               a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
         default: launch_chained(gauss_backward_kernel<3, kFresh>, grid, block, stream, a.scenes, a.scene, a.views,
-                                a.view, a.grads, ctrl, list, list_count, a.sorted, rank, offs, rect_sorted, grad_pair); break;
+                                a.view, a.grads, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair); break;
     }
 }
 }  // namespace
@@ -665,9 +665,8 @@ void launch_gauss_backward(const GaussBackwardArgs& a, const Ctrl* ctrl, const u
                            const float* grad_pair, unsigned* list, unsigned* list_count, cudaStream_t stream) {
     const unsigned lblocks = static_cast<unsigned>((a.n + 256 * kListItems - 1) / (256 * kListItems));
     if (lblocks == 0) return;
-    if (!a.sorted)  // a frame of one view walks the depth-sorted list instead: no compaction
-        launch_chained(visible_list_kernel, dim3(lblocks), dim3(256), stream, a.n, a.entry_base, depth_key, list,
-                       list_count);
+    launch_chained(visible_list_kernel, dim3(lblocks), dim3(256), stream, a.n, a.entry_base, depth_key, list,
+                   list_count);
     const dim3 grid(static_cast<unsigned>((a.n + 127) / 128)), block(128);
     if (a.fresh)
         launch_gauss_backward_t<true>(a, ctrl, list, list_count, rank, offs, rect_sorted, grad_pair, grid, block,

@@ -111,6 +111,12 @@ struct Arena {
     unsigned ctas = 0;
     DevBuf<unsigned> pcounts;
     DevBuf<unsigned> chunk_first;
+    // The one-pass tile binning (frames of at most bin_max_tiles() tiles): the (block, tile) count
+    // matrix, sized for the pair capacity and the widest such frame seen (bin_tiles), and the
+    // tiles' starts.
+    unsigned bin_tiles = 0;
+    DevBuf<unsigned> bin_counts;
+    DevBuf<unsigned> tile_start;
     // Counts the (re)allocations of these buffers: a recorded graph is valid while it is unchanged.
     // Global so that a re-initialised arena never repeats an older arena's value.
     uint64_t gen = 0;
@@ -154,9 +160,29 @@ struct Arena {
         return init(entries, static_cast<unsigned>(std::min<uint64_t>(cap, kMaxPairs)));
     }
 
+    // Tile ranges for `tiles` tiles, and the tile binning's buffers when it takes such frames.
     int reserve_ranges(size_t tiles) {
         if (tiles > ranges.cap || !ranges.p) gen = next_gen();
-        return ranges.reserve(tiles);
+        AB_TRY(ranges.reserve(tiles));
+        if (tiles > bin_tiles && tiles <= bin_max_tiles()) {
+            bin_tiles = static_cast<unsigned>(tiles);
+            return reserve_bins();
+        }
+        return 0;
+    }
+
+    int reserve_bins() {
+        if (!bin_tiles || pair_cap > bin_max_pairs()) return 0;
+        const size_t words = bin_count_words(pair_cap, bin_tiles);
+        if (words > bin_counts.cap || !bin_counts.p || !tile_start.p) gen = next_gen();
+        AB_TRY(bin_counts.reserve(words));
+        return tile_start.reserve(bin_max_tiles());
+    }
+
+    // The tile binning can sort a frame of `tiles` tiles at the current pair capacity.
+    bool bins_for(unsigned tiles) const {
+        return tiles > 0 && tiles <= bin_tiles && pair_cap <= bin_max_pairs() && tile_start.p &&
+               bin_counts.cap >= bin_count_words(pair_cap, tiles);
     }
 
     int grow_pairs(unsigned cap) {
@@ -167,6 +193,7 @@ struct Arena {
             AB_TRY(pair_val[k].reserve(cap));
         }
         pair_cap = cap;
+        AB_TRY(reserve_bins());
         return chunk_start.reserve(chunks_of(cap, expand_chunk_pairs()) + 2);
     }
 };
@@ -249,7 +276,9 @@ int enqueue_sort_persistent(Arena& A, unsigned entries, unsigned tiles, const Ba
 // that count matrix first; every other pass has its own upsweep. (Counting in the downsweeps too
 // was measured slower: keys written next to each other often share the next digit, the high depth
 // digits taking few values, so one atomic per key contends -- 0.177 ms against 0.139 ms for the
-// sort of the 740k / 1280x720 frame.) Where the persistent sort can run (A.ctas), it replaces this
+// sort of the 740k / 1280x720 frame.) A frame of at most bin_max_tiles() tiles (A.bins_for) takes
+// the one-pass tile binning after the expansion instead of the tile passes and the ranges. Where
+// the persistent sort is selected (A.ctas), it replaces this
 // whole sequence with one launch and the same outputs.
 int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank, int bits,
                  bool first_counted, cudaStream_t st, int* final_buf) {
@@ -260,7 +289,8 @@ int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& 
     unsigned* totals = A.sort_scratch.p + 2 * sort_count_words();
     int tile_bits[4];
     const int tile_passes = tile_pass_widths(tiles, bits, tile_bits);
-    const bool expand_counts = A.pair_cap <= kProducerCountMax;
+    const bool bins = A.bins_for(tiles);
+    const bool expand_counts = !bins && A.pair_cap <= kProducerCountMax;
     const unsigned tile_spans = sort_spans(A.pair_cap);
     const PassCounts first_tile =
         expand_counts
@@ -283,6 +313,14 @@ int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& 
     }
     const int sorted = (kDepthPasses - 1) & 1;
     const DupBuffers dup{A.offs.p, keep_rank ? A.rank.p : nullptr, A.rect_sorted.p, A.chunk_start.p, A.span_sum.p};
+    if (bins) {  // one stable counting pass over the tile id (and the ranges) instead of the tile passes
+        launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, dup, A.pair_key[0].p,
+                         A.pair_val[0].p, st, PassCounts{}, A.bin_counts.p, tiles);
+        launch_tile_bins(A.pair_key[0].p, A.pair_val[0].p, A.pair_key[1].p, A.pair_val[1].p, A.bin_counts.p, tiles,
+                         A.tile_start.p, A.ranges.p, ctrl, A.pair_cap, st);
+        *final_buf = 1;
+        return 0;
+    }
     launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, dup, A.pair_key[0].p,
                      A.pair_val[0].p, st, first_tile);
     for (int t = 0, shift = 0; t < tile_passes; shift += tile_bits[t], ++t) {
@@ -1717,11 +1755,9 @@ int train_backward(aniso_b200_trainer* t, const float* const* grad_images, const
         launch_blend_backward(in, static_cast<unsigned>(P.tiles), P.shape.tile_w, P.shape.tile_h, t->grad_pair.p, cs);
         for (size_t k = 0; k < P.views.size(); ++k) {
             const unsigned s = P.views[k].scene;
-            // One view: every visible entry is this view's, so the sort's depth-ordered list serves
-            // as the work list (coalesced pair-slot reads, no compaction launch).
             const GaussBackwardArgs ga{scenes, s, views, static_cast<unsigned>(k), slot.grads_dev(P),
                                        P.scenes[s].src.n, P.views[k].entry_base, P.views[k].cam.shDegree,
-                                       fresh[k] != 0, P.views.size() == 1 ? A.vis_idx[1].p : nullptr};
+                                       fresh[k] != 0};
             launch_gauss_backward(ga, A.ctrl.p, A.depth_key.p, A.rank.p, A.offs.p, A.rect_sorted.p, t->grad_pair.p,
                                   t->vis_list.p, t->vis_counts.p + k, cs);
         }

@@ -128,7 +128,8 @@ struct Ctrl {
     unsigned int vis_count;             // visible entries
     unsigned int flags;                 // kFlag* bits, read back by the host after the frame
     unsigned int sticky_flags;          // OR of the flags of earlier frames since the host last read it
-    unsigned int sort_barrier;          // arrivals at the persistent sort's grid barriers (cleared per frame)
+    unsigned int sort_barrier;          // arrivals at the persistent sort's grid barriers, or CTAs done
+                                        // with the tile-bin scan (cleared per frame)
     unsigned long long max_pair_total;  // largest pair_total of earlier frames since then
 };
 
@@ -197,21 +198,28 @@ bool chain_enabled();
 uint64_t chained_launches();
 void note_chained_launch();
 
-// kernel<<<grid, block, 0, stream>>>(args...) with programmatic stream serialisation.
+// kernel<<<grid, block, smem, stream>>>(args...) with programmatic stream serialisation.
 template <typename... P, typename... A>
-inline void launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, cudaStream_t stream, A&&... args) {
+inline void launch_chained_smem(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                                A&&... args) {
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = chain_enabled() ? 1 : 0;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     note_chained_launch();
     cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...);
+}
+
+// kernel<<<grid, block, 0, stream>>>(args...) with programmatic stream serialisation.
+template <typename... P, typename... A>
+inline void launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, cudaStream_t stream, A&&... args) {
+    launch_chained_smem(kernel, grid, block, 0, stream, static_cast<A&&>(args)...);
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {

@@ -90,9 +90,25 @@ struct DupBuffers {
 };
 size_t sort_span_sums();
 unsigned expand_chunk_pairs();
+// bin_counts (with bin_tiles = the frame's global tiles): the expansion also writes each block's
+// per-tile pair counts there, for the one-pass tile binning (launch_tile_bins).
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
                       unsigned max_visible, const BatchTables& tables, const DupBuffers& buf, unsigned* pair_key,
-                      unsigned* pair_val, cudaStream_t stream, const PassCounts& first = PassCounts{});
+                      unsigned* pair_val, cudaStream_t stream, const PassCounts& first = PassCounts{},
+                      unsigned* bin_counts = nullptr, unsigned bin_tiles = 0);
+
+// The tile order in one stable counting pass over the tile id, for frames of at most
+// bin_max_tiles() global tiles and at most bin_max_pairs() pair capacity: keys_in / vals_in are
+// the expansion's depth-ordered pairs, counts its (block, tile) matrix (bin_count_words words;
+// made into offsets in place); writes the tile-ordered pairs, the tiles' starts (tile_start, one
+// word per tile) and every tile's range. Two kernels; same outputs as the LSD tile passes and
+// launch_ranges.
+unsigned bin_max_tiles();
+unsigned bin_max_pairs();
+size_t bin_count_words(unsigned capacity, unsigned tiles);
+void launch_tile_bins(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
+                      unsigned* counts, unsigned tiles, unsigned* tile_start, uint2* ranges, Ctrl* ctrl,
+                      unsigned capacity, cudaStream_t stream);
 
 // ranges[tile] = [start, end) over the sorted tile keys (gpu_render.cu:164-177); ranges must be
 // zeroed before.
@@ -186,9 +202,6 @@ struct GaussBackwardArgs {
     unsigned entry_base;
     int sh_degree;
     bool fresh;
-    // A frame of one view: its depth-sorted visible entries (the sort's output), walked in that
-    // order instead of a compacted list; NULL otherwise.
-    const unsigned* sorted;
 };
 // The view's visible Gaussians add their gradients to the scene's buffers. list (the scene's n
 // words) and *list_count (zero on entry) are work space for the compacted visible list.

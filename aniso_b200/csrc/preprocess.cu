@@ -20,16 +20,12 @@ constexpr float kShC3_0 = -0.5900435899266435f, kShC3_1 = 2.890611442640554f, kS
                 kShC3_3 = 0.3731763325901154f, kShC3_4 = -0.4570457994644658f, kShC3_5 = 1.445305721320277f,
                 kShC3_6 = -0.5900435899266435f;
 
-// MUFU approximations (relative error ~2^-22) for quantities that carry their own margins or only
-// feed the colour, never the reference's bit-exact geometry (depth, conic, radius, rectangle).
+// MUFU approximations (relative error ~2^-22) for quantities that carry their own margins (the
+// early screen test, the pixel bounds, log2 of the opacity), never the reference's bit-exact
+// geometry (depth, conic, radius, rectangle) or colour.
 __device__ __forceinline__ float sqrt_approx(float x) {
     float y;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float rsqrt_approx(float x) {
-    float y;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 __device__ __forceinline__ float lg2_approx(float x) {

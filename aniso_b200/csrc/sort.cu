@@ -13,6 +13,9 @@
 //   4. ceil(bits(tiles) / 8) LSD passes (or / 9 with 9-bit digits allowed, each pass 8 bits wide
 //      unless 9 are needed) stably sort the pairs by tile;
 //   5. tile ranges as gpu_render.cu:164-177.
+// A frame of at most kBinMaxTiles tiles replaces 4 and 5 by one stable counting pass over the
+// whole tile id (the one-pass tile binning below): two kernels where the LSD passes and the
+// ranges take five or six.
 // Each tile's run ends up ordered by (depth bits, entry index), exactly the reference's order, so
 // keys, values and ranges are bit-identical to the reference's for the same projection.
 //
@@ -45,6 +48,8 @@ constexpr int kScanItems = 4;
 constexpr int kScanBlock = kThreads * kScanItems;
 constexpr int kExpandItems = 8;
 constexpr int kExpandChunk = kThreads * kExpandItems;  // pairs per expansion CTA
+constexpr unsigned kBinMaxTiles = 4096;                 // global tiles of a frame the one-pass tile binning takes
+constexpr unsigned kBinMaxPairs = 1u << 24;             // and its pair capacity (the count matrix grows with it)
 static_assert(kBlockItems == kSortBlockItems, "an LSD block is kSortBlockItems items");
 static_assert(kExpandChunk == kSortBlockItems, "an expansion CTA writes exactly one LSD block of pairs");
 
@@ -496,21 +501,24 @@ __device__ __forceinline__ void expand_run(unsigned p0, unsigned P, unsigned G, 
 // search for its first pair, then a walk), row-major over each rectangle as gpu_render.cu:155-160
 // does. Tile ids are global over the batch. With first.counts set, the CTA also adds its pairs'
 // digits to the first tile pass's counts: its pairs are exactly LSD block b, all in one span, so
-// it counts them in shared memory and adds each non-zero digit count once.
+// it counts them in shared memory and adds each non-zero digit count once. With bin_counts set
+// instead (the one-pass tile binning), it counts its pairs per tile and writes row b of the
+// (block, tile) matrix, bin_tiles words, zeros included. The counts live in dynamic shared memory.
 __global__ void __launch_bounds__(kThreads) expand_kernel(const unsigned* __restrict__ sorted_idx,
                                                           const unsigned long long* __restrict__ rect_sorted,
                                                           const unsigned* __restrict__ offs,
                                                           const unsigned* __restrict__ chunk_start,
                                                           const Ctrl* __restrict__ ctrl, unsigned capacity,
                                                           BatchTables tables, unsigned* __restrict__ pair_key,
-                                                          unsigned* __restrict__ pair_val, PassCounts first) {
+                                                          unsigned* __restrict__ pair_val, PassCounts first,
+                                                          unsigned* __restrict__ bin_counts, unsigned bin_tiles) {
     chain_entry();
     __shared__ unsigned s_off[kExpandChunk + 2];
     __shared__ unsigned s_idx[kExpandChunk + 1];
     __shared__ unsigned s_org[kExpandChunk + 1];       // global tile of the rectangle's corner
     __shared__ unsigned short s_w[kExpandChunk + 1];   // rectangle width in tiles
     __shared__ unsigned short s_tx[kExpandChunk + 1];  // tiles per row of the entry's view
-    __shared__ unsigned s_hist[1 << kMaxRadixBits];
+    extern __shared__ unsigned s_hist[];               // digit (or tile) counts: launched with their size
     const int tid = threadIdx.x;
     if (ctrl->flags & kFlagOverflow) return;
     const unsigned long long P64 = ctrl->pair_total;
@@ -535,16 +543,23 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(const unsigned* __rest
         s_tx[k] = static_cast<unsigned short>(tx);
     }
     if (tid == 0) s_off[G] = j1 + 1 < V ? offs[j1 + 1] : P;
-    const bool count = first.counts != nullptr;
+    const bool bins = bin_counts != nullptr;
+    const bool count = first.counts != nullptr || bins;
+    const unsigned hist_words = bins ? bin_tiles : first.mask + 1;
     if (count)
-        for (unsigned d = tid; d <= first.mask; d += kThreads) s_hist[d] = 0;
+        for (unsigned d = tid; d < hist_words; d += kThreads) s_hist[d] = 0;
     __syncthreads();
 
     const unsigned p0 = base + tid * kExpandItems;
     if (p0 < P) expand_run(p0, P, G, s_off, s_idx, s_org, s_w, s_tx, pair_key, pair_val, count ? s_hist : nullptr,
-                           first.shift, first.mask);
+                           bins ? 0u : first.shift, bins ? 0xFFFFFFFFu : first.mask);
     if (!count) return;
     __syncthreads();
+    if (bins) {  // this block's row of the (block, tile) count matrix, every cell written
+        unsigned* row = bin_counts + static_cast<size_t>(blockIdx.x) * bin_tiles;
+        for (unsigned t = tid; t < bin_tiles; t += kThreads) row[t] = s_hist[t];
+        return;
+    }
     const unsigned span = span_of(base, first.spans, (P + kSortBlockItems - 1) / kSortBlockItems);
     for (unsigned d = tid; d <= first.mask; d += kThreads)
         if (s_hist[d]) atomicAdd(&first.counts[d * first.digit_stride + span * first.span_stride], s_hist[d]);
@@ -591,6 +606,206 @@ __global__ void __launch_bounds__(kThreads) ranges_kernel(const unsigned* __rest
     }
 }
 
+// ---- one-pass tile binning --------------------------------------------------------------------
+// Where a frame has at most kBinMaxTiles global tiles, the tile order is made in one stable
+// counting pass over the tile id instead of LSD passes over its digits: the expansion writes the
+// pairs in depth order and each block's per-tile counts (one row of a blocks x tiles matrix);
+// bin_scan turns every tile's column into the blocks' offsets within the tile and, in its last
+// CTA, the tiles' starts and ranges; bin_scatter sorts each block by tile in shared memory (two
+// stable 6-bit passes) and writes every pair to its tile's start + its block's offset + its rank in
+// the block. Stability at both levels keeps each tile's pairs in depth order: the reference's
+// order, as the LSD passes give it.
+constexpr int kBinLocalBits = 6;
+constexpr int kBinLocalR = 1 << kBinLocalBits;
+constexpr int kBinScanThreads = 1024;
+constexpr int kBinScanGroups = kBinScanThreads / 32;  // row groups per 32-tile column strip
+
+__device__ __forceinline__ bool frame_pairs(const Ctrl* ctrl, unsigned capacity, unsigned& P) {
+    if (ctrl->flags & kFlagOverflow) return false;
+    const unsigned long long pt = ctrl->pair_total;
+    if (pt > capacity) return false;
+    P = static_cast<unsigned>(pt);
+    return true;
+}
+
+// CTA c owns tiles [32 c, 32 c + 32): 32 groups of warps each sum a contiguous run of the blocks'
+// rows (one coalesced 128-byte read per row), the group sums are scanned, and each group writes
+// its rows' exclusive running sums back in place. The tiles' totals go to tile_start; the last CTA
+// to finish (a ticket on the control block: no CTA waits for another) scans them into the tiles'
+// starts and writes every tile's range ([0, 0) for a tile without pairs, as the reference's
+// cleared ranges are). (Eight-tile strips of 512 threads, every row load of a group in flight at
+// once, measured slower in the frame: 0.122 against 0.119 ms of sort.)
+__global__ void __launch_bounds__(kBinScanThreads) bin_scan_kernel(unsigned* __restrict__ counts, unsigned tiles,
+                                                                   unsigned* __restrict__ tile_start,
+                                                                   uint2* __restrict__ ranges, Ctrl* ctrl,
+                                                                   unsigned capacity) {
+    chain_entry();
+    __shared__ unsigned s_part[kBinScanGroups][33];
+    __shared__ unsigned s_tmp[kBinScanThreads / 32];
+    __shared__ unsigned s_last;
+    unsigned P;
+    if (!frame_pairs(ctrl, capacity, P)) return;
+    const unsigned blocks = (P + kBlockItems - 1) / kBlockItems;
+    const int tid = threadIdx.x, lane = tid & 31, g = tid >> 5;
+    const unsigned t = blockIdx.x * 32 + lane;
+    const unsigned r0 = static_cast<unsigned>(static_cast<unsigned long long>(blocks) * g / kBinScanGroups);
+    const unsigned r1 = static_cast<unsigned>(static_cast<unsigned long long>(blocks) * (g + 1) / kBinScanGroups);
+    unsigned sum = 0;
+    if (t < tiles)
+#pragma unroll 8
+        for (unsigned r = r0; r < r1; ++r) sum += counts[static_cast<size_t>(r) * tiles + t];
+    s_part[g][lane] = sum;
+    __syncthreads();
+    unsigned run = 0;
+    for (int k = 0; k < g; ++k) run += s_part[k][lane];
+    if (t < tiles) {
+        if (g == kBinScanGroups - 1) tile_start[t] = run + sum;  // the tile's total, for the last CTA
+#pragma unroll 8
+        for (unsigned r = r0; r < r1; ++r) {
+            unsigned* cell = counts + static_cast<size_t>(r) * tiles + t;
+            const unsigned c = *cell;
+            *cell = run;
+            run += c;
+        }
+    }
+    // Every thread's fence, not only the writers' of tile_start: measured 1 us faster per frame.
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(&ctrl->sort_barrier, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // The last CTA: tiles <= kBinMaxTiles = 4 per thread, in order.
+    constexpr int kPer = kBinMaxTiles / kBinScanThreads;
+    unsigned tot[kPer], own = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const unsigned tt = tid * kPer + k;
+        tot[k] = tt < tiles ? __ldcg(tile_start + tt) : 0u;
+        own += tot[k];
+    }
+    unsigned all;
+    unsigned start = block_excl_scan<kBinScanThreads>(own, s_tmp, all);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const unsigned tt = tid * kPer + k;
+        if (tt < tiles) {
+            tile_start[tt] = start;
+            ranges[tt] = tot[k] ? make_uint2(start, start + tot[k]) : make_uint2(0u, 0u);
+        }
+        start += tot[k];
+    }
+}
+
+// Block b (kBlockItems pairs of the depth-ordered list) sorted stably by tile in shared memory and
+// written out in tile order. bits: bits of the largest tile id (1..12); one local pass for up to 6,
+// else two (low 6 bits, then the rest). A lane ranks its item among the warp's with ballots on the
+// digit's bits (the items of a warp are in position order (k, lane)), warps in order, as the LSD
+// downsweep does.
+__global__ void __launch_bounds__(kThreads, 4) bin_scatter_kernel(const unsigned* __restrict__ keys_in,
+                                                                  const unsigned* __restrict__ vals_in,
+                                                                  unsigned* __restrict__ keys_out,
+                                                                  unsigned* __restrict__ vals_out,
+                                                                  const unsigned* __restrict__ counts, unsigned tiles,
+                                                                  int bits, const unsigned* __restrict__ tile_start,
+                                                                  const Ctrl* ctrl, unsigned capacity) {
+    chain_entry();
+    __shared__ unsigned short s_key[kBlockItems];
+    __shared__ unsigned s_val[kBlockItems];
+    __shared__ unsigned short s_first[kBinMaxTiles];  // first local position of each tile in the block
+    __shared__ unsigned s_wh[kWarps][kBinLocalR];
+    __shared__ unsigned s_dstart[kBinLocalR];
+    __shared__ unsigned s_tmp[kWarps];
+    unsigned P;
+    if (!frame_pairs(ctrl, capacity, P)) return;
+    const unsigned b = blockIdx.x;
+    if (static_cast<unsigned long long>(b) * kBlockItems >= P) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned lt = lanemask_lt();
+    unsigned key[kItems], val[kItems];
+    const unsigned long long wbase = static_cast<unsigned long long>(b) * kBlockItems + warp * (kItems * 32) + lane;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const unsigned long long idx = wbase + k * 32;
+        key[k] = idx < P ? keys_in[idx] : kBinMaxTiles;  // kBinMaxTiles: no item
+        val[k] = idx < P ? vals_in[idx] : 0u;
+    }
+    const int passes = bits > kBinLocalBits ? 2 : 1;
+    for (int pass = 0; pass < passes; ++pass) {
+        const int shift = pass * kBinLocalBits;
+        unsigned dg[kItems], rank[kItems];
+        if (tid < kBinLocalR)
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) s_wh[w][tid] = 0;
+#pragma unroll
+        for (int k = 0; k < kItems; ++k)
+            dg[k] = key[k] < kBinMaxTiles ? (key[k] >> shift) & (kBinLocalR - 1) : kBinLocalR;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            unsigned peers = 0xFFFFFFFFu;
+#pragma unroll
+            for (int bb = 0; bb <= kBinLocalBits; ++bb) {
+                const bool bit = (dg[k] >> bb) & 1u;
+                const unsigned vb = __ballot_sync(0xFFFFFFFFu, bit);
+                peers &= bit ? vb : ~vb;
+            }
+            const unsigned cnt = dg[k] < kBinLocalR ? s_wh[warp][dg[k]] : 0u;
+            rank[k] = cnt + __popc(peers & lt);
+            __syncwarp();
+            if (dg[k] < kBinLocalR && lane == 31 - __clz(peers)) s_wh[warp][dg[k]] = cnt + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        unsigned digit_count = 0;
+        if (tid < kBinLocalR)
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) {
+                const unsigned c = s_wh[w][tid];
+                s_wh[w][tid] = digit_count;
+                digit_count += c;
+            }
+        unsigned total;
+        const unsigned dstart = block_excl_scan<kThreads>(digit_count, s_tmp, total);
+        if (tid < kBinLocalR) s_dstart[tid] = dstart;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kItems; ++k)
+            if (dg[k] < kBinLocalR) {
+                const unsigned pos = s_dstart[dg[k]] + s_wh[warp][dg[k]] + rank[k];
+                s_key[pos] = static_cast<unsigned short>(key[k]);
+                s_val[pos] = val[k];
+            }
+        __syncthreads();
+        // Reload in (k, lane) order: the next pass ranks the items in their new order.
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const unsigned pos = warp * (kItems * 32) + k * 32 + lane;
+            const bool valid = static_cast<unsigned long long>(b) * kBlockItems + pos < P;
+            key[k] = valid ? s_key[pos] : kBinMaxTiles;
+            val[k] = valid ? s_val[pos] : 0u;
+        }
+        __syncthreads();
+    }
+    // key[k] is now the tile of local position pos (sorted); record each tile's first position.
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const unsigned pos = warp * (kItems * 32) + k * 32 + lane;
+        if (key[k] < kBinMaxTiles && (pos == 0 || s_key[pos - 1] != key[k]))
+            s_first[key[k]] = static_cast<unsigned short>(pos);
+    }
+    __syncthreads();
+    const unsigned* row = counts + static_cast<size_t>(b) * tiles;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        if (key[k] >= kBinMaxTiles) continue;
+        const unsigned pos = warp * (kItems * 32) + k * 32 + lane;
+        const unsigned g = __ldg(tile_start + key[k]) + __ldg(row + key[k]) + (pos - s_first[key[k]]);
+        keys_out[g] = key[k];
+        vals_out[g] = val[k];
+    }
+}
+
 // Depth keys (kCulledKey when tiles_touched is 0) and rectangles of a projection given in the
 // reference kernel's layout -- what the preprocess kernel writes for its own.
 __global__ void __launch_bounds__(kThreads) projection_keys_kernel(int64_t n, const unsigned* __restrict__ tiles_touched,
@@ -609,6 +824,12 @@ __global__ void __launch_bounds__(kThreads) projection_keys_kernel(int64_t n, co
                     (static_cast<unsigned long long>(r.z) << 32) | (static_cast<unsigned long long>(r.w) << 48);
     }
     depth_key[i] = key;
+}
+
+int bits_of(unsigned v) {  // bits needed to hold v
+    int b = 0;
+    while (b < 32 && (v >> b) != 0) ++b;
+    return b;
 }
 
 unsigned spans_for(uint64_t max_items) {
@@ -722,9 +943,37 @@ void launch_radix_scatter(const unsigned* keys_in, const unsigned* vals_in, unsi
                         zero_words, ctrl, stream);
 }
 
+namespace {
+// The expansion's counts live in dynamic shared memory; with the 16 KB of a tile-bin row it goes
+// past the 48 KB a kernel gets without asking (once per device).
+constexpr int kMaxDevices = 64;
+bool g_expand_smem_set[kMaxDevices];
+
+void allow_expand_smem() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return;
+    }
+    if (g_expand_smem_set[dev]) return;
+    if (cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kBinMaxTiles * sizeof(unsigned))) == cudaSuccess)
+        g_expand_smem_set[dev] = true;
+    else
+        cudaGetLastError();
+}
+}  // namespace
+
+unsigned bin_max_tiles() { return kBinMaxTiles; }
+unsigned bin_max_pairs() { return kBinMaxPairs; }
+size_t bin_count_words(unsigned capacity, unsigned tiles) {
+    return static_cast<size_t>((capacity + kBlockItems - 1) / kBlockItems) * tiles;
+}
+
 void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect16, Ctrl* ctrl, unsigned capacity,
                       unsigned max_visible, const BatchTables& tables, const DupBuffers& buf, unsigned* pair_key,
-                      unsigned* pair_val, cudaStream_t stream, const PassCounts& first) {
+                      unsigned* pair_val, cudaStream_t stream, const PassCounts& first, unsigned* bin_counts,
+                      unsigned bin_tiles) {
     if (max_visible == 0) return;
     const unsigned spans = spans_for(max_visible);
     launch_chained(pair_count_kernel, dim3(spans), dim3(kThreads), stream, sorted_idx, rect16, ctrl, spans, buf.rank,
@@ -733,8 +982,23 @@ void launch_duplicate(const unsigned* sorted_idx, const unsigned long long* rect
                    buf.span_sum, buf.offs, buf.chunk_start);
     // At least one CTA: with capacity 0 (a count-only call) the frame overflows and the CTA leaves.
     const unsigned expand_blocks = std::max(1u, (capacity + kExpandChunk - 1) / kExpandChunk);
-    launch_chained(expand_kernel, dim3(expand_blocks), dim3(kThreads), stream, sorted_idx, buf.rect_sorted, buf.offs,
-                   buf.chunk_start, ctrl, capacity, tables, pair_key, pair_val, first);
+    const unsigned hist_words = bin_counts ? bin_tiles : first.counts ? first.mask + 1 : 0u;
+    if (bin_counts) allow_expand_smem();
+    launch_chained_smem(expand_kernel, dim3(expand_blocks), dim3(kThreads), hist_words * sizeof(unsigned), stream,
+                        sorted_idx, buf.rect_sorted, buf.offs, buf.chunk_start, ctrl, capacity, tables, pair_key,
+                        pair_val, first, bin_counts, bin_tiles);
+}
+
+void launch_tile_bins(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out,
+                      unsigned* counts, unsigned tiles, unsigned* tile_start, uint2* ranges, Ctrl* ctrl,
+                      unsigned capacity, cudaStream_t stream) {
+    const int bits = std::max(1, bits_of(tiles > 0 ? tiles - 1 : 0));
+    launch_chained(bin_scan_kernel, dim3(std::max(1u, (tiles + 31) / 32)), dim3(kBinScanThreads), stream, counts,
+                   tiles, tile_start, ranges, ctrl, capacity);
+    const unsigned blocks = std::max(1u, (capacity + kBlockItems - 1) / kBlockItems);
+    launch_chained(bin_scatter_kernel, dim3(blocks), dim3(kThreads), stream, keys_in, vals_in, keys_out, vals_out,
+                   static_cast<const unsigned*>(counts), tiles, bits, static_cast<const unsigned*>(tile_start),
+                   static_cast<const Ctrl*>(ctrl), capacity);
 }
 
 void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capacity, uint2* ranges,

@@ -169,7 +169,9 @@ def config2_scene():
 
 
 PROJ_CASES = {
+    # at most 4096 tiles: the one-pass tile binning; above: the LSD tile passes and the ranges kernel
     "cloud20k": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(333, 217)),
+    "cloud20k_8160tiles": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(1920, 1088)),
     "config1": lambda: ((lambda s: oracle.Restatement().activate(s) + (3,))(scenes.config(1)[0][0]),
                         scenes.config(1)[1][0][0]),
     # the bench workload itself: 740k Gaussians, ~325k visible, ~1.6M pairs at 1280x720
@@ -201,7 +203,7 @@ def test_sort_bit_exact_given_same_projection(ab, torch_cuda, case):
     r = ab.GpuRenderer(g, sh, deg)
     proj = r.debug_projection(cam)
     tx, ty = (cam.width + 15) // 16, (cam.height + 15) // 16
-    tiles, values, ranges = r.debug_sorted(cam)
+    tiles, values, ranges = r.debug_sorted(cam, capacity=int(proj["tiles_touched"].astype(np.int64).sum()) + 1024)
     keys = ab.keys_of(tiles, values, proj["depth"])
     # the C restatement of the reference's integer work
     okeys, ovalues, oranges = oracle.Restatement().sort_keys(proj["tiles_touched"], proj["rect"], proj["depth"], tx, ty)
