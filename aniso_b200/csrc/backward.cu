@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_backward_kernel(BackwardIn 
             s_r1[slot] = r.r1;
             s_b[slot] = r.r2.x;
             // The forward's masks (the same function), so the adjoint walks exactly its splats.
-            s_mask[slot] = static_cast<unsigned char>(splat_block_mask<TW, TH>(r, ox, oy));
+            s_mask[slot] = static_cast<unsigned char>(staged_block_mask<TW, TH, true>(r, ox, oy));
             s_hit[slot] = 0;
             const unsigned j = in.rank[g];
             const unsigned long long rc = in.rect_sorted[j];

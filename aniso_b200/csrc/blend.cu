@@ -13,13 +13,17 @@
 //     folded in) are shared, and the two pixels' offsets and FMAs are packed FP32x2 instructions
 //     (three for both pixels' exponents);
 //   * the block stages kBatch splat records per round in shared memory and, per splat, a mask of
-//     the warp blocks it can touch: its pixel bounds (the CPU 8x8-tile rectangle cut by the
-//     ellipse where alpha can reach 1/255, with a margin) against each 8x8 block. The 8x8 part
-//     gives every pixel exactly the splat list of the CPU renderer whatever the tile shape (so the
-//     image does not depend on it); the ellipse part only drops splats that cannot pass the alpha
-//     test anywhere in the block, so it changes no result. Testing each block against the
-//     ellipse itself (splat_block_mask, which the adjoint uses) dropped too few more splats to
-//     pay for the test in the staging: 0.161 -> 0.186 ms per 740k frame;
+//     the warp blocks it can touch (staged_block_mask): its pixel bounds (the CPU 8x8-tile
+//     rectangle cut by the bounding box of the ellipse where alpha can reach 1/255, with a margin)
+//     against each 8x8 block -- which gives every pixel exactly the splat list of the CPU renderer
+//     whatever the tile shape (so the image does not depend on it) -- and, in training, the
+//     record's block bits (the blocks where the ellipse itself reaches the cut, set once per splat
+//     by the training preprocess), which only drop splats that cannot pass the alpha test anywhere
+//     in the block, so they change no result. The plain forward leaves them out: their cost in the
+//     preprocess (+14 us per 740k frame) is more than the blend steps they save (-9 us), where the
+//     training step, whose adjoint replays every step at about four times the cost, gains (forward
+//     and adjoint at 2.2M: 1.84 -> 1.73 ms; the 8-scene training batch 29.0 -> 27.0 ms a step). Testing every block against the ellipse in each
+//     tile's staging instead cost more than it saved: 0.161 -> 0.186 ms of blend;
 //   * each warp walks only its set bits (ballot + ffs); a finished pixel holds T = 0 (T >= 1e-4
 //     while it is not finished), so no separate flag is carried; the warp leaves once all 64
 //     pixels are finished and the block stops loading once all its warps have (__syncthreads_or).
@@ -28,8 +32,6 @@
 
 namespace ab2 {
 namespace {
-
-__device__ __forceinline__ bool overlaps(int lo, int hi, int a, int b) { return lo <= b && hi >= a; }
 
 // One pixel's step for one splat. p is the base-2 exponent including log2(opacity) L, so
 // alpha = min(0.99, 2^p) and the reference's "power > 0" skip is p > L. The new transmittance is
@@ -158,15 +160,7 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
                 s_r0[slot] = r.r0;
                 s_r1[slot] = r.r1;
                 s_b[slot] = r.r2.x;
-                const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
-                const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
-                unsigned cols = 0;
-#pragma unroll
-                for (int c = 0; c < kWarpsX; ++c)
-                    if (overlaps(xlo, xhi, ox + 8 * c, ox + 8 * c + 7)) cols |= 1u << c;
-#pragma unroll
-                for (int rr = 0; rr < TH / 8; ++rr)
-                    if (overlaps(ylo, yhi, oy + 8 * rr, oy + 8 * rr + 7)) m |= cols << (kWarpsX * rr);
+                m = staged_block_mask<TW, TH, kTrain>(r, ox, oy);
             }
             s_mask[slot] = static_cast<unsigned char>(m);
         }

@@ -267,11 +267,13 @@ __device__ __forceinline__ float ex2_approx(float x) {
 }
 
 // Blend record: three float4 per visible Gaussian.
-//   r0 = (u, v, A2, B2)     r1 = (C2, L, r, g)     r2 = (b, bx, by, 0)
+//   r0 = (u, v, A2, B2)     r1 = (C2, L, r, g)     r2 = (b, bx, by, block bits)
 // where the exponent of the Gaussian in base 2 is A2 dx^2 + B2 dx dy + C2 dy^2 (the conic scaled
 // by -log2(e)/2, -log2(e), -log2(e)/2), L = log2(opacity), and bx / by hold two int16 pixel bounds
 // (lo | hi << 16): the pixels that lie both in the splat's 8x8-tile rectangle (render.cpp:166-171)
-// and inside the ellipse where alpha can reach 1/255 (with a safety margin).
+// and inside the ellipse where alpha can reach 1/255 (with a safety margin); the block bits
+// (record_block_bits) mark the 8x8 pixel blocks of those bounds where the splat can pass the
+// alpha test.
 struct SplatRecord {
     float4 r0, r1, r2;
 };
@@ -307,57 +309,112 @@ __device__ __forceinline__ unsigned pack_i16x2(int lo, int hi) {
 __device__ __forceinline__ int unpack_lo(unsigned v) { return static_cast<int>(static_cast<short>(v & 0xFFFFu)); }
 __device__ __forceinline__ int unpack_hi(unsigned v) { return static_cast<int>(static_cast<short>(v >> 16)); }
 
-// The largest base-2 exponent A2 dx^2 + B2 dx dy + C2 dy^2 (a concave form: A2, C2 < 0) over the
-// pixel-centre rectangle [X0, X1] x [Y0, Y1] of offsets from the splat centre. At the centre if the
-// rectangle holds it (0), else on an edge, where the form is a 1-D concave quadratic whose vertex
-// (dy = kx X on an edge X = const, dx = ky Y on an edge Y = const) is clamped into the edge.
-__device__ __forceinline__ float form_max(float A, float B, float C, float kx, float ky, float X0, float X1,
-                                          float Y0, float Y1) {
-    if (X0 <= 0.f && X1 >= 0.f && Y0 <= 0.f && Y1 >= 0.f) return 0.f;
-    const auto q = [&](float x, float y) { return fmaf(fmaf(A, x, B * y), x, C * y * y); };
-    const float ya = fminf(fmaxf(kx * X0, Y0), Y1), yb = fminf(fmaxf(kx * X1, Y0), Y1);
-    const float xa = fminf(fmaxf(ky * Y0, X0), X1), xb = fminf(fmaxf(ky * Y1, X0), X1);
-    return fmaxf(fmaxf(q(X0, ya), q(X1, yb)), fmaxf(q(xa, Y0), q(xb, Y1)));
+__device__ __forceinline__ float sqrt_mufu(float x) {  // MUFU square root, relative error ~2^-22
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
 
-// The 8x8 pixel blocks of a TW x TH tile at pixel (ox, oy) in which a splat can pass the alpha test,
-// bit rr * (TW / 8) + c for block (c, rr). A block is kept when it overlaps the splat's pixel bounds
-// (its 8x8-tile rectangle of the CPU renderer cut by the bounding box of the ellipse where alpha can
-// reach 1/255) AND, over the pixel centres the two share, the splat's exponent can still reach the
-// cut: L + max(form) >= log2(1/255), widened by 0.02 plus a term relative to the size of the form's
-// terms (in log2 units), which covers the rounding of this test and of the blend's own evaluation,
-// so a dropped block is one where no pixel can pass -- the image does not change, only the warp
-// steps that could not apply anything are skipped. The forward and adjoint blends use the same
-// masks, so the adjoint replays exactly the forward's walk.
-template <int TW, int TH>
-__device__ __forceinline__ unsigned splat_block_mask(const SplatRecord& r, int ox, int oy) {
-    constexpr int kWX = TW / 8, kWY = TH / 8;
+// The x-offset interval [xl, xr] (from the splat centre) over which A x^2 + B x y + C y^2 >= D for
+// some y in [Y0, Y1]; false when there is none. The form is concave (A, C < 0, 4AC > B^2), so the
+// region is an ellipse: its right boundary is concave in y, largest (the half-width W) at
+// y = yr = -B W / 2C, so over the band it is largest at the band's point nearest yr (there the
+// larger root of the quadratic in x); the left boundary likewise, mirrored (y = -yr). inv2a =
+// 1 / 2A. MUFU square roots: the caller widens the interval far beyond their error.
+__device__ __forceinline__ bool band_extent(float A, float B, float C, float D, float inv2a, float W, float yr,
+                                            float Y0, float Y1, float& xl, float& xr) {
+    const auto root = [&](float Y, float sign, float& x) {  // sign -1: the larger root, +1: the smaller
+        const float by = B * Y, disc = by * by - 4.f * A * (C * Y * Y - D);
+        if (!(disc >= 0.f)) return false;
+        x = (sign * sqrt_mufu(disc) - by) * inv2a;
+        return true;
+    };
+    if (yr >= Y0 && yr <= Y1) xr = W;
+    else if (!root(yr > Y1 ? Y1 : Y0, -1.f, xr)) return false;
+    const float yl = -yr;
+    if (yl >= Y0 && yl <= Y1) xl = -W;
+    else if (!root(yl > Y1 ? Y1 : Y0, 1.f, xl)) return false;
+    return xl <= xr;
+}
+
+// The block bits of a blend record (its r2.w), made once per visible entry by the training
+// preprocess (the plain one leaves every bit set): over the 8x8 pixel blocks (absolute: block x
+// covers pixels [8x, 8x + 7]) that the splat's pixel bounds (r2.y, r2.z: its 8x8-tile rectangle of
+// the CPU renderer cut by the bounding box of the ellipse where alpha can reach 1/255) overlap,
+// x0b = xlo >> 3 .. and wb blocks wide, bit j * wb + i is set unless the splat's exponent stays
+// below log2(1/255) at every pixel centre of block (x0b + i, y0b + j): per block row, the x-extent
+// of the ellipse over the row band's centre offsets (band_extent, a continuous superset of the
+// centres), widened, against the blocks' centre offsets. The cut is lowered by 0.02 plus a term
+// relative to the size of the form's terms over the bounds (in log2 units), and the extent widened
+// by 1e-3 of the half-width plus 0.01 pixel, which covers the rounding of this test and of the
+// blend's own evaluation. Bounds of more than 32 blocks, or a degenerate form (a coefficient that
+// is 0 or not finite, or not concave), set every bit. A blend skips a splat on a block whose bit is
+// clear: no pixel there could take anything from it, so the image does not change (and does not
+// depend on the tile shape: the blocks are the image's, not the tile's); only warp steps that could
+// apply nothing are saved.
+__device__ __forceinline__ unsigned record_block_bits(const SplatRecord& r) {
     constexpr float kCut = -7.99435343685885793f;  // log2(1/255)
     const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
     const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
+    if (xhi < xlo || yhi < ylo) return 0u;
+    const int x0b = xlo >> 3, y0b = ylo >> 3, wb = (xhi >> 3) - x0b + 1, hb = (yhi >> 3) - y0b + 1;
     const float u = r.r0.x, v = r.r0.y, A = r.r0.z, B = r.r0.w, C = r.r1.x, L = r.r1.y;
-    // A degenerate form (a coefficient that is 0 or not finite) keeps every overlapping block.
-    const bool exact = A < 0.f && C < 0.f && isfinite(A + B + C + L);
-    const float kx = exact ? __fdividef(-B, 2.f * C) : 0.f, ky = exact ? __fdividef(-B, 2.f * A) : 0.f;
+    const float det4 = 4.f * A * C - B * B;
+    if (wb * hb > 32 || !(A < 0.f && C < 0.f && det4 > 0.f && isfinite(A + B + C + L + det4))) return 0xFFFFFFFFu;
+    const float mx = fmaxf(fabsf(xlo + 0.5f - u), fabsf(xhi + 0.5f - u));
+    const float my = fmaxf(fabsf(ylo + 0.5f - v), fabsf(yhi + 0.5f - v));
+    const float size = fabsf(A) * mx * mx + fabsf(B) * mx * my + fabsf(C) * my * my;
+    const float D = kCut - 0.02f - 1e-5f * size - L;  // the form must reach D somewhere
+    if (D > 0.f) return 0u;                             // it cannot: its largest value is 0
+    const float W = sqrt_mufu(D * (4.f * C) * __frcp_rn(det4));  // half-width: D / (A - B^2 / 4C)
+    const float yr = -B * W * __frcp_rn(2.f * C);
+    const float inv2a = __frcp_rn(2.f * A);
+    const float eps = 1e-3f * W + 0.01f;
+    unsigned bits = 0;
+    for (int j = 0; j < hb; ++j) {
+        const int y0 = max(ylo, 8 * (y0b + j)), y1 = min(yhi, 8 * (y0b + j) + 7);
+        float xl, xr;
+        if (!band_extent(A, B, C, D, inv2a, W, yr, y0 + 0.5f - v, y1 + 0.5f - v, xl, xr)) continue;
+        // blocks whose centre offsets [8 b + 0.5 - u, 8 b + 7.5 - u] meet [xl - eps, xr + eps]
+        const int lo = max(0, static_cast<int>(ceilf((u + xl - eps - 7.5f) * 0.125f)) - x0b);
+        const int hi = min(wb - 1, static_cast<int>(floorf((u + xr + eps - 0.5f) * 0.125f)) - x0b);
+        if (lo <= hi) bits |= ((2u << hi) - (1u << lo)) << (j * wb);  // bits lo..hi (2u << 31 wraps to 0)
+    }
+    return bits;
+}
+
+// The 8x8 pixel blocks of a TW x TH tile at pixel (ox, oy, multiples of 8) that a staged splat
+// record may touch, bit rr * (TW / 8) + c for block (c, rr): the blocks its pixel bounds overlap,
+// and with kBits only those whose bit in the record's block bits is set. The training forward and
+// the adjoint stage the same masks.
+template <int TW, int TH, bool kBits>
+__device__ __forceinline__ unsigned staged_block_mask(const SplatRecord& r, int ox, int oy) {
+    constexpr int kWX = TW / 8, kWY = TH / 8;
+    const unsigned bx = __float_as_uint(r.r2.y), by = __float_as_uint(r.r2.z);
+    const int xlo = unpack_lo(bx), xhi = unpack_hi(bx), ylo = unpack_lo(by), yhi = unpack_hi(by);
     unsigned m = 0;
+    if (!kBits) {
+        unsigned cols = 0;
+#pragma unroll
+        for (int c = 0; c < kWX; ++c)
+            if (xlo <= ox + 8 * c + 7 && xhi >= ox + 8 * c) cols |= 1u << c;
+#pragma unroll
+        for (int rr = 0; rr < kWY; ++rr)
+            if (ylo <= oy + 8 * rr + 7 && yhi >= oy + 8 * rr) m |= cols << (kWX * rr);
+        return m;
+    }
+    const unsigned bits = __float_as_uint(r.r2.w);
+    const int x0b = xlo >> 3, y0b = ylo >> 3, wb = (xhi >> 3) - x0b + 1;
 #pragma unroll
     for (int rr = 0; rr < kWY; ++rr) {
-        const int y0 = max(ylo, oy + 8 * rr), y1 = min(yhi, oy + 8 * rr + 7);
-        if (y0 > y1) continue;
-        const float Y0 = static_cast<float>(y0) + 0.5f - v, Y1 = static_cast<float>(y1) + 0.5f - v;
+        const int py = oy + 8 * rr;
+        if (ylo > py + 7 || yhi < py) continue;
 #pragma unroll
         for (int c = 0; c < kWX; ++c) {
-            const int x0 = max(xlo, ox + 8 * c), x1 = min(xhi, ox + 8 * c + 7);
-            if (x0 > x1) continue;
-            bool keep = true;
-            if (exact) {
-                const float X0 = static_cast<float>(x0) + 0.5f - u, X1 = static_cast<float>(x1) + 0.5f - u;
-                const float best = form_max(A, B, C, kx, ky, X0, X1, Y0, Y1);
-                const float mx = fmaxf(fabsf(X0), fabsf(X1)), my = fmaxf(fabsf(Y0), fabsf(Y1));
-                const float size = fabsf(A) * mx * mx + fabsf(B) * mx * my + fabsf(C) * my * my;
-                keep = L + best + 0.02f + 1e-5f * size >= kCut;
-            }
-            if (keep) m |= 1u << (rr * kWX + c);
+            const int px = ox + 8 * c;
+            if (xlo > px + 7 || xhi < px) continue;
+            const int idx = ((py >> 3) - y0b) * wb + ((px >> 3) - x0b);
+            if (idx >= 32 || ((bits >> idx) & 1u)) m |= 1u << (rr * kWX + c);
         }
     }
     return m;

@@ -7,6 +7,8 @@
 //   * writes the blend record (SplatRecord) and the tile rectangle of visible Gaussians;
 //   * writes every entry's depth key (the float bits of its depth; a sentinel if culled) -- the
 //     first LSD pass of the depth sort compacts the visible ones as it ranks them.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -288,7 +290,8 @@ __device__ __forceinline__ void project_entry(const Src& src, int64_t i, const f
     SplatRecord r;
     r.r0 = make_float4(p.u, p.v, kHalfLog2e * p.conicA, kLog2e * p.conicB);
     r.r1 = make_float4(kHalfLog2e * p.conicC, log2_opacity, rgb.x, rgb.y);
-    r.r2 = make_float4(rgb.z, __uint_as_float(bx), __uint_as_float(by), 0.f);
+    r.r2 = make_float4(rgb.z, __uint_as_float(bx), __uint_as_float(by), __uint_as_float(0xFFFFFFFFu));
+    if (std::is_same<Src, RawParams>::value) r.r2.w = __uint_as_float(record_block_bits(r));  // training
     rec[e] = r;
     rect16[e] = static_cast<unsigned long long>(p.x0) | (static_cast<unsigned long long>(p.y0) << 16) |
                 (static_cast<unsigned long long>(p.x1) << 32) | (static_cast<unsigned long long>(p.y1) << 48);
