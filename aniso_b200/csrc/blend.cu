@@ -22,8 +22,9 @@
 //     in the block, so they change no result. The plain forward leaves them out: their cost in the
 //     preprocess (+14 us per 740k frame) is more than the blend steps they save (-9 us), where the
 //     training step, whose adjoint replays every step at about four times the cost, gains (forward
-//     and adjoint at 2.2M: 1.84 -> 1.73 ms; the 8-scene training batch 29.0 -> 27.0 ms a step). Testing every block against the ellipse in each
-//     tile's staging instead cost more than it saved: 0.161 -> 0.186 ms of blend;
+//     and adjoint at 2.2M: 1.84 -> 1.73 ms; the 8-scene training batch 29.0 -> 27.0 ms a step).
+//     Testing every block against the ellipse in each tile's staging instead cost more than it
+//     saved: 0.161 -> 0.186 ms of blend;
 //   * each warp walks only its set bits (ballot + ffs); a finished pixel holds T = 0 (T >= 1e-4
 //     while it is not finished), so no separate flag is carried; the warp leaves once all 64
 //     pixels are finished and the block stops loading once all its warps have (__syncthreads_or).
