@@ -356,8 +356,11 @@ __device__ __forceinline__ void copy_words(T& dst, const T& src) {
         reinterpret_cast<unsigned*>(&dst)[threadIdx.x] = reinterpret_cast<const unsigned*>(&src)[threadIdx.x];
 }
 
+// Held to 128 registers (four CTAs per SM): the kernel waits on memory, and the extra warps
+// measured faster where it runs many times per step (the 8-scene training batch: 27.0 -> 25.2 ms a
+// step; 102 registers spilled and was no faster; the adjoint blend held to 64 was slower).
 template <int D, bool kFresh>
-__global__ void __launch_bounds__(128) gauss_backward_kernel(const BatchScene<RawParams>* __restrict__ scenes,
+__global__ void __launch_bounds__(128, 4) gauss_backward_kernel(const BatchScene<RawParams>* __restrict__ scenes,
                                                              unsigned scene, const ViewInfo* __restrict__ views,
                                                              unsigned view, const RawGrads* __restrict__ grads_table,
                                                              const Ctrl* ctrl, const unsigned* __restrict__ list,
