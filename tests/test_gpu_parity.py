@@ -1,6 +1,6 @@
 """Parity of the B200 rasterizer with the reference, through the C ABI (needs a GPU).
 
-Bars (north star): images within 2/255 max-abs and at least 75 dB PSNR of the reference CPU
+Bars: images within 2/255 max-abs and at least 75 dB PSNR of the reference CPU
 renderer (render.cpp); tile ranges, sorted keys and values bit-identical to the reference GPU
 path (gpu_render.cu built without fast-math) given the same projection; the projection itself
 bit-identical to the reference preprocess kernel built the same way (depth, uv, conic, opacity,

@@ -2,7 +2,7 @@
 oracle: the oracle's analytic adjoint on every parameter, and FP64 central finite differences
 (h = 1e-4) on 256 sampled parameters.
 
-Bar (north star): <= 1e-3 relative error per parameter group,
+Bar: <= 1e-3 relative error per parameter group,
     rel = ||g_gpu - g_ref||_2 / ||g_ref||_2.
 Finite differences straddle the renderer's discontinuities (alpha clamp at 0.99, the 1/255 cut,
 early termination, the radius ceil of the tile rectangles) for a few samples: a sample whose
