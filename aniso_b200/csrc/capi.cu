@@ -553,17 +553,34 @@ struct Slot {
         return reinterpret_cast<const RawGrads*>(dev.p + P.grads_offset());
     }
     // Stages the blob and enqueues its upload on `st` (a chained kernel reading the mapped staging
-    // buffer, else a copy); returns the device views, scenes, tables.
+    // buffer, else a copy); returns the device views, scenes, tables. With `begin`, the frame's
+    // start (frame_begin's clears) is enqueued too, in the same kernel as the upload where that is
+    // a kernel.
+    struct FrameBegin {
+        Ctrl* ctrl;
+        unsigned* zero;
+        unsigned zero_words;
+        uint2* ranges;
+        unsigned tiles;
+    };
     template <class Src>
     int fill(const Plan<Src>& P, cudaStream_t st, const ViewInfo** views, const BatchScene<Src>** scenes,
-             BatchTables& tables) {
+             BatchTables& tables, const FrameBegin* begin = nullptr) {
         AB_TRY(stage(P));
         const size_t bytes = P.blob_bytes();
-        if (pinned_dev && bytes % 4 == 0)
-            launch_upload(reinterpret_cast<const unsigned*>(pinned_dev), reinterpret_cast<unsigned*>(dev.p),
-                          static_cast<unsigned>(bytes / 4), st);
-        else
+        if (pinned_dev && bytes % 4 == 0) {
+            if (begin)
+                launch_frame_start(reinterpret_cast<const unsigned*>(pinned_dev), reinterpret_cast<unsigned*>(dev.p),
+                                   static_cast<unsigned>(bytes / 4), begin->ctrl, begin->zero, begin->zero_words,
+                                   begin->ranges, begin->tiles, st);
+            else
+                launch_upload(reinterpret_cast<const unsigned*>(pinned_dev), reinterpret_cast<unsigned*>(dev.p),
+                              static_cast<unsigned>(bytes / 4), st);
+        } else {
             AB_CUDA(cudaMemcpyAsync(dev.p, pinned, bytes, cudaMemcpyHostToDevice, st));
+            if (begin)
+                launch_frame_begin(begin->ctrl, begin->zero, begin->zero_words, begin->ranges, begin->tiles, st);
+        }
         const size_t V = P.views.size(), S = P.scenes.size();
         unsigned char* d = dev.p;
         *views = reinterpret_cast<const ViewInfo*>(d);
@@ -602,12 +619,12 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     const ViewInfo* views = nullptr;
     const BatchScene<Src>* scenes = nullptr;
     BatchTables tables;
-    AB_TRY(slot.fill(P, st, &views, &scenes, tables));
     AB_TRY(A.reserve_ranges(static_cast<size_t>(P.tiles)));
-    if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
     unsigned zero_words = 0;
     const PassCounts first = first_pass_counts(A, static_cast<unsigned>(P.entries), &zero_words);
-    launch_frame_begin(A.ctrl.p, first.counts, zero_words, A.ranges.p, static_cast<unsigned>(P.tiles), st);
+    if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
+    const Slot::FrameBegin begin{A.ctrl.p, first.counts, zero_words, A.ranges.p, static_cast<unsigned>(P.tiles)};
+    AB_TRY(slot.fill(P, st, &views, &scenes, tables, &begin));
     launch_preprocess_any(scenes, P, views, A, dbg, first, st);
     if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
     int fin = 0;

@@ -32,6 +32,9 @@ void launch_upload(const unsigned* src_mapped, unsigned* dst, unsigned words, cu
 void launch_publish_ctrl(Ctrl* ctrl, Ctrl* host_mapped, cudaStream_t stream);
 void launch_frame_begin(Ctrl* ctrl, unsigned* zero, unsigned zero_words, uint2* ranges, unsigned tiles,
                         cudaStream_t stream);
+// launch_upload and then launch_frame_begin, as one kernel.
+void launch_frame_start(const unsigned* src_mapped, unsigned* dst, unsigned words, Ctrl* ctrl, unsigned* zero,
+                        unsigned zero_words, uint2* ranges, unsigned tiles, cudaStream_t stream);
 
 // Projection of every (view, Gaussian) entry of a batch; `blocks` = sum over scenes of
 // ceil(n / preprocess_gaussians_per_block()) (scene s starts at block scenes[s].block_base). counts.counts set: each visible

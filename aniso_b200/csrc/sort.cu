@@ -83,6 +83,27 @@ __global__ void upload_kernel(const unsigned* __restrict__ src, unsigned* __rest
     if (i < words) dst[i] = __ldcv(src + i);
 }
 
+// upload_kernel and frame_begin_kernel as one launch (the frame's first): threads copy the tables
+// and clear the control block, the counts and the ranges side by side. One kernel fewer at the
+// head of every frame's chain.
+__global__ void frame_start_kernel(const unsigned* __restrict__ src, unsigned* __restrict__ dst, unsigned words,
+                                   Ctrl* ctrl, unsigned* __restrict__ zero, unsigned zero_words,
+                                   uint2* __restrict__ range, unsigned ranges) {
+    chain_entry();
+    const unsigned stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
+    for (unsigned i = first; i < words; i += stride) dst[i] = __ldcv(src + i);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctrl->sticky_flags |= ctrl->flags;
+        if (ctrl->pair_total > ctrl->max_pair_total) ctrl->max_pair_total = ctrl->pair_total;
+        ctrl->pair_total = 0;
+        ctrl->vis_count = 0;
+        ctrl->flags = 0;
+        ctrl->sort_barrier = 0;
+    }
+    for (unsigned i = first; i < zero_words; i += stride) zero[i] = 0;
+    for (unsigned long long i = first; i < ranges; i += stride) range[i] = make_uint2(0u, 0u);
+}
+
 // Copies the control block into `host` (page-locked host memory this device maps) and clears its
 // flags, so that the next frame_begin does not fold flags the host has already read into the
 // sticky ones. One chained launch where a device-to-host copy and a memset would be two
@@ -842,6 +863,14 @@ unsigned spans_for(uint64_t max_items) {
 void launch_upload(const unsigned* src_mapped, unsigned* dst, unsigned words, cudaStream_t stream) {
     const unsigned blocks = std::max(1u, (words + kThreads - 1) / kThreads);
     launch_chained(upload_kernel, dim3(blocks), dim3(kThreads), stream, src_mapped, dst, words);
+}
+
+void launch_frame_start(const unsigned* src_mapped, unsigned* dst, unsigned words, Ctrl* ctrl, unsigned* zero,
+                        unsigned zero_words, uint2* ranges, unsigned tiles, cudaStream_t stream) {
+    const unsigned most = std::max(std::max(zero_words, tiles), words);
+    const unsigned blocks = std::max(1u, std::min((most + kThreads * 4 - 1) / (kThreads * 4), 148u));
+    launch_chained(frame_start_kernel, dim3(blocks), dim3(kThreads), stream, src_mapped, dst, words, ctrl, zero,
+                   zero_words, ranges, tiles);
 }
 
 void launch_publish_ctrl(Ctrl* ctrl, Ctrl* host, cudaStream_t stream) {

@@ -134,24 +134,25 @@ def test_many_tiles_with_nine_bit_digits(ab, torch, tile):
 
 
 def test_frame_kernel_count(ab):
-    """A small frame: the tables' upload, frame_begin, preprocess (which also counts the first
-    depth pass's digits), the multi-kernel sort (the default): the first depth pass (span scan +
-    downsweep), three more of upsweep + span scan + downsweep, pair count / offsets / expansion,
-    then for at most 4096 tiles the tile binning (scan + scatter, which also write the ranges),
-    else the first tile pass (2 kernels: the expansion counted its digits), any second one (3) and
-    the ranges; blend. With ANISO_B200_SORT=persistent the sort is one cooperative launch instead
-    (depth passes, pair expansion, tile passes, ranges)."""
+    """A small frame: the frame's start (the tables' upload and frame_begin's clears in one
+    kernel), preprocess (which also counts the first depth pass's digits), the multi-kernel sort
+    (the default): the first depth pass (span scan + downsweep), three more of upsweep + span
+    scan + downsweep, pair count / offsets / expansion, then for at most 4096 tiles the tile
+    binning (scan + scatter, which also write the ranges), else the first tile pass (2 kernels: the
+    expansion counted its digits), any second one (3) and the ranges; blend. With
+    ANISO_B200_SORT=persistent the sort is one cooperative launch instead (depth passes, pair
+    expansion, tile passes, ranges)."""
     import os
 
     multi = os.environ.get("ANISO_B200_SORT") != "persistent"
     g, sh, d = kat.random_cloud(5000, seed=3)
     r = ab.GpuRenderer(g, sh, d)
     r.render(kat.gpu_test_camera(320, 240))  # 300 tiles: binned
-    assert r.frame_kernels() == (1 + 1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 if multi else 5)
+    assert r.frame_kernels() == (1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 if multi else 4)
     r.render(kat.gpu_test_camera(64, 48))  # 12 tiles: binned
-    assert r.frame_kernels() == (1 + 1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 if multi else 5)
+    assert r.frame_kernels() == (1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 if multi else 4)
     r.render(kat.gpu_test_camera(1920, 1088))  # 8160 tiles: two LSD tile passes
-    assert r.frame_kernels() == (1 + 1 + 1 + 2 + 3 * 3 + 3 + 2 + 3 + 1 + 1 if multi else 5)
+    assert r.frame_kernels() == (1 + 1 + 2 + 3 * 3 + 3 + 2 + 3 + 1 + 1 if multi else 4)
 
 
 def test_large_batch_counts_digits_in_separate_passes(ab, torch):
