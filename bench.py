@@ -14,7 +14,7 @@ camera upload and the image's trip to the host (written across PCIe by the blend
 since the buffer is page-locked) are inside the timed region. Under torchrun each rank renders its own
 replica's 16 views (weak scaling, no collective); time is the max over ranks.
 
-Three more workloads of the same metric family ride along on rank 0 (skip with --no-extra):
+Three more workloads of the same metric family ride along at N = 1 (skip with --no-extra):
   "batched":  one 1M-Gaussian scene, 64 Fibonacci-sphere views of mixed resolution, rendered by one
               autotuned, graph-replayed batch versus 64 plain per-view launches (views/s);
   "fwd_bwd":  the 2.2M-Gaussian scene at 1280x720, forward + hand-written adjoint through the
@@ -659,14 +659,16 @@ def main():
         # Algorithmic bytes of one blend launch (per view): P*4 index + P*36 splat record + W*H*3 out.
         blend_bytes = pairs_per_step / V * 40 + W * H * 3
         achieved = blend_bytes / (blend_ms / 1000.0) / 1e9
-        base, acc = cpu_baseline_leg(gauss, sh, cams, images)
+        # The CPU baseline and the extra workloads run at N = 1 only: under torchrun the other ranks
+        # wait at the closing barrier, whose timeout minutes of rank-0-only work would exceed.
+        base, acc = cpu_baseline_leg(gauss, sh, cams, images) if world == 1 else (None, None)
         ex2_peak, fma_peak = measured_compute_peaks()
         # Algorithmic blend work: P * 256 pixel-splat evaluations per view (the upper bound; early
         # termination counts as speed-up), one MUFU ex2 each.
         evals = pairs_per_step / V * 256
         evals_per_s = evals / (blend_ms / 1000.0)
         extra = {}
-        if not args.no_extra:
+        if not args.no_extra and world == 1:
             extra["batched"] = batched_leg(torch, max(3, min(args.steps, 10)))
             extra["fwd_bwd"], check = fwd_bwd_leg(torch, max(3, min(args.steps, 10)))
             extra["train_batch"] = train_batch_leg(torch, 2)
