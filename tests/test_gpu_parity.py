@@ -171,6 +171,7 @@ def config2_scene():
 PROJ_CASES = {
     # at most 4096 tiles: the one-pass tile binning; above: the LSD tile passes and the ranges kernel
     "cloud20k": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(333, 217)),
+    "cloud20k_4096tiles": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(1024, 1024)),  # the binning's largest
     "cloud20k_8160tiles": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(1920, 1088)),
     "config1": lambda: ((lambda s: oracle.Restatement().activate(s) + (3,))(scenes.config(1)[0][0]),
                         scenes.config(1)[1][0][0]),
