@@ -203,9 +203,14 @@ struct Arena {
 // than a counting kernel; above it the counting kernel's streaming read is the cheaper of the two.
 constexpr uint64_t kProducerCountMax = 1ull << 22;
 
-// Depth passes: four 8-bit digits over the 32-bit depth keys (9-bit digits would need four too).
+// Depth passes: four 8-bit digits over the 32-bit depth keys, or three 9-bit digits over the low
+// 27 bits when every visible depth of the frame is known to be below 8192 (a "short" frame: its
+// keys are below 2^27, common.cuh).
 constexpr int kDepthPasses = 4;
 constexpr int kDepthBits = 8;
+constexpr int kShortDepthPasses = 3;
+constexpr int kShortDepthBits = 9;
+static_assert(kShortDepthPasses * kShortDepthBits == kShortDepthKeyBits, "the short passes cover the short keys");
 
 // Digit widths of the tile passes: as few passes as digits of at most max_bits (8 or 9) allow, each
 // pass 8 bits wide unless 9 are needed to stay within that count (17 tile bits: 9 + 8).
@@ -223,18 +228,19 @@ unsigned* count_matrix(Arena& A, int q) { return A.sort_scratch.p + (q & 1) * so
 
 // The digit counts of the first depth pass when the preprocess accumulates them (the frame is
 // small enough), else {NULL}. *zero_words: the cells frame_begin must clear for it. The persistent
-// sort chunks the pass over its CTAs and keeps the matrix CTA-major; the multi-kernel sort over
-// its spans, digit-major.
-PassCounts first_pass_counts(Arena& A, unsigned entries, unsigned* zero_words) {
+// sort chunks the pass over its CTAs and keeps the matrix CTA-major (its passes are always 8-bit);
+// the multi-kernel sort over its spans, digit-major, with 9-bit digits in a short frame.
+PassCounts first_pass_counts(Arena& A, unsigned entries, bool short_depth, unsigned* zero_words) {
     *zero_words = 0;
     if (entries == 0 || entries > kProducerCountMax) return PassCounts{};
     if (A.ctas) {
         *zero_words = A.ctas << kDepthBits;
         return PassCounts{A.pcounts.p, A.ctas, 0u, (1u << kDepthBits) - 1, 1u, 1u << kDepthBits};
     }
+    const int bits = short_depth ? kShortDepthBits : kDepthBits;
     const unsigned spans = sort_spans(entries);
-    *zero_words = spans << kDepthBits;
-    return PassCounts{count_matrix(A, 0), spans, 0u, (1u << kDepthBits) - 1, spans, 1u};
+    *zero_words = spans << bits;
+    return PassCounts{count_matrix(A, 0), spans, 0u, (1u << bits) - 1, spans, 1u};
 }
 
 // Steps 2-4 of a frame as one cooperative launch (sort_persistent.cu); *final_buf as enqueue_sort.
@@ -277,13 +283,17 @@ int enqueue_sort_persistent(Arena& A, unsigned entries, unsigned tiles, const Ba
 // was measured slower: keys written next to each other often share the next digit, the high depth
 // digits taking few values, so one atomic per key contends -- 0.177 ms against 0.139 ms for the
 // sort of the 740k / 1280x720 frame.) A frame of at most bin_max_tiles() tiles (A.bins_for) takes
-// the one-pass tile binning after the expansion instead of the tile passes and the ranges. Where
-// the persistent sort is selected (A.ctas), it replaces this
-// whole sequence with one launch and the same outputs.
+// the one-pass tile binning after the expansion instead of the tile passes and the ranges.
+// short_depth: every visible key is below 2^27 (Plan::bound_depth), so three 9-bit depth passes
+// replace the four 8-bit ones (measured 0.119 -> 0.111 ms of sort for the 740k frame). Where the
+// persistent sort is selected (A.ctas), it replaces this whole sequence with one launch and the
+// same outputs.
 int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& tables, bool keep_rank, int bits,
-                 bool first_counted, cudaStream_t st, int* final_buf) {
+                 bool first_counted, bool short_depth, cudaStream_t st, int* final_buf) {
     if (A.ctas)
         return enqueue_sort_persistent(A, entries, tiles, tables, keep_rank, bits, first_counted, st, final_buf);
+    const int depth_passes = short_depth ? kShortDepthPasses : kDepthPasses;
+    const int depth_bits = short_depth ? kShortDepthBits : kDepthBits;
     Ctrl* ctrl = A.ctrl.p;
     const unsigned cap = static_cast<unsigned>(std::max<int64_t>(A.n, 0));
     unsigned* totals = A.sort_scratch.p + 2 * sort_count_words();
@@ -294,24 +304,24 @@ int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& 
     const unsigned tile_spans = sort_spans(A.pair_cap);
     const PassCounts first_tile =
         expand_counts
-            ? PassCounts{count_matrix(A, kDepthPasses), tile_spans, 0u, (1u << tile_bits[0]) - 1, tile_spans, 1u}
+            ? PassCounts{count_matrix(A, depth_passes), tile_spans, 0u, (1u << tile_bits[0]) - 1, tile_spans, 1u}
             : PassCounts{};
 
-    for (int p = 0; p < kDepthPasses; ++p) {
+    for (int p = 0; p < depth_passes; ++p) {
         const int src = (p + 1) & 1, dst = p & 1;  // pass 0 reads depth_key and writes buffer 0
         const unsigned* keys_in = p == 0 ? A.depth_key.p : A.vis_key[src].p;
         const SortCount count = p == 0 ? SortCount::kFixed : SortCount::kVisible;
         const unsigned capacity = p == 0 ? entries : cap;
         if (!(p == 0 && first_counted))
-            launch_radix_count(keys_in, p == 0, count, entries, capacity, p * kDepthBits, kDepthBits,
+            launch_radix_count(keys_in, p == 0, count, entries, capacity, p * depth_bits, depth_bits,
                                count_matrix(A, p), ctrl, st);
-        const bool last = p == kDepthPasses - 1;
+        const bool last = p == depth_passes - 1;
         launch_radix_scatter(keys_in, p == 0 ? nullptr : A.vis_idx[src].p, last ? nullptr : A.vis_key[dst].p,
-                             A.vis_idx[dst].p, p == 0, count, entries, capacity, p * kDepthBits, kDepthBits,
+                             A.vis_idx[dst].p, p == 0, count, entries, capacity, p * depth_bits, depth_bits,
                              count_matrix(A, p), totals, last ? first_tile.counts : nullptr,
                              last && expand_counts ? tile_spans << tile_bits[0] : 0u, ctrl, st);
     }
-    const int sorted = (kDepthPasses - 1) & 1;
+    const int sorted = (depth_passes - 1) & 1;
     const DupBuffers dup{A.offs.p, keep_rank ? A.rank.p : nullptr, A.rect_sorted.p, A.chunk_start.p, A.span_sum.p};
     if (bins) {  // one stable counting pass over the tile id (and the ranges) instead of the tile passes
         launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, dup, A.pair_key[0].p,
@@ -324,7 +334,7 @@ int enqueue_sort(Arena& A, unsigned entries, unsigned tiles, const BatchTables& 
     launch_duplicate(A.vis_idx[sorted].p, A.rect16.p, ctrl, A.pair_cap, entries, tables, dup, A.pair_key[0].p,
                      A.pair_val[0].p, st, first_tile);
     for (int t = 0, shift = 0; t < tile_passes; shift += tile_bits[t], ++t) {
-        const int q = kDepthPasses + t;
+        const int q = depth_passes + t;
         const int src = t & 1, dst = src ^ 1;
         if (!(t == 0 && expand_counts))
             launch_radix_count(A.pair_key[src].p, false, SortCount::kPairs, 0u, A.pair_cap, shift, tile_bits[t],
@@ -397,6 +407,29 @@ int check_options(const aniso_b200_batch_options* o, PlanShape& shape) {
     return 0;
 }
 
+// The axis-aligned box of a scene's Gaussian positions, measured once when the scene is made;
+// finite is false when the scene has a position that is not finite (or no box was measured).
+struct PositionBox {
+    bool finite = false;
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+};
+
+// Whether every depth this camera can give a position in `box` is below the short keys' limit
+// (8192): the largest camera-space z over the box's corners, plus a margin far above the rounding
+// of the projection's fp32 z (R[6] x + R[7] y + R[8] z + t[2]), must stay below it.
+bool depth_short(const PositionBox& box, const CamParams& cam) {
+    if (!box.finite) return false;
+    double z = cam.t[2], mag = std::fabs(cam.t[2]);
+    for (int i = 0; i < 3; ++i) {
+        const double r = cam.R[6 + i];
+        z += std::max(r * box.lo[i], r * box.hi[i]);
+        mag += std::fabs(r) * std::max(std::fabs(box.lo[i]), std::fabs(box.hi[i]));
+    }
+    // 2^27 keys above 0.125's bits span 2^(27 - 23) = 16 binades: depths below 0.125 * 2^16.
+    const double limit = std::ldexp(0.125, 1 << (kShortDepthKeyBits - 23));
+    return z + 1e-5 * mag + 1.0 < limit;  // false for a NaN
+}
+
 // V views of S scenes: host tables, uploaded as one blob to a slot before each frame.
 template <class Src>
 struct Plan {
@@ -407,6 +440,7 @@ struct Plan {
     std::vector<RawGrads> grads;  // the backward's gradient buffers, one per scene (empty otherwise)
     uint64_t entries = 0, tiles = 0;
     unsigned pre_blocks = 0;
+    bool short_depth = false;  // three 9-bit depth passes (bound_depth)
 
     // srcs[s], stored degree deg[s]; view k of scene view_scene[k] (consecutive per scene).
     int build(const std::vector<Src>& srcs, const std::vector<int>& deg, const int32_t* view_scene, int n_views,
@@ -457,6 +491,16 @@ struct Plan {
         return 0;
     }
 
+    // Picks the short depth passes when every view's scene box (boxes[s], NULL: unknown) keeps its
+    // depths below 8192 for the view's camera, and the frame has at most kProducerCountMax entries
+    // (larger frames' 9-bit passes were measured slower: the 64-view 1M batch 8.69 -> 8.75 ms).
+    // Without a call (the training path's positions change every step) the frame keeps 8-bit passes.
+    void bound_depth(const std::vector<const PositionBox*>& boxes) {
+        short_depth = entries > 0 && entries <= kProducerCountMax;
+        for (const auto& v : views)
+            if (v.scene >= boxes.size() || !boxes[v.scene] || !depth_short(*boxes[v.scene], v.cam)) short_depth = false;
+    }
+
     // The largest degree any view is coloured with (the preprocess kernel's instantiation).
     int rendered_degree() const {
         int d = 0;
@@ -483,7 +527,7 @@ struct Plan {
                 return false;
         return shape.tile_w == o.shape.tile_w && shape.tile_h == o.shape.tile_h &&
                shape.blend_batch == o.shape.blend_batch && shape.radix_bits == o.shape.radix_bits &&
-               rendered_degree() == o.rendered_degree();
+               rendered_degree() == o.rendered_degree() && short_depth == o.short_depth;
     }
 };
 
@@ -621,7 +665,7 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     BatchTables tables;
     AB_TRY(A.reserve_ranges(static_cast<size_t>(P.tiles)));
     unsigned zero_words = 0;
-    const PassCounts first = first_pass_counts(A, static_cast<unsigned>(P.entries), &zero_words);
+    const PassCounts first = first_pass_counts(A, static_cast<unsigned>(P.entries), P.short_depth, &zero_words);
     if (ev) AB_CUDA(cudaEventRecord(ev[0], st));
     const Slot::FrameBegin begin{A.ctrl.p, first.counts, zero_words, A.ranges.p, static_cast<unsigned>(P.tiles)};
     AB_TRY(slot.fill(P, st, &views, &scenes, tables, &begin));
@@ -629,7 +673,7 @@ int enqueue_plan(Arena& A, Slot& slot, const Plan<Src>& P, cudaStream_t st, cuda
     if (ev) AB_CUDA(cudaEventRecord(ev[1], st));
     int fin = 0;
     AB_TRY(enqueue_sort(A, static_cast<unsigned>(P.entries), static_cast<unsigned>(P.tiles), tables, train,
-                        P.shape.radix_bits, first.counts != nullptr, st, &fin));
+                        P.shape.radix_bits, first.counts != nullptr, P.short_depth, st, &fin));
     if (ev) AB_CUDA(cudaEventRecord(ev[2], st));
     if (!stop_after_sort)
         launch_blend(static_cast<unsigned>(P.tiles), A.ranges.p, A.pair_val[fin].p, A.rec.p, A.ctrl.p, views, tables,
@@ -754,6 +798,7 @@ struct aniso_b200_scene {
     int degree = 0;
     int planes = 0;
     DevBuf<float4> pos_op, scale, rot, sh;
+    PositionBox box;  // of pos_op's positions, measured when the scene is made
     Arena arena;  // work buffers of the scene's own renders
     Slot slots[kSlots];
     int next_slot = 0;
@@ -976,6 +1021,86 @@ int device_present() {
     return 0;
 }
 
+constexpr int kBoxBlocks = 296;  // 2 CTAs per SM, 256 threads each, grid-strided
+
+// Per CTA, 7 floats: the smallest and largest x, y, z over the finite coordinates of the positions
+// (x, y, z of pos[i]) this CTA visits, and 1 when one of its coordinates was not finite, else 0.
+__global__ void __launch_bounds__(256) position_box_kernel(const float4* __restrict__ pos, int64_t n,
+                                                           float* __restrict__ out) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float bad = 0.f;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float4 p = pos[i];
+        const float c[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (!isfinite(c[k])) {
+                bad = 1.f;
+                continue;
+            }
+            lo[k] = fminf(lo[k], c[k]);
+            hi[k] = fmaxf(hi[k], c[k]);
+        }
+    }
+    __shared__ float s[8][7];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = fminf(lo[k], __shfl_xor_sync(0xFFFFFFFFu, lo[k], o));
+            hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xFFFFFFFFu, hi[k], o));
+        }
+        bad = fmaxf(bad, __shfl_xor_sync(0xFFFFFFFFu, bad, o));
+    }
+    if (lane == 0) {
+        for (int k = 0; k < 3; ++k) {
+            s[warp][k] = lo[k];
+            s[warp][3 + k] = hi[k];
+        }
+        s[warp][6] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        float v = s[0][threadIdx.x];
+        for (int w = 1; w < 8; ++w)
+            v = threadIdx.x < 3 ? fminf(v, s[w][threadIdx.x]) : fmaxf(v, s[w][threadIdx.x]);
+        out[blockIdx.x * 7 + threadIdx.x] = v;
+    }
+}
+
+// Measures the scene's position box (after the positions were written on s->stream; waits).
+int measure_box(aniso_b200_scene* s) {
+    s->box = PositionBox{};
+    if (s->n <= 0) return 0;
+    DevBuf<float> d;
+    AB_TRY(d.reserve(kBoxBlocks * 7));
+    position_box_kernel<<<kBoxBlocks, 256, 0, s->stream>>>(s->pos_op.p, s->n, d.p);
+    AB_CUDA(cudaGetLastError());
+    std::vector<float> h(kBoxBlocks * 7);
+    AB_CUDA(cudaMemcpyAsync(h.data(), d.p, h.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    AB_CUDA(cudaStreamSynchronize(s->stream));
+    PositionBox b;
+    b.finite = true;
+    for (int k = 0; k < 3; ++k) {
+        b.lo[k] = INFINITY;
+        b.hi[k] = -INFINITY;
+    }
+    for (int c = 0; c < kBoxBlocks; ++c) {
+        const float* r = &h[c * 7];
+        for (int k = 0; k < 3; ++k) {
+            b.lo[k] = std::min(b.lo[k], static_cast<double>(r[k]));
+            b.hi[k] = std::max(b.hi[k], static_cast<double>(r[3 + k]));
+        }
+        if (r[6] != 0.f) b.finite = false;
+    }
+    for (int k = 0; k < 3; ++k)
+        if (!(b.lo[k] <= b.hi[k])) b.finite = false;  // no finite coordinate on an axis
+    s->box = b;
+    return 0;
+}
+
 int new_scene(int64_t n, int degree, aniso_b200_scene** out, aniso_b200_scene** made) {
     if (!out) return fail(ANISO_B200_ERR_ARGUMENT, "out is NULL");
     if (n < 0 || n >= (int64_t(1) << 31)) return fail(ANISO_B200_ERR_ARGUMENT, "n must be in [0, 2^31)");
@@ -1012,7 +1137,9 @@ int single_plan(aniso_b200_scene* s, const aniso_b200_camera* camera, const anis
                 Plan<SceneView>& P) {
     if (options && options->sh_degree < 0) return fail(ANISO_B200_ERR_ARGUMENT, "sh_degree must be >= 0");
     const int32_t vs = 0;
-    return P.build({s->view()}, {s->degree}, &vs, 1, camera, scene_shape(options));
+    AB_TRY(P.build({s->view()}, {s->degree}, &vs, 1, camera, scene_shape(options)));
+    P.bound_depth({&s->box});
+    return 0;
 }
 
 }  // namespace
@@ -1061,6 +1188,7 @@ int aniso_b200_scene_create(const float* gaussians, const float* sh, int64_t n, 
         if (dg) cudaFree(dg);
         if (ds) cudaFree(ds);
         if (e != cudaSuccess) rc = cuda_fail(e, "scene upload");
+        else rc = measure_box(s);
     }
     if (rc != 0) {
         delete s;
@@ -1108,6 +1236,7 @@ int aniso_b200_scene_create_raw(const float* xyz, const float* f_dc, const float
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
         if (d) cudaFree(d);
         if (e != cudaSuccess) rc = cuda_fail(e, "scene upload");
+        else rc = measure_box(s);
     }
     if (rc != 0) {
         delete s;
@@ -1154,6 +1283,7 @@ int aniso_b200_scene_load_ply(const char* path, aniso_b200_scene** out) {
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
         if (d) cudaFree(d);
         if (e != cudaSuccess) rc = cuda_fail(e, "scene upload");
+        else rc = measure_box(s);
     }
     if (rc != 0) {
         delete s;
@@ -1368,7 +1498,11 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
         return fail(ANISO_B200_ERR_ARGUMENT, "bad size or NULL pairs");
     if (n > 0 && (!tiles_touched || !rect || !depth)) return fail(ANISO_B200_ERR_ARGUMENT, "input is NULL");
     uint64_t Pn = 0;
-    for (int64_t i = 0; i < n; ++i) Pn += tiles_touched[i];
+    bool short_depth = true;  // every listed depth in [0.125, 8192): offset keys, three 9-bit passes
+    for (int64_t i = 0; i < n; ++i) {
+        Pn += tiles_touched[i];
+        if (tiles_touched[i] && !(depth[i] >= 0.125f && depth[i] < 8192.0f)) short_depth = false;
+    }
     *pairs = Pn;
     if (Pn > capacity) return fail(ANISO_B200_ERR_ARGUMENT, "capacity too small");
     if (Pn > kMaxPairs) return fail(ANISO_B200_ERR_ARGUMENT, "more than 2^30 pairs");
@@ -1396,9 +1530,10 @@ int aniso_b200_sort_projection(int64_t n, const uint32_t* tiles_touched, const u
     const unsigned T = static_cast<unsigned>(tiles_x) * static_cast<unsigned>(tiles_y);
     AB_TRY(A.reserve_ranges(T));
     launch_frame_begin(A.ctrl.p, nullptr, 0u, A.ranges.p, T, st);
-    launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.depth_key.p, A.rect16.p, st);
+    launch_projection_keys(n, dtt.p, ddepth.p, drect.p, A.depth_key.p, A.rect16.p, st,
+                           short_depth ? kDepthKeyBase : 0u);
     int fin = 0;
-    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, kRadixBits, false, st, &fin));
+    AB_TRY(enqueue_sort(A, static_cast<unsigned>(n), T, tables, false, kRadixBits, false, short_depth, st, &fin));
     AB_CUDA(cudaGetLastError());
     AB_CUDA(cudaStreamSynchronize(st));
     Ctrl h;
@@ -1480,6 +1615,9 @@ int aniso_b200_batch_render(aniso_b200_batch* b, const aniso_b200_camera* camera
     }
     Plan<SceneView> P;
     AB_TRY(P.build(srcs, degs, b->view_scene.data(), static_cast<int>(b->view_scene.size()), cameras, b->shape));
+    std::vector<const PositionBox*> boxes;
+    for (auto* s : b->scenes) boxes.push_back(&s->box);
+    P.bound_depth(boxes);
     for (size_t k = 0; k < P.views.size(); ++k) {
         if (!rgb_device[k]) return fail(ANISO_B200_ERR_ARGUMENT, "an output buffer is NULL");
         P.views[k].rgb8 = rgb_device[k];

@@ -133,9 +133,16 @@ struct Ctrl {
     unsigned long long max_pair_total;  // largest pair_total of earlier frames since then
 };
 
-// Depth key of a culled Gaussian. Visible depths are >= 0.2 (or a canonical NaN), so their float
-// bits never have the sign bit set.
+// Depth key of a culled Gaussian. A visible entry's key is its depth's float bits less
+// kDepthKeyBase; visible depths are >= 0.2, so the keys never have the sign bit set.
 constexpr unsigned kCulledKey = 0xFFFFFFFFu;
+
+// The float bits of 0.125. Every visible depth is >= 0.2 > 0.125, so subtracting them keeps the
+// keys' order (positive floats order as their bits), and a depth below 8192 = 0.125 * 2^16 leaves
+// a key below 2^27: three 9-bit LSD passes then order the keys as four 8-bit passes over the
+// 32-bit depth bits do.
+constexpr unsigned kDepthKeyBase = 0x3E000000u;
+constexpr unsigned kShortDepthKeyBits = 27;
 
 enum : unsigned {
     kFlagOverflow = 1u,     // pairs exceeded the pair capacity: nothing after duplication ran

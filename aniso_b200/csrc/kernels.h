@@ -119,9 +119,11 @@ void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capac
                    cudaStream_t stream);
 
 // Depth keys and rectangles of a projection computed elsewhere (tiles_touched, rect, depth in the
-// reference kernel's layout), as the preprocess kernel writes them.
+// reference kernel's layout); a visible entry's key is its depth's bits less key_base (the
+// preprocess kernel's keys with kDepthKeyBase, the raw bits with 0).
 void launch_projection_keys(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
-                            unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream);
+                            unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream,
+                            unsigned key_base = 0);
 
 // ---- the persistent sort: steps 2-4 of a frame (depth passes, pair scan and expansion, tile
 // passes, tile ranges) as ONE cooperative launch of one 1024-thread CTA per SM, its phases

@@ -295,11 +295,11 @@ __device__ __forceinline__ void project_entry(const Src& src, int64_t i, const f
     rec[e] = r;
     rect16[e] = static_cast<unsigned long long>(p.x0) | (static_cast<unsigned long long>(p.y0) << 16) |
                 (static_cast<unsigned long long>(p.x1) << 32) | (static_cast<unsigned long long>(p.y1) << 48);
-    // The depth key: visible depths are >= 0.2 (or the canonical NaN), so the sign bit of
-    // kCulledKey never collides. The first depth pass compacts the visible entries.
-    const unsigned depth_bits = __float_as_uint(p.depth);
-    depth_key[e] = depth_bits;
-    if (counts.counts) count_key(counts, count_blocks, e, depth_bits);
+    // The depth key (the depth's bits less kDepthKeyBase: visible depths are >= 0.2, so the sign
+    // bit of kCulledKey never collides). The first depth pass compacts the visible entries.
+    const unsigned key = __float_as_uint(p.depth) - kDepthKeyBase;
+    depth_key[e] = key;
+    if (counts.counts) count_key(counts, count_blocks, e, key);
     if (kDebug) {
         dbg.uv[e] = make_float2(p.u, p.v);
         dbg.conic_opacity[e] = make_float4(p.conicA, p.conicB, p.conicC, pg.w);

@@ -827,19 +827,21 @@ __global__ void __launch_bounds__(kThreads, 4) bin_scatter_kernel(const unsigned
     }
 }
 
-// Depth keys (kCulledKey when tiles_touched is 0) and rectangles of a projection given in the
-// reference kernel's layout -- what the preprocess kernel writes for its own.
+// Depth keys (kCulledKey when tiles_touched is 0; else the depth's bits less key_base) and
+// rectangles of a projection given in the reference kernel's layout -- what the preprocess kernel
+// writes for its own.
 __global__ void __launch_bounds__(kThreads) projection_keys_kernel(int64_t n, const unsigned* __restrict__ tiles_touched,
                                                                    const float* __restrict__ depth,
                                                                    const uint4* __restrict__ rect,
                                                                    unsigned* __restrict__ depth_key,
-                                                                   unsigned long long* __restrict__ rect16) {
+                                                                   unsigned long long* __restrict__ rect16,
+                                                                   unsigned key_base) {
     chain_entry();
     const int64_t i = static_cast<int64_t>(blockIdx.x) * kThreads + threadIdx.x;
     if (i >= n) return;
     unsigned key = kCulledKey;
     if (tiles_touched[i]) {
-        key = __float_as_uint(depth[i]);
+        key = __float_as_uint(depth[i]) - key_base;
         const uint4 r = rect[i];
         rect16[i] = static_cast<unsigned long long>(r.x) | (static_cast<unsigned long long>(r.y) << 16) |
                     (static_cast<unsigned long long>(r.z) << 32) | (static_cast<unsigned long long>(r.w) << 48);
@@ -1038,11 +1040,11 @@ void launch_ranges(const unsigned* sorted_keys, const Ctrl* ctrl, unsigned capac
 }
 
 void launch_projection_keys(int64_t n, const unsigned* tiles_touched, const float* depth, const uint4* rect,
-                            unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream) {
+                            unsigned* depth_key, unsigned long long* rect16, cudaStream_t stream, unsigned key_base) {
     const unsigned blocks = static_cast<unsigned>((n + kThreads - 1) / kThreads);
     if (blocks == 0) return;
     launch_chained(projection_keys_kernel, dim3(blocks), dim3(kThreads), stream, n, tiles_touched, depth, rect,
-                   depth_key, rect16);
+                   depth_key, rect16, key_base);
 }
 
 }  // namespace ab2

@@ -133,26 +133,78 @@ def test_many_tiles_with_nine_bit_digits(ab, torch, tile):
     assert any(img.any() for img in nine)
 
 
+def test_batch_of_near_and_far_scenes(ab, torch):
+    """A scene with Gaussians past depth 8192 makes the whole batch sort depths with four 8-bit
+    passes; its views still equal single renders, which for the near scene take three 9-bit ones."""
+    near = kat.random_cloud(8000, seed=21)
+    g, sh, d = kat.random_cloud(8000, seed=22)
+    g = g.copy()
+    ratio = np.float32(12000.0) / g[:500, 2]
+    g[:500, 0] *= ratio
+    g[:500, 1] *= ratio
+    g[:500, 2] = 12000.0  # on screen and visible, past 8192
+    rs = [ab.GpuRenderer(*near), ab.GpuRenderer(g, sh, d)]
+    cams = [kat.gpu_test_camera(320, 240), kat.gpu_test_camera(333, 217), kat.gpu_test_camera(320, 240)]
+    view_scene = [0, 1, 1]
+    single = [rs[s].render(c) for s, c in zip(view_scene, cams)]
+    for graph in (False, True):
+        _, imgs, _ = render_batch(ab, torch, rs, view_scene, cams, ab.BatchOptions(use_graph=graph))
+        for k, (a, b) in enumerate(zip(imgs, single)):
+            np.testing.assert_array_equal(a, b, err_msg="view %d, graph %s" % (k, graph))
+
+
+def test_graph_batch_follows_cameras_across_the_depth_limit(ab, torch):
+    """A recorded batch whose cameras move back past depth 8192 (and forward again) is recorded
+    again for the other depth passes; every replay equals the single renders."""
+    g, sh, d = kat.random_cloud(6000, seed=23)
+    r = ab.GpuRenderer(g, sh, d)
+    b = ab.BatchRenderer([r], [0, 0], ab.BatchOptions(use_graph=True))
+    for tz in (0.0, 9000.0, 0.0):
+        cams = []
+        for w, h in ((320, 240), (256, 160)):
+            c = kat.gpu_test_camera(w, h)
+            f = c.fx * (1.0 + tz / 5.0)  # a longer lens keeps the cloud's size on screen
+            cams.append(scenes.Camera(w, h, f, f, c.cx, c.cy, np.asarray(c.R), np.array([0.0, 0.0, tz])))
+        outs = [torch.zeros((c.height, c.width, 3), dtype=torch.uint8, device="cuda") for c in cams]
+        for attempt in range(3):
+            b.render_device(cams, [o.data_ptr() for o in outs], torch.cuda.current_stream().cuda_stream)
+            try:
+                b.sync()
+                break
+            except ab.AnisoError as e:
+                if "pair capacity exceeded" not in str(e) or attempt == 2:
+                    raise
+        for k, c in enumerate(cams):
+            single = r.render(c)
+            assert single.any()
+            np.testing.assert_array_equal(outs[k].cpu().numpy(), single, err_msg="view %d, tz %g" % (k, tz))
+
+
 def test_frame_kernel_count(ab):
     """A small frame: the frame's start (the tables' upload and frame_begin's clears in one
     kernel), preprocess (which also counts the first depth pass's digits), the multi-kernel sort
-    (the default): the first depth pass (span scan + downsweep), three more of upsweep + span
-    scan + downsweep, pair count / offsets / expansion, then for at most 4096 tiles the tile
-    binning (scan + scatter, which also write the ranges), else the first tile pass (2 kernels: the
-    expansion counted its digits), any second one (3) and the ranges; blend. With
-    ANISO_B200_SORT=persistent the sort is one cooperative launch instead (depth passes, pair
-    expansion, tile passes, ranges)."""
+    (the default): the first depth pass (span scan + downsweep), two more of upsweep + span
+    scan + downsweep (three when a depth can reach 8192: the scene's box decides), pair count /
+    offsets / expansion, then for at most 4096 tiles the tile binning (scan + scatter, which also
+    write the ranges), else the first tile pass (2 kernels: the expansion counted its digits), any
+    second one (3) and the ranges; blend. With ANISO_B200_SORT=persistent the sort is one
+    cooperative launch instead (depth passes, pair expansion, tile passes, ranges)."""
     import os
 
     multi = os.environ.get("ANISO_B200_SORT") != "persistent"
     g, sh, d = kat.random_cloud(5000, seed=3)
     r = ab.GpuRenderer(g, sh, d)
     r.render(kat.gpu_test_camera(320, 240))  # 300 tiles: binned
-    assert r.frame_kernels() == (1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 if multi else 4)
+    assert r.frame_kernels() == (1 + 1 + 2 + 2 * 3 + 3 + 2 + 1 if multi else 4)
     r.render(kat.gpu_test_camera(64, 48))  # 12 tiles: binned
-    assert r.frame_kernels() == (1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 if multi else 4)
+    assert r.frame_kernels() == (1 + 1 + 2 + 2 * 3 + 3 + 2 + 1 if multi else 4)
     r.render(kat.gpu_test_camera(1920, 1088))  # 8160 tiles: two LSD tile passes
-    assert r.frame_kernels() == (1 + 1 + 2 + 3 * 3 + 3 + 2 + 3 + 1 + 1 if multi else 4)
+    assert r.frame_kernels() == (1 + 1 + 2 + 2 * 3 + 3 + 2 + 3 + 1 + 1 if multi else 4)
+    g = g.copy()
+    g[0, :3] = (0.0, 0.0, 9000.0)  # one Gaussian (on the axis, visible) past 8192: four depth passes
+    far = ab.GpuRenderer(g, sh, d)
+    far.render(kat.gpu_test_camera(320, 240))
+    assert far.frame_kernels() == (1 + 1 + 2 + 3 * 3 + 3 + 2 + 1 if multi else 4)
 
 
 def test_large_batch_counts_digits_in_separate_passes(ab, torch):

@@ -168,9 +168,29 @@ def config2_scene():
     return oracle.Restatement().activate(raws[0]) + (3,), camsets[0]
 
 
+def pushed_cloud(n_far, z_lo, z_hi):
+    """The 20k cloud with n_far of its Gaussians moved along their lines of sight to depths in
+    [z_lo, z_hi): they stay on screen (and visible: the 0.3-pixel dilation gives every splat in
+    front of the camera a few pixels)."""
+    g, sh, d = kat.random_cloud(20000)
+    g = g.copy()
+    rng = np.random.default_rng(5)
+    k = rng.choice(len(g), n_far, replace=False)
+    z = rng.uniform(z_lo, z_hi, n_far).astype(np.float32)
+    ratio = z / g[k, 2]
+    g[k, 0] *= ratio
+    g[k, 1] *= ratio
+    g[k, 2] = z
+    return g, sh, d
+
+
 PROJ_CASES = {
     # at most 4096 tiles: the one-pass tile binning; above: the LSD tile passes and the ranges kernel
     "cloud20k": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(333, 217)),
+    # depths up to 8100: three 9-bit depth passes, keys up to the top of their 27 bits
+    "cloud20k_deep": lambda: (pushed_cloud(300, 4000.0, 8100.0), kat.gpu_test_camera(333, 217)),
+    # depths past 8192: the scene's box keeps the four 8-bit depth passes
+    "cloud20k_far": lambda: (pushed_cloud(300, 8000.0, 30000.0), kat.gpu_test_camera(333, 217)),
     "cloud20k_4096tiles": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(1024, 1024)),  # the binning's largest
     "cloud20k_8160tiles": lambda: (kat.random_cloud(20000), kat.gpu_test_camera(1920, 1088)),
     "config1": lambda: ((lambda s: oracle.Restatement().activate(s) + (3,))(scenes.config(1)[0][0]),
