@@ -62,6 +62,26 @@ __device__ __forceinline__ void blend_px(float p, float L, float r, float g, flo
     }
 }
 
+// blend_px for both of a lane's pixels (the plain forward): the same arithmetic per pixel, with the
+// weights, the new transmittances and the colour sums as packed FP32x2 instructions (per component
+// the rounding of the scalar ones; T + (-1) w in one rounding is T - w) and the conditions as
+// selects: a pixel that does not take the splat adds 0 x colour, which leaves its sum as it was
+// for the finite colours the blend stages.
+__device__ __forceinline__ void blend_px2(float2 p, float L, float r, float g, float b, float2& T, float2& cr,
+                                          float2& cg, float2& cb) {
+    bool v0, v1;
+    const float a0 = splat_alpha(p.x, L, v0), a1 = splat_alpha(p.y, L, v1);
+    const float2 w = __fmul2_rn(make_float2(a0, a1), T);
+    const float2 nt = __ffma2_rn(make_float2(-1.f, -1.f), w, T);
+    const bool k0 = v0 && !(nt.x < 1e-4f), k1 = v1 && !(nt.y < 1e-4f);
+    T.x = v0 ? (k0 ? nt.x : 0.f) : T.x;  // taken, finished (0: it stays finished), or skipped
+    T.y = v1 ? (k1 ? nt.y : 0.f) : T.y;
+    const float2 wk = make_float2(k0 ? w.x : 0.f, k1 ? w.y : 0.f);
+    cr = __ffma2_rn(make_float2(r, r), wk, cr);
+    cg = __ffma2_rn(make_float2(g, g), wk, cg);
+    cb = __ffma2_rn(make_float2(b, b), wk, cb);
+}
+
 // The training outputs of one pixel: float colour, final transmittance, one past the last splat.
 __device__ __forceinline__ void store_train_px(const ViewInfo& vi, int x, int y, float tfin, float cr, float cg,
                                                float cb, unsigned last) {
@@ -143,14 +163,13 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
     const uint2 range = (ctrl->flags & kFlagOverflow) ? make_uint2(0, 0) : ranges[gtile];
 
     // Pixels outside the image start finished.
-    float T0 = (x0 < width && y < height) ? 1.0f : 0.f;
-    float T1 = (x0 + 1 < width && y < height) ? 1.0f : 0.f;
-    float r0 = 0.f, g0 = 0.f, b0c = 0.f, r1 = 0.f, g1 = 0.f, b1c = 0.f;
+    float2 T = make_float2((x0 < width && y < height) ? 1.0f : 0.f, (x0 + 1 < width && y < height) ? 1.0f : 0.f);
+    float2 cr = make_float2(0.f, 0.f), cg = cr, cb = cr;
     unsigned last0 = range.x, last1 = range.x;
     float tf0 = 1.0f, tf1 = 1.0f;
 
     for (unsigned base = range.x; base < range.y; base += kBatch) {
-        if (!__syncthreads_or(T0 + T1 > 0.f)) break;
+        if (!__syncthreads_or(T.x + T.y > 0.f)) break;
 #pragma unroll
         for (int h = 0; h < kBatch / kThreads; ++h) {
             const int slot = tid + h * kThreads;
@@ -158,16 +177,17 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
             unsigned m = 0;
             if (j < range.y) {
                 const SplatRecord r = rec[vals[j]];
+                constexpr float kMax = 3.40282347e38f;  // an infinite colour quantises as the largest finite one
                 s_r0[slot] = r.r0;
-                s_r1[slot] = r.r1;
-                s_b[slot] = r.r2.x;
+                s_r1[slot] = kTrain ? r.r1 : make_float4(r.r1.x, r.r1.y, fminf(r.r1.z, kMax), fminf(r.r1.w, kMax));
+                s_b[slot] = kTrain ? r.r2.x : fminf(r.r2.x, kMax);
                 m = staged_block_mask<TW, TH, kTrain>(r, ox, oy);
             }
             s_mask[slot] = static_cast<unsigned char>(m);
         }
         __syncthreads();
         const unsigned cnt = min(static_cast<unsigned>(kBatch), range.y - base);
-        bool warp_done = !__any_sync(0xFFFFFFFFu, T0 + T1 > 0.f);
+        bool warp_done = !__any_sync(0xFFFFFFFFu, T.x + T.y > 0.f);
         for (unsigned c = 0; c * 32 < cnt && !warp_done; ++c) {
             const unsigned idx = c * 32 + lane;
             unsigned bits = __ballot_sync(0xFFFFFFFFu, idx < cnt && ((s_mask[idx] >> warp) & 1u));
@@ -185,11 +205,15 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
                     const float bb = s_b[jj];
                     float2 dx;
                     const float2 pp = splat_exponents2(a, k, make_float2(px0, px0 + 1.0f), __fsub_rn(py, a.y), dx);
-                    const unsigned pos = base + jj + 1;
-                    blend_px<kTrain>(pp.x, k.y, k.z, k.w, bb, T0, r0, g0, b0c, tf0, last0, pos);
-                    blend_px<kTrain>(pp.y, k.y, k.z, k.w, bb, T1, r1, g1, b1c, tf1, last1, pos);
+                    if (kTrain) {
+                        const unsigned pos = base + jj + 1;
+                        blend_px<kTrain>(pp.x, k.y, k.z, k.w, bb, T.x, cr.x, cg.x, cb.x, tf0, last0, pos);
+                        blend_px<kTrain>(pp.y, k.y, k.z, k.w, bb, T.y, cr.y, cg.y, cb.y, tf1, last1, pos);
+                    } else {
+                        blend_px2(pp, k.y, k.z, k.w, bb, T, cr, cg, cb);
+                    }
                 }
-                if (!__any_sync(0xFFFFFFFFu, T0 + T1 > 0.f)) {
+                if (!__any_sync(0xFFFFFFFFu, T.x + T.y > 0.f)) {
                     warp_done = true;
                     break;
                 }
@@ -197,15 +221,15 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_kernel(const uint2* __restr
         }
     }
     if (kTrain) {
-        store_train_px(vi, x0, y, tf0, r0, g0, b0c, last0);
-        store_train_px(vi, x0 + 1, y, tf1, r1, g1, b1c, last1);
+        store_train_px(vi, x0, y, tf0, cr.x, cg.x, cb.x, last0);
+        store_train_px(vi, x0 + 1, y, tf1, cr.y, cg.y, cb.y, last1);
     }
     if (vi.rgb8) {  // the same for the whole block: one view per tile
         // The lane's two pixels are 6 bytes at an even pixel column: three 2-byte words.
         unsigned short* q = reinterpret_cast<unsigned short*>(s_px + ((y - oy) * TW + (x0 - ox)) * 3);
-        q[0] = static_cast<unsigned short>(quantise(r0) | quantise(g0) << 8);
-        q[1] = static_cast<unsigned short>(quantise(b0c) | quantise(r1) << 8);
-        q[2] = static_cast<unsigned short>(quantise(g1) | quantise(b1c) << 8);
+        q[0] = static_cast<unsigned short>(quantise(cr.x) | quantise(cg.x) << 8);
+        q[1] = static_cast<unsigned short>(quantise(cb.x) | quantise(cr.y) << 8);
+        q[2] = static_cast<unsigned short>(quantise(cg.y) | quantise(cb.y) << 8);
         __syncthreads();
         write_tile_rgb8<TW, TH, kThreads>(s_px, vi.rgb8, width, height, ox, oy);
     }
