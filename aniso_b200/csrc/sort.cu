@@ -137,23 +137,37 @@ __device__ __forceinline__ void span_blocks(unsigned n, unsigned spans, unsigned
     t1 = static_cast<unsigned>(T * (b + 1) / spans);
 }
 
-// Loads block t: lane `lane` of warp `warp` holds items base + warp*kItems*32 + k*32 + lane, so
-// (k, lane) order within a warp is ascending position. dg = the digit (R digits), or R for no item.
-template <int R, bool kMasked, bool kVals>
-__device__ __forceinline__ void load_block(const unsigned* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
-                                           unsigned t, unsigned n, int shift, int warp, int lane, unsigned (&key)[kItems],
-                                           unsigned (&val)[kItems], unsigned (&dg)[kItems]) {
+// Block t: lane `lane` of warp `warp` holds items base + warp*kItems*32 + k*32 + lane, so (k, lane)
+// order within a warp is ascending position. fetch_block issues the loads of the keys (and values
+// with kVals, unless kMasked: there the value is the position); block_digits then gives each item
+// its digit dg (R digits), or R for no item. The two are apart so that a kernel walking several
+// blocks can issue the next block's loads while it still works on the current one.
+template <bool kMasked, bool kVals>
+__device__ __forceinline__ void fetch_block(const unsigned* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
+                                            unsigned t, unsigned n, int warp, int lane, unsigned (&key)[kItems],
+                                            unsigned (&val)[kItems]) {
+    const unsigned long long wbase = static_cast<unsigned long long>(t) * kBlockItems + warp * (kItems * 32) + lane;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const unsigned long long idx = wbase + k * 32;
+        const bool valid = idx < n;
+        key[k] = valid ? keys_in[idx] : 0u;
+        if (!kMasked && kVals) val[k] = valid ? vals_in[idx] : 0u;
+    }
+}
+
+template <int R, bool kMasked>
+__device__ __forceinline__ void block_digits(unsigned t, unsigned n, int shift, int warp, int lane,
+                                             const unsigned (&key)[kItems], unsigned (&val)[kItems],
+                                             unsigned (&dg)[kItems]) {
     const unsigned long long wbase = static_cast<unsigned long long>(t) * kBlockItems + warp * (kItems * 32) + lane;
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
         const unsigned long long idx = wbase + k * 32;
         bool valid = idx < n;
-        key[k] = valid ? keys_in[idx] : 0u;
         if (kMasked) {
             valid = valid && key[k] != kCulledKey;
             val[k] = static_cast<unsigned>(idx);
-        } else if (kVals) {
-            val[k] = valid ? vals_in[idx] : 0u;
         }
         dg[k] = valid ? ((key[k] >> shift) & (R - 1)) : R;
     }
@@ -176,13 +190,14 @@ __global__ void __launch_bounds__(kThreads) upsweep_kernel(const unsigned* __res
     unsigned t0, t1;
     span_blocks(n, spans, blockIdx.x, t0, t1);
     unsigned key[kItems], val[kItems], dg[kItems];
-    if (t0 < t1) load_block<R, kMasked, false>(keys_in, nullptr, t0, n, shift, warp, lane, key, val, dg);
+    if (t0 < t1) fetch_block<kMasked, false>(keys_in, nullptr, t0, n, warp, lane, key, val);
     for (int d = tid; d < R; d += kThreads)
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) s_h[w][d] = 0;
     __syncthreads();
     for (unsigned t = t0; t < t1; ++t) {
-        if (t != t0) load_block<R, kMasked, false>(keys_in, nullptr, t, n, shift, warp, lane, key, val, dg);
+        block_digits<R, kMasked>(t, n, shift, warp, lane, key, val, dg);
+        if (t + 1 < t1) fetch_block<kMasked, false>(keys_in, nullptr, t + 1, n, warp, lane, key, val);  // in flight
 #pragma unroll
         for (int k = 0; k < kItems; ++k)
             if (dg[k] < R) atomicAdd(&s_h[warp][dg[k]], 1u);
@@ -274,13 +289,19 @@ __global__ void __launch_bounds__(kThreads, 4) downsweep_kernel(const unsigned* 
     }
     const unsigned lt = lanemask_lt();
 
+    // The large passes (match_any ranking: many blocks per span) load each next block while the
+    // current one is written out; the small ones (ballots: a block or a few per span) load at the
+    // top of each block, which keeps their registers below the four-CTAs-per-SM bound unspilled.
+    constexpr bool kPrefetch = !kBallot;
+    unsigned key[kItems], val[kItems], dg[kItems];
+    if (kPrefetch && t0 < t1) fetch_block<kMasked, true>(keys_in, vals_in, t0, n, warp, lane, key, val);
     for (unsigned t = t0; t < t1; ++t) {
 #pragma unroll
         for (int j = 0; j < DPT; ++j)
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) s_wh[w][d0 + j] = 0;
-        unsigned key[kItems], val[kItems], dg[kItems];
-        load_block<R, kMasked, true>(keys_in, vals_in, t, n, shift, warp, lane, key, val, dg);
+        if (!kPrefetch) fetch_block<kMasked, true>(keys_in, vals_in, t, n, warp, lane, key, val);
+        block_digits<R, kMasked>(t, n, shift, warp, lane, key, val, dg);
         __syncthreads();
         // Warp-level stable ranking: items in (k, lane) order, i.e. ascending position.
         unsigned rank[kItems];
@@ -337,6 +358,8 @@ __global__ void __launch_bounds__(kThreads, 4) downsweep_kernel(const unsigned* 
             }
         }
         __syncthreads();
+        // The next block's loads go out now and are in flight while this block is written out.
+        if (kPrefetch && t + 1 < t1) fetch_block<kMasked, true>(keys_in, vals_in, t + 1, n, warp, lane, key, val);
         for (unsigned p = tid; p < block_total; p += kThreads) {
             const unsigned k = s_keys[p];
             const unsigned g = s_gbase[(k >> shift) & (R - 1)] + p;
