@@ -23,9 +23,10 @@
 // blocks, one span per CTA, four CTAs per SM): an upsweep counts each span's digits (in a small
 // frame the preprocess and the expansion count the first depth and tile passes as they write the
 // keys, and those passes have no upsweep), one CTA per digit scans that digit's counts over the
-// spans, and a downsweep re-reads each block, ranks it within each warp (match_any, or ballots on
-// the latency-bound small passes), and scatters it through shared memory so global writes are
-// contiguous per digit.
+// spans, and a downsweep re-reads each block, ranks it within each warp (ballots on the
+// latency-bound passes of at most 4M items; match_any in 512-thread CTAs over 4096-item chunks on
+// the large passes of a batch, whose longer digit runs fill more of each written sector), and
+// scatters it through shared memory so global writes are contiguous per digit.
 // No CTA ever waits on another, so there is no spin loop anywhere in the sort; item counts that
 // are known only on the device (visible entries, pairs) are read from the control block, and the
 // grids are sized for the capacity.
@@ -236,15 +237,14 @@ __global__ void __launch_bounds__(kThreads) span_scan_kernel(unsigned* __restric
     if (threadIdx.x == 0) totals[blockIdx.x] = carry;
 }
 
-// Ranks, scatters and writes each block of the span. The masked pass publishes the visible count.
+// The downsweep of a pass of at most kBallotRankMax items (larger ones take downsweep_wide_kernel):
+// ranks, scatters and writes each block of the span. The masked pass publishes the visible count.
 // Thread tid owns digits [tid * DPT, tid * DPT + DPT) in the per-digit phases, so a block scan over
-// the threads' sums is a scan in digit order. Four CTAs per SM (64 registers) keep all
-// kMaxSpans = 4 x 148 spans of a large pass resident in one wave. A lane's peers (the lanes
-// holding the same digit) come from __match_any_sync, or with kBallot from BITS + 1 ballots (one
-// per digit bit, one for validity): more instructions but a shorter dependent chain, which wins
-// where a pass is latency-bound -- a pass of at most 4M items (0.336 -> 0.330 ms per 740k frame)
-// -- and loses on the large passes of a batch.
-template <int BITS, bool kMasked, bool kKeysOut, bool kBallot>
+// the threads' sums is a scan in digit order. Four CTAs per SM (64 registers). A lane's peers (the
+// lanes holding the same digit) come from BITS + 1 ballots (one per digit bit, one for validity):
+// more instructions than __match_any_sync but a shorter dependent chain, which wins where a pass
+// is latency-bound (0.336 -> 0.330 ms per 740k frame).
+template <int BITS, bool kMasked, bool kKeysOut>
 __global__ void __launch_bounds__(kThreads, 4) downsweep_kernel(const unsigned* __restrict__ keys_in,
                                                                 const unsigned* __restrict__ vals_in,
                                                                 unsigned* __restrict__ keys_out,
@@ -289,35 +289,25 @@ __global__ void __launch_bounds__(kThreads, 4) downsweep_kernel(const unsigned* 
     }
     const unsigned lt = lanemask_lt();
 
-    // The large passes (match_any ranking: many blocks per span) load each next block while the
-    // current one is written out; the small ones (ballots: a block or a few per span) load at the
-    // top of each block, which keeps their registers below the four-CTAs-per-SM bound unspilled.
-    constexpr bool kPrefetch = !kBallot;
-    unsigned key[kItems], val[kItems], dg[kItems];
-    if (kPrefetch && t0 < t1) fetch_block<kMasked, true>(keys_in, vals_in, t0, n, warp, lane, key, val);
     for (unsigned t = t0; t < t1; ++t) {
 #pragma unroll
         for (int j = 0; j < DPT; ++j)
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) s_wh[w][d0 + j] = 0;
-        if (!kPrefetch) fetch_block<kMasked, true>(keys_in, vals_in, t, n, warp, lane, key, val);
+        unsigned key[kItems], val[kItems], dg[kItems];
+        fetch_block<kMasked, true>(keys_in, vals_in, t, n, warp, lane, key, val);
         block_digits<R, kMasked>(t, n, shift, warp, lane, key, val, dg);
         __syncthreads();
         // Warp-level stable ranking: items in (k, lane) order, i.e. ascending position.
         unsigned rank[kItems];
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
-            unsigned peers;
-            if (kBallot) {
-                peers = 0xFFFFFFFFu;
+            unsigned peers = 0xFFFFFFFFu;
 #pragma unroll
-                for (int b = 0; b <= BITS; ++b) {
-                    const bool bit = (dg[k] >> b) & 1u;
-                    const unsigned vb = __ballot_sync(0xFFFFFFFFu, bit);
-                    peers &= bit ? vb : ~vb;
-                }
-            } else {
-                peers = __match_any_sync(0xFFFFFFFFu, dg[k]);
+            for (int b = 0; b <= BITS; ++b) {
+                const bool bit = (dg[k] >> b) & 1u;
+                const unsigned vb = __ballot_sync(0xFFFFFFFFu, bit);
+                peers &= bit ? vb : ~vb;
             }
             const unsigned cnt = dg[k] < R ? s_wh[warp][dg[k]] : 0u;
             rank[k] = cnt + __popc(peers & lt);
@@ -358,9 +348,135 @@ __global__ void __launch_bounds__(kThreads, 4) downsweep_kernel(const unsigned* 
             }
         }
         __syncthreads();
-        // The next block's loads go out now and are in flight while this block is written out.
-        if (kPrefetch && t + 1 < t1) fetch_block<kMasked, true>(keys_in, vals_in, t + 1, n, warp, lane, key, val);
         for (unsigned p = tid; p < block_total; p += kThreads) {
+            const unsigned k = s_keys[p];
+            const unsigned g = s_gbase[(k >> shift) & (R - 1)] + p;
+            if (kKeysOut) keys_out[g] = k;
+            vals_out[g] = s_vals[p];
+        }
+        __syncthreads();
+    }
+}
+
+// The downsweep of a large pass (match_any ranking) in 512-thread CTAs over chunks of
+// kWideItems = 4096 items: the same span, digit offsets and stable order as downsweep_kernel,
+// with each chunk's digit runs twice as long (fuller 32-byte sectors in the scattered writes) and
+// half the barriers per item. Thread tid owns digit tid in the per-digit phases (threads past R
+// own none). Shared memory (dynamic): the chunk's keys and values, the warps' digit counts, the
+// digits' chunk starts and global bases.
+constexpr int kWideThreads = 512;
+constexpr int kWideWarps = kWideThreads / 32;
+constexpr int kWideItems = kWideThreads * kItems;
+
+__host__ __device__ constexpr size_t wide_smem_bytes(int bits) {
+    return (2 * static_cast<size_t>(kWideItems) + (kWideWarps + 2) * (static_cast<size_t>(1) << bits)) *
+           sizeof(unsigned);
+}
+
+template <int BITS, bool kMasked, bool kKeysOut>
+__global__ void __launch_bounds__(kWideThreads, 2) downsweep_wide_kernel(const unsigned* __restrict__ keys_in,
+                                                                         const unsigned* __restrict__ vals_in,
+                                                                         unsigned* __restrict__ keys_out,
+                                                                         unsigned* __restrict__ vals_out, SortCount src,
+                                                                         unsigned fixed, unsigned capacity, int shift,
+                                                                         unsigned spans,
+                                                                         const unsigned* __restrict__ counts,
+                                                                         const unsigned* __restrict__ totals, Ctrl* ctrl) {
+    chain_entry();
+    constexpr int R = 1 << BITS;
+    static_assert(R <= kWideThreads, "one digit per thread at most");
+    extern __shared__ unsigned s_dyn[];
+    unsigned* s_keys = s_dyn;                   // [kWideItems]
+    unsigned* s_vals = s_keys + kWideItems;     // [kWideItems]
+    unsigned* s_wh = s_vals + kWideItems;       // [kWideWarps][R]
+    unsigned* s_dstart = s_wh + kWideWarps * R; // [R]
+    unsigned* s_gbase = s_dstart + R;           // [R]
+    __shared__ unsigned s_tmp[kWideWarps];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned n;
+    if (!pass_items(ctrl, src, fixed, capacity, n)) return;
+    unsigned t0, t1;
+    span_blocks(n, spans, blockIdx.x, t0, t1);
+    if (t0 == t1 && !(kMasked && blockIdx.x == 0)) return;  // an empty span (span 0 publishes the count)
+    // The span's items: [i0, i1).
+    const unsigned long long i0 = static_cast<unsigned long long>(t0) * kBlockItems;
+    const unsigned long long i1 = min(static_cast<unsigned long long>(t1) * kBlockItems,
+                                      static_cast<unsigned long long>(n));
+    const bool own = tid < R;
+    unsigned run = 0;  // next global output position of the thread's digit
+    {
+        const unsigned tot = own ? totals[tid] : 0u;
+        unsigned all;
+        const unsigned g = block_excl_scan<kWideThreads>(tot, s_tmp, all);
+        if (kMasked && blockIdx.x == 0 && tid == 0) ctrl->vis_count = all;
+        if (own) run = g + counts[static_cast<size_t>(tid) * spans + blockIdx.x];
+    }
+    const unsigned lt = lanemask_lt();
+
+    unsigned key[kItems], val[kItems], dg[kItems];
+    // Item (warp, k, lane) of the chunk at c: c + warp * kItems * 32 + k * 32 + lane.
+    const auto fetch = [&](unsigned long long c) {
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const unsigned long long idx = c + warp * (kItems * 32) + k * 32 + lane;
+            const bool valid = idx < i1;
+            key[k] = valid ? keys_in[idx] : 0u;
+            if (!kMasked) val[k] = valid ? vals_in[idx] : 0u;
+        }
+    };
+    if (i0 < i1) fetch(i0);
+    for (unsigned long long c = i0; c < i1; c += kWideItems) {
+        for (int i = tid; i < kWideWarps * R; i += kWideThreads) s_wh[i] = 0;
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const unsigned long long idx = c + warp * (kItems * 32) + k * 32 + lane;
+            bool valid = idx < i1;
+            if (kMasked) {
+                valid = valid && key[k] != kCulledKey;
+                val[k] = static_cast<unsigned>(idx);
+            }
+            dg[k] = valid ? ((key[k] >> shift) & (R - 1)) : R;
+        }
+        __syncthreads();
+        unsigned rank[kItems];
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, dg[k]);
+            const unsigned cnt = dg[k] < R ? s_wh[warp * R + dg[k]] : 0u;
+            rank[k] = cnt + __popc(peers & lt);
+            __syncwarp();
+            if (dg[k] < R && lane == 31 - __clz(peers)) s_wh[warp * R + dg[k]] = cnt + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        unsigned cnt = 0;
+        if (own)
+#pragma unroll
+            for (int w = 0; w < kWideWarps; ++w) {
+                const unsigned c2 = s_wh[w * R + tid];
+                s_wh[w * R + tid] = cnt;
+                cnt += c2;
+            }
+        unsigned chunk_total;
+        const unsigned dstart = block_excl_scan<kWideThreads>(cnt, s_tmp, chunk_total);
+        if (own) {
+            s_dstart[tid] = dstart;
+            s_gbase[tid] = run - dstart;
+            run += cnt;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            if (dg[k] < R) {
+                const unsigned pos = s_dstart[dg[k]] + s_wh[warp * R + dg[k]] + rank[k];
+                s_keys[pos] = key[k];
+                s_vals[pos] = val[k];
+            }
+        }
+        __syncthreads();
+        if (c + kWideItems < i1) fetch(c + kWideItems);  // in flight while this chunk is written out
+        for (unsigned p = tid; p < chunk_total; p += kWideThreads) {
             const unsigned k = s_keys[p];
             const unsigned g = s_gbase[(k >> shift) & (R - 1)] + p;
             if (kKeysOut) keys_out[g] = k;
@@ -935,6 +1051,26 @@ void count_pass(const unsigned* keys_in, bool masked, SortCount src, unsigned fi
                        counts, ctrl);
 }
 
+// Launches the wide downsweep, raising its dynamic shared memory limit once per device first.
+template <int BITS, bool kMasked, bool kKeysOut>
+void launch_wide(dim3 grid, cudaStream_t stream, const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out,
+                 unsigned* vals_out, SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned spans,
+                 unsigned* counts, unsigned* totals, Ctrl* ctrl) {
+    constexpr int kDevices = 64;
+    static bool raised[kDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kDevices && !raised[dev]) {
+        if (cudaFuncSetAttribute(downsweep_wide_kernel<BITS, kMasked, kKeysOut>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(wide_smem_bytes(BITS))) == cudaSuccess)
+            raised[dev] = true;
+    }
+    cudaGetLastError();  // a failed raise shows up as the launch's error
+    launch_chained_smem(downsweep_wide_kernel<BITS, kMasked, kKeysOut>, grid, dim3(kWideThreads),
+                        wide_smem_bytes(BITS), stream, keys_in, vals_in, keys_out, vals_out, src, fixed, capacity,
+                        shift, spans, static_cast<const unsigned*>(counts), static_cast<const unsigned*>(totals), ctrl);
+}
+
 template <int BITS>
 void scatter_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* keys_out, unsigned* vals_out, bool masked,
                   SortCount src, unsigned fixed, unsigned capacity, int shift, unsigned* counts, unsigned* totals,
@@ -945,28 +1081,27 @@ void scatter_pass(const unsigned* keys_in, const unsigned* vals_in, unsigned* ke
     launch_chained(span_scan_kernel, dim3(R), block, stream, counts, totals, spans, src, fixed, capacity, ctrl, zero,
                    zero_words);
     const bool small = (src == SortCount::kFixed ? fixed : capacity) <= kBallotRankMax;
-    if (masked) {
-        if (small)
-            launch_chained(downsweep_kernel<BITS, true, true, true>, grid, block, stream, keys_in, vals_in, keys_out,
-                           vals_out, src, fixed, capacity, shift, spans, counts, totals, ctrl);
+    if (!small) {  // a large pass: the wide downsweep
+        if (masked)
+            launch_wide<BITS, true, true>(grid, stream, keys_in, vals_in, keys_out, vals_out, src, fixed, capacity,
+                                          shift, spans, counts, totals, ctrl);
+        else if (keys_out)
+            launch_wide<BITS, false, true>(grid, stream, keys_in, vals_in, keys_out, vals_out, src, fixed, capacity,
+                                           shift, spans, counts, totals, ctrl);
         else
-            launch_chained(downsweep_kernel<BITS, true, true, false>, grid, block, stream, keys_in, vals_in, keys_out,
-                           vals_out, src, fixed, capacity, shift, spans, counts, totals, ctrl);
-    } else if (keys_out) {
-        if (small)
-            launch_chained(downsweep_kernel<BITS, false, true, true>, grid, block, stream, keys_in, vals_in, keys_out,
-                           vals_out, src, fixed, capacity, shift, spans, counts, totals, ctrl);
-        else
-            launch_chained(downsweep_kernel<BITS, false, true, false>, grid, block, stream, keys_in, vals_in, keys_out,
-                           vals_out, src, fixed, capacity, shift, spans, counts, totals, ctrl);
-    } else {
-        if (small)
-            launch_chained(downsweep_kernel<BITS, false, false, true>, grid, block, stream, keys_in, vals_in, keys_out,
-                           vals_out, src, fixed, capacity, shift, spans, counts, totals, ctrl);
-        else
-            launch_chained(downsweep_kernel<BITS, false, false, false>, grid, block, stream, keys_in, vals_in, keys_out,
-                           vals_out, src, fixed, capacity, shift, spans, counts, totals, ctrl);
+            launch_wide<BITS, false, false>(grid, stream, keys_in, vals_in, keys_out, vals_out, src, fixed, capacity,
+                                            shift, spans, counts, totals, ctrl);
+        return;
     }
+    if (masked)
+        launch_chained(downsweep_kernel<BITS, true, true>, grid, block, stream, keys_in, vals_in, keys_out, vals_out,
+                       src, fixed, capacity, shift, spans, counts, totals, ctrl);
+    else if (keys_out)
+        launch_chained(downsweep_kernel<BITS, false, true>, grid, block, stream, keys_in, vals_in, keys_out, vals_out,
+                       src, fixed, capacity, shift, spans, counts, totals, ctrl);
+    else
+        launch_chained(downsweep_kernel<BITS, false, false>, grid, block, stream, keys_in, vals_in, keys_out, vals_out,
+                       src, fixed, capacity, shift, spans, counts, totals, ctrl);
 }
 }  // namespace
 
