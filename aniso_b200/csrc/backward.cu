@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_backward_kernel(BackwardIn 
             s_pos[slot] = in.offs[j] + (static_cast<unsigned>(ty) - ry0) * (rx1 - rx0 + 1) + (static_cast<unsigned>(tx) - rx0);
         }
         __syncthreads();
-        if (__any_sync(0xFFFFFFFFu, start < mylast)) {
+        if (start < wlast) {  // some pixel of the warp applied a splat of this batch
             for (int c = static_cast<int>((cnt - 1) / 32); c >= 0; --c) {
                 const unsigned idx = c * 32 + lane;
                 unsigned bits = __ballot_sync(0xFFFFFFFFu, idx < cnt && ((s_mask[idx] >> warp) & 1u));
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(TW * TH / 2) blend_backward_kernel(BackwardIn 
                     bits &= ~(1u << b);
                     const unsigned jj = c * 32 + b;
                     const unsigned pos = start + jj;
-                    if (!__any_sync(0xFFFFFFFFu, pos < mylast)) continue;
+                    if (pos >= wlast) continue;  // behind every pixel's last applied splat
                     const float4 r0 = s_r0[jj];
                     const float4 r1 = s_r1[jj];
                     const float rb = s_b[jj];
