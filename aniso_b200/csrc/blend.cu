@@ -26,9 +26,9 @@
 //     Testing every block against the ellipse in each tile's staging instead cost more than it
 //     saved: 0.161 -> 0.186 ms of blend;
 //   * each warp walks only its splats (listed once per round from the masks by ballot and
-//     popcount); a finished pixel holds T = 0 (T >= 1e-4
-//     while it is not finished), so no separate flag is carried; the warp leaves once all 64
-//     pixels are finished and the block stops loading once all its warps have (__syncthreads_or).
+//     popcount); a finished pixel holds T = 0 (T >= 1e-4 while it is not finished), so no
+//     separate flag is carried; the warp leaves once all 64 pixels are finished and the block
+//     stops loading once all its warps have (__syncthreads_or).
 #include "common.cuh"
 #include "kernels.h"
 
