@@ -11,7 +11,7 @@
 // Per view:
 //   rec     float4[3][N]  blend record of each visible Gaussian (see SplatRecord)
 //   rect    uint64[N]     16x16-tile rectangle x0 | y0 << 16 | x1 << 32 | y1 << 48
-//   depth_key uint32[N]   float bits of each Gaussian's depth, kCulledKey when culled
+//   depth_key uint32[N]   float bits of each Gaussian's depth less kDepthKeyBase, kCulledKey when culled
 //   vis_key / vis_idx     the visible list being depth-sorted: depth bits and Gaussian index
 //   pair_key / pair_val   one (tile, Gaussian) pair per tile a splat touches
 //   ranges  uint2[tiles]  [start, end) of each tile's run in the sorted pair list
